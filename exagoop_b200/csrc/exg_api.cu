@@ -1,0 +1,1001 @@
+// exg_api.cu -- C ABI of the B200 MPM step: context, particle upload and
+// download, one entry point per reference L5 step function, and the fused,
+// graph-replayed exg_step.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <tuple>
+#include "exg_internal.h"
+
+using namespace exg;
+
+struct exg_ctx {
+    Ctx c;
+};
+
+namespace {
+
+int fail(exg_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->c.err = msg;
+    return code;
+}
+
+#define EXG_TRY(ctx, ...)                                          \
+    try {                                                          \
+        __VA_ARGS__;                                               \
+    } catch (const std::exception &e) {                            \
+        return fail(ctx, EXG_ERR_CUDA, e.what());                  \
+    }
+
+bool fp64(const Ctx &c) { return c.precision == EXG_PREC_FP64; }
+
+// precision dispatch of the launchers
+#define DISPATCH(name, ...) (fp64(c) ? name##_fp64(__VA_ARGS__) : name##_fp32(__VA_ARGS__))
+
+template <class T>
+T *dalloc(size_t n) {
+    void *p = nullptr;
+    if (n == 0) n = 1;
+    EXG_CUDA_OK(cudaMalloc(&p, n * sizeof(T)));
+    return reinterpret_cast<T *>(p);
+}
+
+int ilog2(int v) {
+    int s = 0;
+    while ((1 << s) < v) ++s;
+    return s;
+}
+
+void build_params(Ctx &c) {
+    const exg_specs &s = c.specs;
+    Params &P = c.P;
+    std::memset(&P, 0, sizeof(P));
+    for (int d = 0; d < 3; ++d) {
+        P.plo[d] = s.plo[d];
+        P.phi[d] = s.phi[d];
+        P.nc[d] = s.ncells[d];
+        P.nn[d] = s.ncells[d] + 1;
+        // AMReX Geometry: dx = (hi - lo) / n, inv_dx = 1 / dx
+        P.dx[d] = (s.phi[d] - s.plo[d]) / (double)s.ncells[d];
+        P.dxi[d] = 1.0 / P.dx[d];
+        P.periodic[d] = s.periodic[d];
+        P.order[d] = s.order[d];
+        P.gravity[d] = s.gravity[d];
+        P.slab_lo[d] = s.force_slab_lo[d];
+        P.slab_hi[d] = s.force_slab_hi[d];
+        P.extforce[d] = s.extforce[d];
+        P.bclo[d] = s.bclo[d];
+        P.bchi[d] = s.bchi[d];
+        P.wmu_lo[d] = s.wall_mu_lo[d];
+        P.wmu_hi[d] = s.wall_mu_hi[d];
+        P.udf_lo[d] = s.udf_wallvel_lo[d] != nullptr;
+        P.udf_hi[d] = s.udf_wallvel_hi[d] != nullptr;
+    }
+    for (int i = 0; i < 9; ++i) {
+        P.wvel_lo[i] = s.wall_vel_lo[i];
+        P.wvel_hi[i] = s.wall_vel_hi[i];
+    }
+    P.nnodes = (long long)P.nn[0] * P.nn[1] * P.nn[2];
+    P.uniform_order = (s.order[0] == s.order[1] && s.order[1] == s.order[2]) ? s.order[0] : 0;
+    P.external_loads = s.external_loads;
+    P.mass_tol = s.mass_tolerance;
+    P.alpha = s.alpha_pic_flip;
+    P.applied_sr = s.applied_strainrate;
+    P.applied_sr_time = s.applied_strainrate_time;
+    P.fixed_dt = s.fixed_timestep == 1;
+    P.timestep = s.timestep;
+    P.cfl = s.cfl;
+    P.dt_min = s.dt_min_limit;
+    P.dt_max = s.dt_max_limit;
+    P.dxmin = std::min(P.dx[0], std::min(P.dx[1], P.dx[2]));
+    P.num_bodies = s.num_bodies;
+    for (int b = 0; b < s.num_bodies && b < kMaxBodies; ++b) {
+        const exg_body &e = s.bodies[b];
+        Body &o = P.body[b];
+        o.mom_bc = e.mom_bc;
+        o.wall_mu = e.wall_mu;
+        for (int d = 0; d < 3; ++d) o.wall_vel[d] = e.wall_vel[d];
+        o.temp_bc = e.temp_bc;
+        o.T_wall = e.T_wall;
+        o.heat_flux = e.heat_flux;
+        o.h_conv = e.h_conv;
+        o.T_inf = e.T_inf;
+    }
+    P.use_temp = s.use_temp;
+    // tile geometry
+    int T = s.tile > 0 ? s.tile : 8;
+    P.T = T;
+    P.tshift = ilog2(T);
+    const bool lin = (P.uniform_order == 1);
+    P.hlo = lin ? 0 : 1;
+    P.hhi = lin ? 1 : 2;
+    P.B = T + P.hlo + P.hhi;
+    for (int d = 0; d < 3; ++d)
+        P.ntile[d] = s.periodic[d] ? s.ncells[d] / T : (s.ncells[d] + 1 + T - 1) / T;
+    P.ntiles = (long long)P.ntile[0] * P.ntile[1] * P.ntile[2];
+}
+
+std::string validate(const exg_specs &s) {
+    for (int d = 0; d < 3; ++d) {
+        if (s.ncells[d] < 1) return "mpm.ncells must be positive";
+        if (!(s.phi[d] > s.plo[d])) return "mpm.prob_hi must exceed mpm.prob_lo";
+        if (s.order[d] < 1 || s.order[d] > 3) return "order_scheme_directional must be 1, 2 or 3";
+    }
+    int T = s.tile > 0 ? s.tile : 8;
+    if (T != 4 && T != 8) return "exg.tile must be 4 or 8";
+    for (int d = 0; d < 3; ++d)
+        if (s.periodic[d] && (s.ncells[d] % T != 0 || s.ncells[d] < 3 * T))
+            return "periodic axes need ncells to be a multiple of the tile edge and at least three tiles";
+    if (s.calculate_strain_based_on_delta) return "calculate_strain_based_on_delta = 1 is outside this library's scope";
+    if (s.num_bodies < 0 || s.num_bodies > EXG_MAX_BODIES) return "too many level-set bodies";
+    return "";
+}
+
+template <class R>
+void alloc_parts(Ctx &c, Parts<R> &P, std::vector<void *> &al, long long n, bool temp) {
+    auto A = [&](auto *&ptr) {
+        using T = std::remove_pointer_t<std::remove_reference_t<decltype(ptr)>>;
+        ptr = dalloc<T>(n);
+        al.push_back(ptr);
+    };
+    std::memset(&P, 0, sizeof(P));
+    for (int d = 0; d < 3; ++d) {
+        A(P.x[d]);
+        A(P.v[d]);
+        A(P.vp[d]);
+    }
+    for (int k = 0; k < 6; ++k) {
+        A(P.sr[k]);
+        A(P.eps[k]);
+        A(P.sig[k]);
+    }
+    for (int k = 0; k < 9; ++k) A(P.E[k]);
+    A(P.vol);
+    A(P.mass);
+    A(P.rho);
+    A(P.J);
+    A(P.pres);
+    A(P.vol0);
+    A(P.radius);
+    A(P.yacc);
+    if (temp) {
+        A(P.T);
+        A(P.cp);
+        A(P.kc);
+        for (int d = 0; d < 3; ++d) A(P.q[d]);
+        A(P.Q);
+    }
+    A(P.mat);
+    A(P.phase);
+    A(P.rigid);
+    A(P.pid);
+    (void)c;
+}
+
+void free_list(std::vector<void *> &al) {
+    for (void *p : al) cudaFree(p);
+    al.clear();
+}
+
+template <class R>
+void upload_parts(Ctx &c, const exg_particle_soa *h, const std::vector<int32_t> &mat) {
+    Parts<R> &P = c.A<R>();
+    const long long n = h->np;
+    std::vector<R> buf(n);
+    auto put_r = [&](R *dst, int field, double sub = 0.0) {
+        const double *src = h->rdata + (size_t)field * n;
+        for (long long i = 0; i < n; ++i) buf[i] = (R)(src[i] - sub);
+        EXG_CUDA_OK(cudaMemcpy(dst, buf.data(), sizeof(R) * n, cudaMemcpyHostToDevice));
+    };
+    for (int d = 0; d < 3; ++d) {
+        EXG_CUDA_OK(cudaMemcpy(P.x[d], h->pos + (size_t)d * n, sizeof(double) * n, cudaMemcpyHostToDevice));
+        put_r(P.v[d], EXG_R_VEL + d);
+        put_r(P.vp[d], EXG_R_VEL_PRIME + d);
+    }
+    for (int k = 0; k < 6; ++k) {
+        put_r(P.sr[k], EXG_R_STRAINRATE + k);
+        put_r(P.eps[k], EXG_R_STRAIN + k);
+        put_r(P.sig[k], EXG_R_STRESS + k);
+    }
+    for (int k = 0; k < 9; ++k) put_r(P.E[k], EXG_R_DEFGRAD + k, (k % 4 == 0) ? 1.0 : 0.0);
+    put_r(P.vol, EXG_R_VOLUME);
+    put_r(P.mass, EXG_R_MASS);
+    put_r(P.rho, EXG_R_DENSITY);
+    put_r(P.J, EXG_R_JACOBIAN);
+    put_r(P.pres, EXG_R_PRESSURE);
+    put_r(P.vol0, EXG_R_VOL_INIT);
+    put_r(P.radius, EXG_R_RADIUS);
+    put_r(P.yacc, EXG_R_YACC);
+    if (c.specs.use_temp) {
+        put_r(P.T, EXG_R_TEMPERATURE);
+        put_r(P.cp, EXG_R_SPHEAT);
+        put_r(P.kc, EXG_R_THERMCOND);
+        for (int d = 0; d < 3; ++d) put_r(P.q[d], EXG_R_HEATFLUX + d);
+        put_r(P.Q, EXG_R_HEATSRC);
+    }
+    EXG_CUDA_OK(cudaMemcpy(P.mat, mat.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    std::vector<uint8_t> ph(n);
+    std::vector<int32_t> rid(n), pid(n);
+    for (long long i = 0; i < n; ++i) {
+        ph[i] = (uint8_t)h->idata[(size_t)EXG_I_PHASE * n + i];
+        rid[i] = h->idata[(size_t)EXG_I_RIGID_ID * n + i];
+        pid[i] = (int32_t)i;
+    }
+    EXG_CUDA_OK(cudaMemcpy(P.phase, ph.data(), n, cudaMemcpyHostToDevice));
+    EXG_CUDA_OK(cudaMemcpy(P.rigid, rid.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    EXG_CUDA_OK(cudaMemcpy(P.pid, pid.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+}
+
+template <class R>
+void download_parts(Ctx &c, exg_particle_soa *h) {
+    Parts<R> &P = c.A<R>();
+    const long long n = c.np;
+    std::vector<int32_t> pid(n);
+    EXG_CUDA_OK(cudaMemcpy(pid.data(), P.pid, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    std::vector<R> buf(n);
+    auto get_r = [&](const R *src, int field, double add = 0.0) {
+        EXG_CUDA_OK(cudaMemcpy(buf.data(), src, sizeof(R) * n, cudaMemcpyDeviceToHost));
+        double *dst = h->rdata + (size_t)field * n;
+        for (long long i = 0; i < n; ++i) dst[pid[i]] = (double)buf[i] + add;
+    };
+    std::vector<double> xb(n);
+    for (int d = 0; d < 3; ++d) {
+        EXG_CUDA_OK(cudaMemcpy(xb.data(), P.x[d], sizeof(double) * n, cudaMemcpyDeviceToHost));
+        for (long long i = 0; i < n; ++i) h->pos[(size_t)d * n + pid[i]] = xb[i];
+        get_r(P.v[d], EXG_R_VEL + d);
+        get_r(P.vp[d], EXG_R_VEL_PRIME + d);
+    }
+    for (int k = 0; k < 6; ++k) {
+        get_r(P.sr[k], EXG_R_STRAINRATE + k);
+        get_r(P.eps[k], EXG_R_STRAIN + k);
+        get_r(P.sig[k], EXG_R_STRESS + k);
+    }
+    for (int k = 0; k < 9; ++k) get_r(P.E[k], EXG_R_DEFGRAD + k, (k % 4 == 0) ? 1.0 : 0.0);
+    get_r(P.vol, EXG_R_VOLUME);
+    get_r(P.mass, EXG_R_MASS);
+    get_r(P.rho, EXG_R_DENSITY);
+    get_r(P.J, EXG_R_JACOBIAN);
+    get_r(P.pres, EXG_R_PRESSURE);
+    get_r(P.vol0, EXG_R_VOL_INIT);
+    get_r(P.radius, EXG_R_RADIUS);
+    get_r(P.yacc, EXG_R_YACC);
+    if (c.specs.use_temp) {
+        get_r(P.T, EXG_R_TEMPERATURE);
+        get_r(P.cp, EXG_R_SPHEAT);
+        get_r(P.kc, EXG_R_THERMCOND);
+        for (int d = 0; d < 3; ++d) get_r(P.q[d], EXG_R_HEATFLUX + d);
+        get_r(P.Q, EXG_R_HEATSRC);
+    } else {
+        const int tf[7] = {EXG_R_TEMPERATURE, EXG_R_SPHEAT,         EXG_R_THERMCOND, EXG_R_HEATFLUX,
+                           EXG_R_HEATFLUX + 1, EXG_R_HEATFLUX + 2, EXG_R_HEATSRC};
+        for (int f : tf)
+            std::fill(h->rdata + (size_t)f * n, h->rdata + (size_t)(f + 1) * n, 0.0);
+    }
+    std::vector<int32_t> mat(n), rid(n);
+    std::vector<uint8_t> ph(n);
+    EXG_CUDA_OK(cudaMemcpy(mat.data(), P.mat, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    EXG_CUDA_OK(cudaMemcpy(rid.data(), P.rigid, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    EXG_CUDA_OK(cudaMemcpy(ph.data(), P.phase, n, cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < n; ++i) {
+        const Material &m = c.mats[mat[i]];
+        const long long j = pid[i];
+        h->rdata[(size_t)EXG_R_E * n + j] = m.E;
+        h->rdata[(size_t)EXG_R_NU * n + j] = m.nu;
+        h->rdata[(size_t)EXG_R_BULK * n + j] = m.K;
+        h->rdata[(size_t)EXG_R_GAMMA * n + j] = m.gamma;
+        h->rdata[(size_t)EXG_R_VISC * n + j] = m.mu;
+        h->idata[(size_t)EXG_I_PHASE * n + j] = ph[i];
+        h->idata[(size_t)EXG_I_RIGID_ID * n + j] = rid[i];
+        h->idata[(size_t)EXG_I_MODEL * n + j] = m.model;
+    }
+}
+
+void sync(Ctx &c) { EXG_CUDA_OK(cudaStreamSynchronize(c.stream)); }
+
+void ctl_pull(Ctx &c) {
+    EXG_CUDA_OK(cudaMemcpyAsync(c.ctl_host, c.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c.stream));
+    sync(c);
+}
+
+// UDF wall tables of compute_udf_wall_vel_at_nodes (nodal_data_ops.cpp:929-1059),
+// tabulated on the host at time t and copied to the device.
+void tabulate_udf(Ctx &c, double t) {
+    for (int side = 0; side < 2; ++side)
+        for (int d = 0; d < 3; ++d) {
+            exg_wallvel_udf fn = side ? c.specs.udf_wallvel_hi[d] : c.specs.udf_wallvel_lo[d];
+            if (!fn) continue;
+            const int p0 = (d == 0) ? 1 : 0, p1 = (d == 2) ? 1 : 2;
+            const int n0 = c.P.nc[p0] + 1, n1 = c.P.nc[p1] + 1;
+            std::vector<double> &tab = c.udf_host[side][d];
+            tab.assign((size_t)n0 * n1 * 3, 0.0);
+            for (int j = 0; j < n0; ++j)
+                for (int k = 0; k < n1; ++k) {
+                    double xc[3] = {0, 0, 0};
+                    xc[d] = side ? c.P.phi[d] : c.P.plo[d];
+                    xc[p0] = c.P.plo[p0] + j * c.P.dx[p0];
+                    xc[p1] = c.P.plo[p1] + k * c.P.dx[p1];
+                    double vel[3] = {0, 0, 0};
+                    fn(xc[0], xc[1], xc[2], t, vel);
+                    for (int q = 0; q < 3; ++q) tab[((size_t)j * n1 + k) * 3 + q] = vel[q];
+                }
+            if (!c.udf_tab[side][d]) c.udf_tab[side][d] = dalloc<double>(tab.size());
+            EXG_CUDA_OK(cudaMemcpyAsync(c.udf_tab[side][d], tab.data(), sizeof(double) * tab.size(),
+                                        cudaMemcpyHostToDevice, c.stream));
+            sync(c);
+        }
+}
+bool has_udf(const Ctx &c) {
+    for (int d = 0; d < 3; ++d)
+        if (c.specs.udf_wallvel_lo[d] || c.specs.udf_wallvel_hi[d]) return true;
+    return false;
+}
+
+int status_from_ctl(Ctx &c) {
+    ctl_pull(c);
+    unsigned st = c.ctl_host->status;
+    if (st) {
+        EXG_CUDA_OK(cudaMemsetAsync(&c.ctl->status, 0, sizeof(unsigned), c.stream));
+        sync(c);
+    }
+    if (st & ST_BC) {
+        c.err = "outflow wall BC reached applybc (the reference aborts here)";
+        return EXG_ERR_BC;
+    }
+    if (st & ST_NAN) {
+        c.err = "non-finite particle velocity, stress or Jacobian";
+        return EXG_ERR_NAN;
+    }
+    if (st & ST_OVERFLOW) {
+        c.err = "fixed-point range overflow";
+        return EXG_ERR_OVERFLOW;
+    }
+    return EXG_OK;
+}
+
+// Sort by cell key for the current storage order (Redistribute).
+void do_sort(Ctx &c, bool touched) {
+    launch_keys(c);
+    launch_sort_rest(c, touched);
+    c.parts_sorted = true;
+}
+
+// Fresh particle reductions into the control block accumulators.
+void do_reduce(Ctx &c) {
+    launch_reset_accum(c, &c.ctl->bound_bits[0], &c.ctl->dtmin_bits);
+    DISPATCH(launch_state_reduce, c, &c.ctl->bound_bits[0], &c.ctl->dtmin_bits);
+    c.reduce_stale = false;
+}
+
+void ensure_nodes_clean(Ctx &c);
+
+// One fused step, enqueued on c.stream (capturable).
+void enqueue_step(Ctx &c) {
+    EXG_CUDA_OK(cudaMemcpyAsync(c.bounds_cur, &c.ctl->bound_bits[0], sizeof(unsigned long long) * CH_ALL,
+                                cudaMemcpyDeviceToDevice, c.stream));
+    launch_dt_finalize(c, true);
+    if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[0], c.stream));
+    launch_keys(c);
+    launch_sort_rest(c, true);
+    if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[1], c.stream));
+    launch_scales_from(c, c.bounds_cur);
+    DISPATCH(launch_p2g, c, PF_MASS | PF_VEL | PF_FORCE);
+    if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[2], c.stream));
+    DISPATCH(launch_nodes, c, NM_FUSED, PF_MASS | PF_VEL | PF_FORCE, false);
+    if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[3], c.stream));
+    if (c.specs.stress_update_scheme == 0) {
+        DISPATCH(launch_g2p_fused, c, GM_FULL);
+    } else {
+        DISPATCH(launch_g2p_fused, c, GM_VEL);
+        launch_reset_accum(c, c.bounds2, c.dtmin2);
+        DISPATCH(launch_state_reduce, c, c.bounds2, c.dtmin2);
+        launch_scales_from(c, c.bounds2);
+        DISPATCH(launch_p2g, c, PF_VEL);
+        DISPATCH(launch_nodes, c, NM_MUSL2, PF_VEL, false);
+        DISPATCH(launch_g2p_fused, c, GM_STRAIN);
+    }
+    DISPATCH(launch_copy_lost, c);
+    if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[4], c.stream));
+    launch_time_advance(c);
+}
+
+void swap_parts(Ctx &c) {
+    std::swap(c.pa, c.pb);
+    c.orient ^= 1;
+}
+
+void drop_graphs(Ctx &c) {
+    for (int k = 0; k < 2; ++k) {
+        if (c.gexec[k]) cudaGraphExecDestroy(c.gexec[k]);
+        c.gexec[k] = nullptr;
+        c.warm[k] = false;
+    }
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+int exg_ctx_create(const exg_specs *specs, int device, exg_ctx **out) {
+    if (!specs || !out) return EXG_ERR_ARG;
+    *out = nullptr;
+    std::string v = validate(*specs);
+    if (!v.empty()) {
+        fprintf(stderr, "exg_ctx_create: %s\n", v.c_str());
+        return EXG_ERR_CONFIG;
+    }
+    exg_ctx *ctx = new exg_ctx();
+    Ctx &c = ctx->c;
+    try {
+        c.specs = *specs;
+        c.precision = specs->precision;
+        c.timing = std::getenv("EXG_STAGE_TIMING") != nullptr;
+        c.device = device;
+        EXG_CUDA_OK(cudaSetDevice(device));
+        EXG_CUDA_OK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        upload_tables_fp64();
+        upload_tables_fp32();
+        build_params(c);
+        const size_t esz = fp64(c) ? 8 : 4;
+        // nodes: 26 reference components, dense
+        if (fp64(c)) {
+            auto *N = new Nodes<double>();
+            for (int k = 0; k < EXG_N_NCOMP; ++k) {
+                N->c[k] = dalloc<double>(c.P.nnodes);
+                c.node_allocs.push_back(N->c[k]);
+            }
+            c.nodes = N;
+        } else {
+            auto *N = new Nodes<float>();
+            for (int k = 0; k < EXG_N_NCOMP; ++k) {
+                N->c[k] = dalloc<float>(c.P.nnodes);
+                c.node_allocs.push_back(N->c[k]);
+            }
+            c.nodes = N;
+        }
+        for (void *p : c.node_allocs) EXG_CUDA_OK(cudaMemset(p, 0, esz * c.P.nnodes));
+        c.ctl = dalloc<Ctl>(1);
+        EXG_CUDA_OK(cudaMemset(c.ctl, 0, sizeof(Ctl)));
+        EXG_CUDA_OK(cudaMallocHost(&c.ctl_host, sizeof(Ctl)));
+        c.bounds_cur = dalloc<unsigned long long>(CH_ALL);
+        c.bounds2 = dalloc<unsigned long long>(CH_ALL);
+        c.dtmin2 = dalloc<unsigned long long>(1);
+        c.diag_dev = nullptr;
+        // sort and tile buffers
+        const long long nt = c.P.ntiles;
+        c.sb.tile_count = dalloc<int>(nt);
+        c.sb.tile_fill = dalloc<int>(nt);
+        c.sb.tile_start = dalloc<int>(nt);
+        c.sb.active = dalloc<int>(nt);
+        c.sb.slot = dalloc<int>(nt);
+        c.sb.touched = dalloc<int>(nt);
+        c.sb.touched_step = dalloc<long long>(nt);
+        EXG_CUDA_OK(cudaMemset(c.sb.touched_step, 0xff, sizeof(long long) * nt));  // -1: never
+        EXG_CUDA_OK(cudaMemset(c.sb.slot, 0xff, sizeof(int) * nt));
+        c.nch = specs->use_temp ? CH_ALL : CH_MOM_END;
+        const long long B3 = (long long)c.P.B * c.P.B * c.P.B;
+        c.staging_cap = (size_t)nt;
+        c.staging = dalloc<long long>((size_t)nt * c.nch * B3);
+        for (int k = 0; k < 6; ++k) EXG_CUDA_OK(cudaEventCreate(&c.ev[k]));
+        // initial dt accumulators: "no particles"
+        launch_reset_accum(c, &c.ctl->bound_bits[0], &c.ctl->dtmin_bits);
+        sync(c);
+    } catch (const std::exception &e) {
+        fprintf(stderr, "exg_ctx_create: %s\n", e.what());
+        exg_ctx_destroy(ctx);
+        return EXG_ERR_CUDA;
+    }
+    *out = ctx;
+    return EXG_OK;
+}
+
+int exg_ctx_destroy(exg_ctx *ctx) {
+    if (!ctx) return EXG_OK;
+    Ctx &c = ctx->c;
+    drop_graphs(c);
+    free_list(c.allocs_a);
+    free_list(c.allocs_b);
+    free_list(c.node_allocs);
+    if (c.precision == EXG_PREC_FP64) {
+        delete reinterpret_cast<Parts<double> *>(c.pa);
+        delete reinterpret_cast<Parts<double> *>(c.pb);
+        delete reinterpret_cast<Nodes<double> *>(c.nodes);
+    } else {
+        delete reinterpret_cast<Parts<float> *>(c.pa);
+        delete reinterpret_cast<Parts<float> *>(c.pb);
+        delete reinterpret_cast<Nodes<float> *>(c.nodes);
+    }
+    for (double *p : c.ls) cudaFree(p);
+    for (auto &row : c.udf_tab)
+        for (double *p : row) cudaFree(p);
+    void *bufs[] = {c.sb.key, c.sb.perm, c.sb.bucket, c.sb.tile_count, c.sb.tile_fill, c.sb.tile_start,
+                    c.sb.active, c.sb.slot, c.sb.touched, c.sb.touched_step, c.staging, c.ctl,
+                    c.bounds_cur, c.bounds2, c.dtmin2, c.mat_dev, c.diag_dev};
+    for (void *p : bufs) cudaFree(p);
+    if (c.ctl_host) cudaFreeHost(c.ctl_host);
+    for (auto &e : c.ev)
+        if (e) cudaEventDestroy(e);
+    if (c.stream) cudaStreamDestroy(c.stream);
+    delete ctx;
+    return EXG_OK;
+}
+
+const char *exg_last_error(const exg_ctx *ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
+
+int exg_synchronize(exg_ctx *ctx) {
+    if (!ctx) return EXG_ERR_ARG;
+    EXG_TRY(ctx, sync(ctx->c));
+    return EXG_OK;
+}
+
+int exg_check_status(exg_ctx *ctx) {
+    if (!ctx) return EXG_ERR_ARG;
+    EXG_TRY(ctx, return status_from_ctl(ctx->c));
+}
+
+int exg_set_levelset(exg_ctx *ctx, int body, const double *phi) {
+    if (!ctx || body < 0 || body >= EXG_MAX_BODIES || !phi) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        if (!c.ls[body]) c.ls[body] = dalloc<double>(c.P.nnodes);
+        EXG_CUDA_OK(cudaMemcpy(c.ls[body], phi, sizeof(double) * c.P.nnodes, cudaMemcpyHostToDevice));
+        drop_graphs(c);
+    });
+    return EXG_OK;
+}
+
+int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
+    if (!ctx || !p || p->np < 0) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (p->np > (long long)0x7fffffff) return fail(ctx, EXG_ERR_ARG, "more than 2^31-1 particles");
+    EXG_TRY(ctx, {
+        const long long n = p->np;
+        // material table: one entry per distinct (E, nu, K, gamma, mu, model)
+        std::map<std::tuple<double, double, double, double, double, int>, int> idx;
+        std::vector<int32_t> mat(n);
+        c.mats.clear();
+        for (long long i = 0; i < n; ++i) {
+            Material m;
+            m.E = p->rdata[(size_t)EXG_R_E * n + i];
+            m.nu = p->rdata[(size_t)EXG_R_NU * n + i];
+            m.K = p->rdata[(size_t)EXG_R_BULK * n + i];
+            m.gamma = p->rdata[(size_t)EXG_R_GAMMA * n + i];
+            m.mu = p->rdata[(size_t)EXG_R_VISC * n + i];
+            m.model = p->idata[(size_t)EXG_I_MODEL * n + i];
+            m.pad = 0;
+            auto key = std::make_tuple(m.E, m.nu, m.K, m.gamma, m.mu, m.model);
+            auto it = idx.find(key);
+            if (it == idx.end()) {
+                it = idx.emplace(key, (int)c.mats.size()).first;
+                c.mats.push_back(m);
+            }
+            mat[i] = it->second;
+        }
+        if (c.mats.empty()) c.mats.push_back(Material{});
+        if (c.mat_dev) cudaFree(c.mat_dev);
+        c.mat_dev = dalloc<Material>(c.mats.size());
+        EXG_CUDA_OK(cudaMemcpy(c.mat_dev, c.mats.data(), sizeof(Material) * c.mats.size(), cudaMemcpyHostToDevice));
+        // particle storage (re-allocated on every upload)
+        free_list(c.allocs_a);
+        free_list(c.allocs_b);
+        drop_graphs(c);
+        if (c.orient) std::swap(c.pa, c.pb);
+        c.orient = 0;
+        const bool temp = c.specs.use_temp != 0;
+        if (fp64(c)) {
+            delete reinterpret_cast<Parts<double> *>(c.pa);
+            delete reinterpret_cast<Parts<double> *>(c.pb);
+            auto *a = new Parts<double>(), *b = new Parts<double>();
+            alloc_parts(c, *a, c.allocs_a, n, temp);
+            alloc_parts(c, *b, c.allocs_b, n, temp);
+            c.pa = a;
+            c.pb = b;
+            c.np = n;
+            upload_parts<double>(c, p, mat);
+        } else {
+            delete reinterpret_cast<Parts<float> *>(c.pa);
+            delete reinterpret_cast<Parts<float> *>(c.pb);
+            auto *a = new Parts<float>(), *b = new Parts<float>();
+            alloc_parts(c, *a, c.allocs_a, n, temp);
+            alloc_parts(c, *b, c.allocs_b, n, temp);
+            c.pa = a;
+            c.pb = b;
+            c.np = n;
+            upload_parts<float>(c, p, mat);
+        }
+        c.cap = n;
+        cudaFree(c.sb.key);
+        cudaFree(c.sb.perm);
+        cudaFree(c.sb.bucket);
+        c.sb.key = dalloc<uint32_t>(n);
+        c.sb.perm = dalloc<int32_t>(n);
+        c.sb.bucket = dalloc<int32_t>(2 * n);
+        c.parts_sorted = false;
+        c.reduce_stale = true;
+        sync(c);
+    });
+    return EXG_OK;
+}
+
+int exg_particles_download(exg_ctx *ctx, exg_particle_soa *p) {
+    if (!ctx || !p) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (p->np != c.np) return fail(ctx, EXG_ERR_ARG, "np mismatch");
+    EXG_TRY(ctx, {
+        sync(c);
+        if (fp64(c))
+            download_parts<double>(c, p);
+        else
+            download_parts<float>(c, p);
+    });
+    return EXG_OK;
+}
+
+int exg_num_particles(exg_ctx *ctx, int64_t *np) {
+    if (!ctx || !np) return EXG_ERR_ARG;
+    *np = ctx->c.np;
+    return EXG_OK;
+}
+
+int exg_nodes_download(exg_ctx *ctx, int comp, double *out) {
+    if (!ctx || !out || comp < 0 || comp >= EXG_N_NCOMP) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        sync(c);
+        const long long n = c.P.nnodes;
+        if (fp64(c)) {
+            EXG_CUDA_OK(cudaMemcpy(out, c.N<double>().c[comp], sizeof(double) * n, cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<float> b(n);
+            EXG_CUDA_OK(cudaMemcpy(b.data(), c.N<float>().c[comp], sizeof(float) * n, cudaMemcpyDeviceToHost));
+            for (long long i = 0; i < n; ++i) out[i] = b[i];
+        }
+        // periodic axes: node ncells is node 0
+        const int *nn = c.P.nn;
+        for (int k = 0; k < nn[2]; ++k)
+            for (int j = 0; j < nn[1]; ++j)
+                for (int i = 0; i < nn[0]; ++i) {
+                    int w[3] = {i, j, k};
+                    bool alias = false;
+                    for (int d = 0; d < 3; ++d)
+                        if (c.P.periodic[d] && w[d] == c.P.nc[d]) {
+                            w[d] = 0;
+                            alias = true;
+                        }
+                    if (alias)
+                        out[((long long)k * nn[1] + j) * nn[0] + i] = out[((long long)w[2] * nn[1] + w[1]) * nn[0] + w[0]];
+                }
+    });
+    return EXG_OK;
+}
+
+// ----------------------------------------------------- L5 step functions
+int exg_redistribute(exg_ctx *ctx) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        EXG_CUDA_OK(cudaMemsetAsync(&c.ctl->lost, 0, sizeof(unsigned long long), c.stream));
+        EXG_CUDA_OK(cudaMemsetAsync(&c.ctl->maxppc, 0, sizeof(int), c.stream));
+        do_sort(c, false);
+        ctl_pull(c);
+        if (c.ctl_host->lost) {
+            c.err = std::to_string(c.ctl_host->lost) + " particles are outside the domain";
+            return EXG_ERR_DOMAIN;
+        }
+    });
+    return EXG_OK;
+}
+
+int exg_calculate_time_step(exg_ctx *ctx, double *dt) {
+    if (!ctx || !dt) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        do_reduce(c);
+        launch_dt_finalize(c, false);
+        ctl_pull(c);
+        *dt = c.ctl_host->dt;
+    });
+    return EXG_OK;
+}
+
+int exg_reset_nodaldata(exg_ctx *ctx) {
+    if (!ctx) return EXG_ERR_ARG;
+    EXG_TRY(ctx, launch_node_reset(ctx->c));
+    return EXG_OK;
+}
+
+int exg_p2g_momentum(exg_ctx *ctx, int update_mass, int update_vel, int update_forces) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (c.np == 0) return fail(ctx, EXG_ERR_NOT_READY, "no particles");
+    EXG_TRY(ctx, {
+        int flags = (update_mass ? PF_MASS : 0) | (update_vel ? PF_VEL : 0) | (update_forces ? PF_FORCE : 0);
+        EXG_CUDA_OK(cudaMemsetAsync(&c.ctl->maxppc, 0, sizeof(int), c.stream));
+        do_sort(c, false);
+        launch_reset_accum(c, c.bounds2, c.dtmin2);
+        DISPATCH(launch_state_reduce, c, c.bounds2, c.dtmin2);
+        launch_scales_from(c, c.bounds2);
+        if (flags) {
+            DISPATCH(launch_p2g, c, flags);
+            DISPATCH(launch_nodes, c, NM_MERGE, flags, true);
+        }
+        return status_from_ctl(c);
+    });
+}
+
+int exg_backup_current_velocity(exg_ctx *ctx) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, DISPATCH(launch_node_backup, c));
+    return EXG_OK;
+}
+
+int exg_nodal_time_update_momentum(exg_ctx *ctx, double dt) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, DISPATCH(launch_node_time_update, c, dt));
+    return EXG_OK;
+}
+
+int exg_apply_nodal_bcs(exg_ctx *ctx, double dt, double time) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    (void)dt;
+    EXG_TRY(ctx, {
+        tabulate_udf(c, time);
+        DISPATCH(launch_node_bcs, c);
+        return status_from_ctl(c);
+    });
+}
+
+int exg_g2p_momentum(exg_ctx *ctx, int update_vel, int update_strainrate, double dt) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        DISPATCH(launch_g2p_simple, c, update_vel, update_strainrate, dt);
+        c.reduce_stale = true;
+    });
+    return EXG_OK;
+}
+
+int exg_update_mp_positions(exg_ctx *ctx, double dt) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        DISPATCH(launch_move, c, dt);
+        c.parts_sorted = false;
+        c.reduce_stale = true;
+        return status_from_ctl(c);
+    });
+}
+
+int exg_update_mp_volume(exg_ctx *ctx) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        DISPATCH(launch_volume, c);
+        c.reduce_stale = true;
+    });
+    return EXG_OK;
+}
+
+int exg_calculate_mp_stress_strain(exg_ctx *ctx, double time, double dt) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        DISPATCH(launch_stress, c, time, dt);
+        c.reduce_stale = true;
+    });
+    return EXG_OK;
+}
+
+int exg_init_internal_forces(exg_ctx *ctx) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (c.specs.use_temp) return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+    int rc = exg_p2g_momentum(ctx, 1, 1, 1);
+    if (rc) return rc;
+    rc = exg_backup_current_velocity(ctx);
+    if (rc) return rc;
+    rc = exg_g2p_momentum(ctx, 0, 1, 0.0);
+    if (rc) return rc;
+    // apply_constitutive_model(dt = 0, applied_strainrate) (mpm_init.cpp:398)
+    EXG_TRY(ctx, {
+        if (c.np)
+            fp64(c) ? launch_stress_fp64(c, -INFINITY, 0.0) : launch_stress_fp32(c, -INFINITY, 0.0);
+        c.reduce_stale = true;
+        sync(c);
+    });
+    return EXG_OK;
+}
+
+int exg_p2g_temperature(exg_ctx *ctx, int, int, int) {
+    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+}
+int exg_backup_current_temperature(exg_ctx *ctx) {
+    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+}
+int exg_nodal_time_update_temperature(exg_ctx *ctx, double) {
+    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+}
+int exg_apply_nodal_bcs_temperature(exg_ctx *ctx, double, double, int) {
+    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+}
+int exg_store_delta_temperature(exg_ctx *ctx) {
+    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+}
+int exg_g2p_temperature(exg_ctx *ctx, int, int) {
+    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+}
+
+// ------------------------------------------------------------ fused step
+int exg_step(exg_ctx *ctx, int nsteps) {
+    if (!ctx || nsteps < 0) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (c.np == 0) return fail(ctx, EXG_ERR_NOT_READY, "no particles");
+    if (c.specs.use_temp) return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+    EXG_TRY(ctx, {
+        if (c.reduce_stale) do_reduce(c);
+        const bool host_dep = has_udf(c);
+        const bool use_graph = !host_dep && !c.timing && std::getenv("EXG_NO_GRAPH") == nullptr;
+        for (int s = 0; s < nsteps; ++s) {
+            if (host_dep) {
+                // UDF wall tables depend on the step's start time: tabulate on
+                // the host before the step's kernels.
+                ctl_pull(c);
+                tabulate_udf(c, c.ctl_host->time);
+            }
+            if (use_graph) {
+                cudaGraphExec_t &g = c.gexec[c.orient];
+                if (!g) {
+                    if (!c.warm[c.orient]) {
+                        // first step of each orientation runs eagerly (kernel
+                        // attributes, occupancy queries), later ones replay
+                        enqueue_step(c);
+                        c.warm[c.orient] = true;
+                        swap_parts(c);
+                        continue;
+                    }
+                    cudaGraph_t graph = nullptr;
+                    EXG_CUDA_OK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+                    enqueue_step(c);
+                    EXG_CUDA_OK(cudaStreamEndCapture(c.stream, &graph));
+                    EXG_CUDA_OK(cudaGraphInstantiate(&g, graph, 0));
+                    cudaGraphDestroy(graph);
+                }
+                EXG_CUDA_OK(cudaGraphLaunch(g, c.stream));
+                swap_parts(c);
+            } else {
+                enqueue_step(c);
+                swap_parts(c);
+                if (c.timing) {
+                    sync(c);
+                    float ms[4];
+                    for (int k = 0; k < 4; ++k) EXG_CUDA_OK(cudaEventElapsedTime(&ms[k], c.ev[k], c.ev[k + 1]));
+                    for (int k = 0; k < 4; ++k) c.stage_ms[k] += ms[k];
+                    c.stage_ms[4] += 1.0;
+                }
+            }
+        }
+        c.parts_sorted = false;
+        int rc = status_from_ctl(c);
+        c.host_time = c.ctl_host->time;
+        c.host_dt = c.ctl_host->dt;
+        c.host_steps = c.ctl_host->steps;
+        return rc;
+    });
+}
+
+int exg_get_time(exg_ctx *ctx, double *time, double *last_dt, int64_t *steps) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        ctl_pull(c);
+        if (time) *time = c.ctl_host->time;
+        if (last_dt) *last_dt = c.ctl_host->dt;
+        if (steps) *steps = c.ctl_host->steps;
+    });
+    return EXG_OK;
+}
+
+int exg_set_time(exg_ctx *ctx, double time, int64_t steps) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        ctl_pull(c);
+        c.ctl_host->time = time;
+        c.ctl_host->steps = steps;
+        EXG_CUDA_OK(cudaMemcpyAsync(&c.ctl->time, &c.ctl_host->time, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        EXG_CUDA_OK(
+            cudaMemcpyAsync(&c.ctl->steps, &c.ctl_host->steps, sizeof(long long), cudaMemcpyHostToDevice, c.stream));
+        sync(c);
+    });
+    return EXG_OK;
+}
+
+int exg_diagnostics(exg_ctx *ctx, exg_diag *out) {
+    if (!ctx || !out) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        const long long nb = (std::max<long long>(c.np, 1) + 255) / 256;
+        if (!c.diag_dev || (long long)c.staging_cap < 0) c.diag_dev = dalloc<double>(32 + 16 * nb);
+        static long long diag_cap = 0;
+        if (nb > diag_cap) {
+            cudaFree(c.diag_dev);
+            c.diag_dev = dalloc<double>(32 + 16 * nb);
+            diag_cap = nb;
+        }
+        DISPATCH(launch_diag, c, c.diag_dev);
+        double h[16];
+        EXG_CUDA_OK(cudaMemcpyAsync(h, c.diag_dev, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+        sync(c);
+        std::memset(out, 0, sizeof(*out));
+        out->tke = h[0];
+        out->tse = h[1];
+        out->mass = h[2];
+        for (int d = 0; d < 3; ++d) {
+            out->momentum[d] = h[3 + d];
+            out->mwa_vel[d] = h[3 + d] / h[2];
+            out->minpos[d] = h[9 + d];
+            out->maxpos[d] = h[12 + d];
+        }
+        out->mwa_velmag = h[6] / h[2];
+        out->np = (int64_t)h[15];
+    });
+    return EXG_OK;
+}
+
+int exg_sort_keys(exg_ctx *ctx, uint32_t *keys, int32_t *perm) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        EXG_CUDA_OK(cudaMemsetAsync(&c.ctl->lost, 0, sizeof(unsigned long long), c.stream));
+        do_sort(c, false);
+        ctl_pull(c);
+        const long long n = c.np;
+        std::vector<uint32_t> k(n);
+        EXG_CUDA_OK(cudaMemcpy(k.data(), c.sb.key, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+        if (keys) std::copy(k.begin(), k.end(), keys);
+        if (perm) {
+            const long long ns = c.ctl_host->n_sorted;
+            EXG_CUDA_OK(cudaMemcpy(perm, c.sb.perm, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost));
+            long long q = ns;
+            for (long long i = 0; i < n; ++i)
+                if (k[i] == 0xFFFFFFFFu) perm[q++] = (int32_t)i;
+        }
+    });
+    return EXG_OK;
+}
+
+int exg_tile_size(exg_ctx *ctx, int *tile) {
+    if (!ctx || !tile) return EXG_ERR_ARG;
+    *tile = ctx->c.P.T;
+    return EXG_OK;
+}
+
+int exg_set_stage_timing(exg_ctx *ctx, int on) {
+    if (!ctx) return EXG_ERR_ARG;
+    ctx->c.timing = on != 0;
+    for (double &v : ctx->c.stage_ms) v = 0.0;
+    return EXG_OK;
+}
+
+int exg_last_step_timing(exg_ctx *ctx, double *ms5) {
+    if (!ctx || !ms5) return EXG_ERR_ARG;
+    const double n = ctx->c.stage_ms[4] > 0 ? ctx->c.stage_ms[4] : 1.0;
+    for (int k = 0; k < 4; ++k) ms5[k] = ctx->c.stage_ms[k] / n;
+    ms5[4] = ctx->c.stage_ms[4];
+    return EXG_OK;
+}
+
+int exg_get_stream(exg_ctx *ctx, void **stream) {
+    if (!ctx || !stream) return EXG_ERR_ARG;
+    *stream = (void *)ctx->c.stream;
+    return EXG_OK;
+}
+
+}  // extern "C"

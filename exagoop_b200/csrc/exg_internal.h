@@ -1,0 +1,129 @@
+// exg_internal.h -- host-side context of the B200 MPM step and the kernel
+// launchers shared by the translation units of libexg.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include "exg_common.cuh"
+
+namespace exg {
+
+enum P2GFlags { PF_MASS = 1, PF_VEL = 2, PF_FORCE = 4, PF_TEMP = 8, PF_SRC = 16 };
+// Nodal kernel modes.
+enum NodeMode {
+    NM_MERGE = 0,      // merge P2G partials into the dense arrays + normalise (P2G_Momentum)
+    NM_FUSED = 1,      // merge + backup + time update + BCs + store delta (one USL step)
+    NM_MUSL2 = 2,      // merge momentum, normalise with the stored mass, BCs, store delta (MUSL pass 2)
+};
+// Fused G2P modes.
+enum G2PMode {
+    GM_FULL = 0,       // G2P vel + strain rate + F, move, volume, stress, reductions (USL)
+    GM_VEL = 1,        // G2P vel only (MUSL pass 1)
+    GM_STRAIN = 2,     // G2P strain rate + F, move, volume, stress, reductions (MUSL pass 2)
+};
+
+struct SortBufs {
+    uint32_t *key = nullptr;
+    int32_t *perm = nullptr;
+    int32_t *bucket = nullptr;
+    int *tile_count = nullptr;   // [ntiles]
+    int *tile_fill = nullptr;    // [ntiles]
+    int *tile_start = nullptr;   // [ntiles]
+    int *active = nullptr;       // [ntiles] active tile ids (ascending)
+    int *slot = nullptr;         // [ntiles] index in active list or -1
+    int *touched = nullptr;      // [ntiles] tiles whose nodes the nodal kernel writes
+    long long *touched_step = nullptr;  // [ntiles] last step the tile was touched
+};
+
+struct Ctx;
+
+// launchers (exg_kernels.cu; _fp64/_fp32 variants come from the two
+// precision builds of that file)
+void upload_tables_fp64();
+void upload_tables_fp32();
+void launch_keys(Ctx &c);
+void launch_sort_rest(Ctx &c, bool touched_list);
+void launch_dt_finalize(Ctx &c, bool reset);
+void launch_reset_accum(Ctx &c, unsigned long long *bounds, unsigned long long *dtmin);
+void launch_scales_from(Ctx &c, const unsigned long long *bounds);
+void launch_time_advance(Ctx &c);
+void launch_node_reset(Ctx &c);
+#define EXG_DECL_PREC(sfx)                                                      \
+    void launch_state_reduce##sfx(Ctx &c, unsigned long long *bounds, unsigned long long *dtmin); \
+    void launch_p2g##sfx(Ctx &c, int flags);                                     \
+    void launch_nodes##sfx(Ctx &c, int mode, int flags, bool all_tiles);         \
+    void launch_g2p_fused##sfx(Ctx &c, int mode);                                \
+    void launch_copy_lost##sfx(Ctx &c);                                          \
+    void launch_g2p_simple##sfx(Ctx &c, int uv, int us, double dt);              \
+    void launch_node_backup##sfx(Ctx &c);                                        \
+    void launch_node_time_update##sfx(Ctx &c, double dt);                        \
+    void launch_node_bcs##sfx(Ctx &c);                                           \
+    void launch_move##sfx(Ctx &c, double dt);                                    \
+    void launch_volume##sfx(Ctx &c);                                             \
+    void launch_stress##sfx(Ctx &c, double time, double dt);                     \
+    void launch_diag##sfx(Ctx &c, double *out_dev);
+EXG_DECL_PREC(_fp64)
+EXG_DECL_PREC(_fp32)
+
+struct Ctx {
+    exg_specs specs;
+    Params P;
+    int precision;  // EXG_PREC_*
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // particles (double buffered: a = current, b = reorder target)
+    long long np = 0, cap = 0;
+    void *pa = nullptr, *pb = nullptr;  // Parts<R>* host-side copies
+    std::vector<void *> allocs_a, allocs_b;
+    // material table
+    Material *mat_dev = nullptr;
+    std::vector<Material> mats;
+    // nodes
+    void *nodes = nullptr;             // Nodes<R> host copy (device pointers)
+    std::vector<void *> node_allocs;
+    double *ls[kMaxBodies] = {};       // nodal level sets (FP64)
+    // UDF wall tables [lo/hi][dir] (FP64)
+    double *udf_tab[2][3] = {};
+    std::vector<double> udf_host[2][3];
+    // sort
+    SortBufs sb;
+    long long *staging = nullptr;      // P2G partial node blocks (fixed point)
+    size_t staging_cap = 0;            // in tiles
+    int nch = 7;
+    // control block
+    Ctl *ctl = nullptr;                // device
+    Ctl *ctl_host = nullptr;           // pinned mirror
+    unsigned long long *bounds_cur = nullptr;  // device: bounds used by this step's P2G
+    unsigned long long *bounds2 = nullptr;     // device: bounds of the MUSL re-projection
+    unsigned long long *dtmin2 = nullptr;      // device: scratch min
+    double *diag_dev = nullptr;
+    // state
+    bool parts_sorted = false;         // perm valid for the current storage order
+    bool reduce_stale = true;          // ctl reductions need recomputing
+    double host_time = 0.0, host_dt = 0.0;
+    long long host_steps = 0;
+    // CUDA graph of one fused step
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // one per buffer orientation
+    bool warm[2] = {false, false};
+    int orient = 0;                                 // 1 when pa holds the second allocation
+    cudaEvent_t ev[6] = {};
+    double stage_ms[5] = {};
+    bool timing = false;
+
+    template <class R>
+    Parts<R> &A() { return *reinterpret_cast<Parts<R> *>(pa); }
+    template <class R>
+    Parts<R> &Bp() { return *reinterpret_cast<Parts<R> *>(pb); }
+    template <class R>
+    Nodes<R> &N() { return *reinterpret_cast<Nodes<R> *>(nodes); }
+};
+
+#define EXG_CUDA_OK(call)                                                              \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) throw std::runtime_error(std::string(#call) + ": " +    \
+                                                        cudaGetErrorString(e_));       \
+    } while (0)
+
+}  // namespace exg

@@ -1,0 +1,1696 @@
+// exg_kernels.cu -- CUDA kernels of the B200 MPM step (sm_100a).
+//
+// One step is four kernel groups:
+//   K1 cell-key binning sort  (replaces AMReX Redistribute)
+//   K2 tile P2G               (deposit_onto_grid_momentum, deterministic fixed-point scatter)
+//   K3 nodal update           (normalise, backup, time update, wall/UDF/level-set BCs, store delta)
+//   K4 fused G2P              (interpolate_from_grid + moveParticles + updateVolume + apply_constitutive_model)
+// plus single-thread bookkeeping kernels that keep dt, time and the
+// reductions on the device so that a whole step can be replayed from a CUDA
+// graph without a host round trip.
+#include <algorithm>
+#include <cstdio>
+#include <stdexcept>
+#include "exg_internal.h"
+
+// This file is compiled twice: with EXG_R_FP64 (FP64 kernels plus the
+// precision-independent ones) and without (the FP32 kernels of the mixed
+// path), so the two halves build in parallel.
+#if defined(EXG_R_FP64)
+#define EXG_R double
+#define EXG_SFX(name) name##_fp64
+#else
+#define EXG_R float
+#define EXG_SFX(name) name##_fp32
+#endif
+
+namespace exg {
+
+namespace {
+__constant__ SplineTables c_tables;
+}
+
+void EXG_SFX(upload_tables)() {
+    // Coefficient tables of Source/interpolants.H:32-183 (see exg_common.cuh).
+    static const SplineTables t = {
+        // cubic value
+        {{{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}},
+         {{kOneBySix, 1.0, 2.0, kFourByThree}, {-kOneBySix, 0.0, 1.0, 1.0}, {kOneBySix, 0.0, -1.0, 1.0},
+          {-kOneBySix, 1.0, -2.0, kFourByThree}},
+         {{0.0, 0.0, 0.0, 0.0}, {-kOneByThree, -1.0, 0.0, kTwoByThree}, {0.5, -1.0, 0.0, kTwoByThree},
+          {-kOneBySix, 1.0, -2.0, kFourByThree}},
+         {{kOneBySix, 1.0, 2.0, kFourByThree}, {-0.5, -1.0, 0.0, kTwoByThree}, {0.5, -1.0, 0.0, kTwoByThree},
+          {-kOneBySix, 1.0, -2.0, kFourByThree}},
+         {{kOneBySix, 1.0, 2.0, kFourByThree}, {-0.5, -1.0, 0.0, kTwoByThree}, {kOneByThree, -1.0, 0.0, kTwoByThree},
+          {0.0, 0.0, 0.0, 0.0}}},
+        // cubic derivative
+        {{{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},
+         {{0.5, 2.0, 2.0}, {-0.5, 0.0, 1.0}, {0.5, 0.0, -1.0}, {-0.5, 2.0, -2.0}},
+         {{0, 0, 0}, {-1.0, -2.0, 0.0}, {1.5, -2.0, 0.0}, {-0.5, 2.0, -2.0}},
+         {{0.5, 2.0, 2.0}, {-1.5, -2.0, 0.0}, {1.5, -2.0, 0.0}, {-0.5, 2.0, -2.0}},
+         {{0.5, 2.0, 2.0}, {-1.5, -2.0, 0.0}, {1.0, -2.0, 0.0}, {0, 0, 0}}},
+        // quadratic value
+        {{{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},
+         {{kTwoByThree, 2.0, 1.5}, {-kFourByThree, 0.0, 1.0}, {-kFourByThree, 0.0, 1.0}, {kTwoByThree, -2.0, 1.5}},
+         {{4.0 / 3.0, 8.0 / 3.0, 4.0 / 3.0}, {-7.0 / 6.0, 1.0 / 6.0, 17.0 / 24.0}, {0.5, -1.5, 1.125}, {0, 0, 0}},
+         {{0.5, 1.5, 1.125}, {-1.0, 0.0, 0.75}, {0.5, -1.5, 1.125}, {0, 0, 0}},
+         {{0.5, 1.5, 1.125}, {-7.0 / 6.0, -1.0 / 6.0, 17.0 / 24.0}, {4.0 / 3.0, -8.0 / 3.0, 4.0 / 3.0}, {0, 0, 0}}},
+        // quadratic derivative
+        {{{0, 0}, {0, 0}, {0, 0}, {0, 0}},
+         {{4.0 / 3.0, 2.0}, {-8.0 / 3.0, 0.0}, {-8.0 / 3.0, 0.0}, {4.0 / 3.0, -2.0}},
+         {{8.0 / 3.0, 8.0 / 3.0}, {-14.0 / 6.0, 1.0 / 6.0}, {1.0, -1.5}, {0, 0}},
+         {{2.0 / 2.0, 3.0 / 2.0}, {-2.0, 0.0}, {2.0 / 2.0, -3.0 / 2.0}, {0, 0}},
+         {{1.0, 1.5}, {-14.0 / 6.0, -1.0 / 6.0}, {8.0 / 3.0, -8.0 / 3.0}, {0, 0}}},
+        // quadratic half-interval map
+        {{-1, -1, -1, -1, -1, -1}, {0, 0, 1, 2, 3, 3}, {0, 1, 1, 2, 2, -1}, {0, 0, 1, 1, 2, 2}, {0, 0, 1, 1, 2, -1}}};
+    EXG_CUDA_OK(cudaMemcpyToSymbol(c_tables, &t, sizeof(t)));
+}
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ void load_tables(SplineTables *dst) {
+    const int n = sizeof(SplineTables) / 4;
+    const int *src = reinterpret_cast<const int *>(&c_tables);
+    int *d = reinterpret_cast<int *>(dst);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = src[i];
+}
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+    }
+    return v;
+}
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one int per thread (blockDim.x <= 1024).
+[[maybe_unused]] __device__ int block_exclusive_scan(int v, int *total, int *sh /* >= 33 ints */) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int n = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += n;
+    }
+    if (lane == 31) sh[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        int s = lane < nw ? sh[lane] : 0;
+        int si = s;
+        for (int o = 1; o < 32; o <<= 1) {
+            int n = __shfl_up_sync(0xffffffffu, si, o);
+            if (lane >= o) si += n;
+        }
+        sh[lane] = si - s;
+        if (lane == 31) sh[32] = si;
+    }
+    __syncthreads();
+    int res = inc - v + sh[wid];
+    *total = sh[32];
+    __syncthreads();
+    return res;
+}
+
+__device__ __forceinline__ void tile_coords(const Params &P, int t, int tc[3]) {
+    tc[0] = t % P.ntile[0];
+    int r = t / P.ntile[0];
+    tc[1] = r % P.ntile[1];
+    tc[2] = r / P.ntile[1];
+}
+
+#if defined(EXG_R_FP64)
+// ---------------------------------------------------------------- K1 sort
+// Cell key per particle, with the periodic wrap of Redistribute.  Keys are
+// tile-major: (tile index << 3 log2 T) | (cell inside tile), so one tile's
+// particles are contiguous after a stable sort by key.
+__global__ void k_keys(Params P, double *x0, double *x1, double *x2, long long n, uint32_t *key, int *tile_count,
+                       Ctl *ctl, int wrap) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int t = -1;
+    if (i < n) {
+        double x[3] = {x0[i], x1[i], x2[i]};
+        if (wrap) {
+            double *xs[3] = {x0, x1, x2};
+            for (int d = 0; d < 3; ++d) {
+                if (!P.periodic[d]) continue;
+                double L = P.phi[d] - P.plo[d];
+                double y = x[d];
+                if (y >= P.phi[d])
+                    y -= L;
+                else if (y < P.plo[d])
+                    y += L;
+                if (y != x[d]) {
+                    x[d] = y;
+                    xs[d][i] = y;
+                }
+            }
+        }
+        int iv[3];
+        cell_of(P, x, iv);
+        bool in = true;
+        for (int d = 0; d < 3; ++d) in = in && iv[d] >= 0 && iv[d] < P.nc[d];
+        if (!in) {
+            key[i] = 0xFFFFFFFFu;
+            atomicAdd(&ctl->lost, 1ull);
+        } else {
+            const int ts = P.tshift, m = P.T - 1;
+            t = ((iv[2] >> ts) * P.ntile[1] + (iv[1] >> ts)) * P.ntile[0] + (iv[0] >> ts);
+            uint32_t loc = (uint32_t)((((iv[2] & m) << ts) | (iv[1] & m)) << ts | (iv[0] & m));
+            key[i] = ((uint32_t)t << (3 * ts)) | loc;
+        }
+    }
+    // warp-aggregated tile histogram (particles arrive nearly sorted)
+    unsigned act = __ballot_sync(0xffffffffu, t >= 0);
+    if (t >= 0) {
+        unsigned peers = __match_any_sync(act, t);
+        int leader = __ffs(peers) - 1;
+        if ((int)(threadIdx.x & 31) == leader) atomicAdd(&tile_count[t], __popc(peers));
+    }
+}
+
+// Exclusive scan of tile counts (one block): tile starts, the ascending
+// list of non-empty tiles and each tile's slot in it.
+__global__ void k_tile_scan(int ntiles, const int *count, int *start, int *active, int *slot, Ctl *ctl) {
+    __shared__ int sh[34];
+    __shared__ int carry, acarry;
+    if (threadIdx.x == 0) {
+        carry = 0;
+        acarry = 0;
+    }
+    __syncthreads();
+    for (int base = 0; base < ntiles; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        int c = i < ntiles ? count[i] : 0;
+        int a = c > 0;
+        int tc, ta;
+        int ec = block_exclusive_scan(c, &tc, sh);
+        int ea = block_exclusive_scan(a, &ta, sh);
+        if (i < ntiles) {
+            start[i] = carry + ec;
+            if (a) {
+                active[acarry + ea] = i;
+                slot[i] = acarry + ea;
+            } else {
+                slot[i] = -1;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            carry += tc;
+            acarry += ta;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        ctl->n_active_tiles = acarry;
+        ctl->n_sorted = carry;
+    }
+}
+
+// Tiles whose owned nodes the nodal kernel writes this step: tiles next to
+// a non-empty tile (they receive P2G halo contributions), plus tiles written
+// in the previous step (their nodes return to zero, as Reset_Nodaldata_to_Zero
+// leaves them).
+__global__ void k_touched(Params P, const int *count, int *touched, long long *touched_step, Ctl *ctl) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.ntiles) return;
+    int tc[3];
+    tile_coords(P, t, tc);
+    bool now = false;
+    for (int dz = -1; dz <= 1 && !now; ++dz)
+        for (int dy = -1; dy <= 1 && !now; ++dy)
+            for (int dx = -1; dx <= 1 && !now; ++dx) {
+                int s[3] = {tc[0] + dx, tc[1] + dy, tc[2] + dz};
+                bool ok = true;
+                for (int d = 0; d < 3; ++d) {
+                    if (s[d] < 0 || s[d] >= P.ntile[d]) {
+                        if (P.periodic[d])
+                            s[d] = (s[d] + P.ntile[d]) % P.ntile[d];
+                        else
+                            ok = false;
+                    }
+                }
+                if (ok && count[(s[2] * P.ntile[1] + s[1]) * P.ntile[0] + s[0]] > 0) now = true;
+            }
+    long long cur = ctl->steps;
+    long long prev = touched_step[t];
+    if (now || prev == cur - 1) {
+        int idx = atomicAdd(&ctl->n_touched_tiles, 1);
+        touched[idx] = t;
+    }
+    if (now) touched_step[t] = cur;
+}
+
+__global__ void k_scatter(long long n, const uint32_t *key, int tshift3, const int *start, int *fill, int32_t *bucket) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int t = -1;
+    if (i < n) {
+        uint32_t k = key[i];
+        if (k != 0xFFFFFFFFu) t = (int)(k >> tshift3);
+    }
+    unsigned act = __ballot_sync(0xffffffffu, t >= 0);
+    if (t >= 0) {
+        unsigned peers = __match_any_sync(act, t);
+        int lane = threadIdx.x & 31;
+        int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&fill[t], __popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        int rank = __popc(peers & ((1u << lane) - 1u));
+        bucket[start[t] + base + rank] = (int32_t)i;
+    }
+}
+
+// Per-tile stable ordering: particles of one tile sorted by (cell, storage
+// index), which equals a stable sort of the whole array by key.
+constexpr int kSortCap = 12288;
+__global__ void __launch_bounds__(kThreads) k_tile_sort(const int *active, const int *start, const int *count,
+                                                        const uint32_t *key, const int32_t *bucket, int32_t *scratch,
+                                                        int32_t *perm, int ncell, Ctl *ctl) {
+    extern __shared__ int sm[];
+    int *cnt = sm, *cst = sm + ncell, *fil = sm + 2 * ncell, *ent_s = sm + 3 * ncell;
+    __shared__ int sh[34];
+    __shared__ int smax;
+    const uint32_t cm = (uint32_t)ncell - 1u;
+    const int nitems = ctl->n_active_tiles;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+        const int t = active[w];
+        const int s0 = start[t], n = count[t];
+        int32_t *ent = (n <= kSortCap) ? ent_s : scratch + s0;
+        for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
+            cnt[c] = 0;
+            fil[c] = 0;
+        }
+        if (threadIdx.x == 0) smax = 0;
+        __syncthreads();
+        for (int e = threadIdx.x; e < n; e += blockDim.x) atomicAdd(&cnt[key[bucket[s0 + e]] & cm], 1);
+        __syncthreads();
+        // exclusive scan of the per-cell counts
+        int carry = 0;
+        for (int base = 0; base < ncell; base += blockDim.x) {
+            int c = base + threadIdx.x;
+            int v = c < ncell ? cnt[c] : 0;
+            int tot;
+            int ex = block_exclusive_scan(v, &tot, sh);
+            if (c < ncell) {
+                cst[c] = carry + ex;
+                if (v > 0) atomicMax(&smax, v);
+            }
+            carry += tot;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            int i = bucket[s0 + e];
+            int c = key[i] & cm;
+            ent[cst[c] + atomicAdd(&fil[c], 1)] = i;
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < n; q += blockDim.x) {
+            int i = ent[q];
+            int c = key[i] & cm;
+            int b = cst[c], e = b + cnt[c];
+            int rank = 0;
+            for (int r = b; r < e; ++r) rank += (ent[r] < i);
+            perm[s0 + b + rank] = i;
+        }
+        if (threadIdx.x == 0) atomicMax(&ctl->maxppc, smax);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- bookkeeping
+// Start of step: dt from the last particle reduction (Calculate_time_step,
+// mpm_particle_timestep.cpp:38-111), current bounds, accumulators reset.
+__global__ void k_dt_finalize(Params P, Ctl *ctl, int reset) {
+    double dtmin = bitsd(ctl->dtmin_bits);
+    double dt;
+    if (P.fixed_dt)
+        dt = P.timestep;
+    else {
+        dt = P.cfl * dtmin;
+        dt = fmax(fmin(dt, P.dt_max), P.dt_min);
+    }
+    ctl->dt = dt;
+    if (reset) {
+        ctl->dtmin_bits = dbits(1.7976931348623157e308);
+        for (int c = 0; c < CH_ALL; ++c) ctl->bound_bits[c] = 0ull;
+        ctl->lost = 0ull;
+        ctl->lost_fill = 0ull;
+        ctl->maxppc = 0;
+        ctl->n_touched_tiles = 0;
+    }
+}
+
+// Fixed-point scales: a channel's node sum is bounded by
+// (particles per cell) x (stencil cells) x (largest per-particle term);
+// the scale 2^e keeps that bound below 2^61.
+__global__ void k_scales(Ctl *ctl, int stencil_cells, const unsigned long long *bounds) {
+    int c = threadIdx.x;
+    if (c >= CH_ALL) return;
+    double b = bitsd(bounds[c]);
+    double S = b * (double)(ctl->maxppc > 0 ? ctl->maxppc : 1) * (double)stencil_cells * 2.0;
+    double sc = 1.0;
+    if (S > 0.0 && S < 1e300) {
+        int ex;
+        frexp(S, &ex);  // S < 2^ex
+        sc = ldexp(1.0, 61 - ex);
+    }
+    ctl->scale[c] = sc;
+    ctl->inv_scale[c] = 1.0 / sc;
+}
+
+__global__ void k_time_advance(Ctl *ctl) {
+    ctl->time += ctl->dt;
+    ctl->steps += 1;
+}
+
+#endif  // EXG_R_FP64
+
+// Reductions over particles that the next step needs before it can start:
+// the CFL minimum and the per-channel P2G bounds.
+template <class R>
+__device__ __forceinline__ void particle_bounds(const Params &P, const Material &mt, double m, const double v[3],
+                                                double vol, const double sig[6], double rho, double cp, double T,
+                                                double kc, const double q[3], double Q, double b[CH_ALL],
+                                                double &dtp) {
+    b[CH_M] = fabs(m);
+    for (int d = 0; d < 3; ++d) b[CH_P + d] = fabs(m * v[d]);
+    const int rowi[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    for (int d = 0; d < 3; ++d) {
+        double s = 0.0;
+        for (int j = 0; j < 3; ++j) s += fabs(sig[rowi[d][j]]) * 2.0 * P.dxi[j];
+        b[CH_F + d] = fabs(m * P.gravity[d]) + (P.external_loads ? fabs(P.extforce[d]) : 0.0) + fabs(vol) * s;
+    }
+    b[CH_MC] = fabs(m * cp);
+    b[CH_MCT] = fabs(m * cp * T);
+    b[CH_MK] = fabs(m * kc);
+    double sq = 0.0;
+    for (int d = 0; d < 3; ++d) sq += fabs(q[d]) * 2.0 * P.dxi[d];
+    b[CH_SRC] = fabs(vol) * sq + fabs(vol * Q);
+    // Calculate_time_step, mpm_particle_timestep.cpp:55-100
+    double Cs;
+    if (mt.model == 1)
+        Cs = sqrt(mt.K / rho);
+    else {
+        double lambda = mt.E * mt.nu / ((1 + mt.nu) * (1 - 2.0 * mt.nu));
+        double mu = mt.E / (2.0 * (1 + mt.nu));
+        Cs = sqrt((lambda + 2.0 * mu) / rho);
+    }
+    double vm = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    dtp = P.dxmin / (Cs + vm);
+}
+
+__device__ __forceinline__ void block_reduce_push(unsigned long long *bounds, unsigned long long *dtmin,
+                                                  double b[CH_ALL], double dtp, bool valid) {
+    __shared__ unsigned long long red[CH_ALL + 1][kThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int c = 0; c < CH_ALL; ++c) {
+        unsigned long long u = valid ? dbits(b[c]) : 0ull;
+        u = warp_max_u64(u);
+        if (lane == 0) red[c][wid] = u;
+    }
+    unsigned long long ud = valid ? dbits(dtp) : dbits(1.7976931348623157e308);
+    ud = warp_min_u64(ud);
+    if (lane == 0) red[CH_ALL][wid] = ud;
+    __syncthreads();
+    if (threadIdx.x < CH_ALL) {
+        unsigned long long m = 0ull;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = red[threadIdx.x][w] > m ? red[threadIdx.x][w] : m;
+        if (m) atomicMax(&bounds[threadIdx.x], m);
+    } else if (threadIdx.x == CH_ALL) {
+        unsigned long long m = ~0ull;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = red[CH_ALL][w] < m ? red[CH_ALL][w] : m;
+        atomicMin(dtmin, m);
+    }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kThreads) k_state_reduce(Params P, Parts<R> A, const Material *mats, long long n,
+                                                           unsigned long long *bounds, unsigned long long *dtmin) {
+    long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    bool valid = false;
+    double b[CH_ALL] = {};
+    double dtp = 0.0;
+    if (p < n && A.phase[p] == 0) {
+        double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+        int iv[3];
+        cell_of(P, x, iv);
+        valid = true;
+        for (int d = 0; d < 3; ++d) valid = valid && iv[d] >= 0 && iv[d] < P.nc[d];
+        if (valid) {
+            double v[3] = {(double)A.v[0][p], (double)A.v[1][p], (double)A.v[2][p]};
+            double s[6];
+            for (int c = 0; c < 6; ++c) s[c] = (double)A.sig[c][p];
+            double q[3] = {0, 0, 0}, cp = 0, T = 0, kc = 0, Q = 0;
+            if (P.use_temp) {
+                for (int d = 0; d < 3; ++d) q[d] = (double)A.q[d][p];
+                cp = A.cp[p];
+                T = A.T[p];
+                kc = A.kc[p];
+                Q = A.Q[p];
+            }
+            particle_bounds<R>(P, mats[A.mat[p]], (double)A.mass[p], v, (double)A.vol[p], s, (double)A.rho[p], cp, T,
+                               kc, q, Q, b, dtp);
+        }
+    }
+    block_reduce_push(bounds, dtmin, b, dtp, valid);
+}
+
+#if defined(EXG_R_FP64)
+__global__ void k_reset_accum(unsigned long long *bounds, unsigned long long *dtmin) {
+    if (threadIdx.x < CH_ALL) bounds[threadIdx.x] = 0ull;
+    if (threadIdx.x == 0) *dtmin = dbits(1.7976931348623157e308);
+}
+#endif
+
+// ---------------------------------------------------------------- K2 P2G
+// deposit_onto_grid_momentum (mpm_particle_grid_ops.cpp:405-588) and the
+// thermal deposit (:703-844), one CTA per non-empty tile.  Contributions are
+// converted to 64-bit fixed point with a per-channel power-of-two scale and
+// accumulated with integer shared-memory atomics: integer addition is
+// associative, so node sums do not depend on thread scheduling and the
+// result is identical run to run.  The CTA then stores its whole node block
+// (tile plus halo) as one partial; the nodal kernel adds the <= 8 partials
+// covering each node.
+template <int ORD>
+struct Stc {
+    static constexpr int W = (ORD == 1) ? 2 : 4;
+    static constexpr int LO = (ORD == 1) ? 0 : -1;
+};
+
+__device__ __forceinline__ void fx_add(unsigned long long *a, double v, double sc) {
+    long long q = __double2ll_rn(v * sc);
+    if (q) atomicAdd(a, (unsigned long long)q);
+}
+
+template <class R, int ORD, bool THERM>
+__global__ void __launch_bounds__(kThreads) k_p2g(Params P, Parts<R> A, const int *active, const int *start,
+                                                  const int *count, const int32_t *perm, long long *staging, Ctl *ctl,
+                                                  int flags) {
+    constexpr int W = Stc<ORD>::W, LO = Stc<ORD>::LO;
+    constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
+    const int B = P.B, B3 = B * B * B;
+    load_tables(tab);
+    double sc[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) sc[c] = ctl->scale[c];
+    const int nitems = ctl->n_active_tiles;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) acc[i] = 0ull;
+    __syncthreads();
+    const int t = active[w];
+    int tc[3];
+    tile_coords(P, t, tc);
+    const int org[3] = {tc[0] * P.T, tc[1] * P.T, tc[2] * P.T};
+    const int s0 = start[t], n = count[t];
+    const bool fm = flags & PF_MASS, fv = flags & PF_VEL, ff = flags & PF_FORCE, fT = flags & PF_TEMP,
+               fS = flags & PF_SRC;
+    for (int k = s0 + threadIdx.x; k < s0 + n; k += blockDim.x) {
+        const int p = perm[k];
+        if (A.phase[p] != 0) continue;
+        const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+        int iv[3];
+        cell_of(P, x, iv);
+        AxisW<R, W> ax, ay, az;
+        axis_weights<R, W, LO>(*tab, P, 0, x[0], iv[0], ax);
+        axis_weights<R, W, LO>(*tab, P, 1, x[1], iv[1], ay);
+        axis_weights<R, W, LO>(*tab, P, 2, x[2], iv[2], az);
+        const int lx = iv[0] - org[0], ly = iv[1] - org[1], lz = iv[2] - org[2];
+        const R m = A.mass[p], vol = A.vol[p];
+        R mv[3], mg[3], ext[3], s[6];
+        for (int d = 0; d < 3; ++d) {
+            mv[d] = m * A.v[d][p];
+            mg[d] = m * (R)P.gravity[d];
+        }
+        bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] && x[1] > P.slab_lo[1] &&
+                    x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] && x[2] < P.slab_hi[2];
+        for (int d = 0; d < 3; ++d) ext[d] = slab ? (R)P.extforce[d] : R(0);
+        for (int c = 0; c < 6; ++c) s[c] = A.sig[c][p];
+        R mcp = R(0), mcpT = R(0), mk = R(0), qv[3] = {R(0), R(0), R(0)}, VQ = R(0);
+        if (THERM) {
+            mcp = m * A.cp[p];
+            mcpT = mcp * A.T[p];
+            mk = m * A.kc[p];
+            for (int d = 0; d < 3; ++d) qv[d] = A.q[d][p];
+            VQ = vol * A.Q[p];
+        }
+#pragma unroll
+        for (int sz = 0; sz < W; ++sz) {
+            if (az.w[sz] == R(0) && az.dw[sz] == R(0)) continue;
+#pragma unroll
+            for (int sy = 0; sy < W; ++sy) {
+                if (ay.w[sy] == R(0) && ay.dw[sy] == R(0)) continue;
+                const R wyz = ay.w[sy] * az.w[sz];
+#pragma unroll
+                for (int sx = 0; sx < W; ++sx) {
+                    if (ax.w[sx] == R(0) && ax.dw[sx] == R(0)) continue;
+                    const R N = ax.w[sx] * ay.w[sy] * az.w[sz];
+                    const int idx = ((lz + sz) * B + (ly + sy)) * B + (lx + sx);
+                    if (fm) fx_add(&acc[CH_M * B3 + idx], (double)(m * N), sc[CH_M]);
+                    if (fv)
+                        for (int d = 0; d < 3; ++d) fx_add(&acc[(CH_P + d) * B3 + idx], (double)(mv[d] * N), sc[CH_P + d]);
+                    if (ff || (THERM && fS)) {
+                        const R g[3] = {ax.dw[sx] * ay.w[sy] * az.w[sz], ax.w[sx] * ay.dw[sy] * az.w[sz],
+                                        ax.w[sx] * ay.w[sy] * az.dw[sz]};
+                        if (ff) {
+                            const R tv[3] = {s[0] * g[0] + s[1] * g[1] + s[2] * g[2],
+                                             s[1] * g[0] + s[3] * g[1] + s[4] * g[2],
+                                             s[2] * g[0] + s[4] * g[1] + s[5] * g[2]};
+                            for (int d = 0; d < 3; ++d)
+                                fx_add(&acc[(CH_F + d) * B3 + idx], (double)((mg[d] * N + ext[d] * N) + (-vol * tv[d])),
+                                       sc[CH_F + d]);
+                        }
+                        if (THERM && fS) {
+                            R net = qv[0] * g[0] + qv[1] * g[1] + qv[2] * g[2];
+                            fx_add(&acc[CH_SRC * B3 + idx], (double)(net * vol + VQ * N), sc[CH_SRC]);
+                        }
+                    }
+                    if (THERM && fT) {
+                        fx_add(&acc[CH_MC * B3 + idx], (double)(mcp * N), sc[CH_MC]);
+                        fx_add(&acc[CH_MCT * B3 + idx], (double)(mcpT * N), sc[CH_MCT]);
+                        fx_add(&acc[CH_MK * B3 + idx], (double)(mk * N), sc[CH_MK]);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    long long *dst = staging + (long long)w * NCH * B3;
+    for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) dst[i] = (long long)acc[i];
+    __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- nodal BCs
+// Domain-wall BCs of one node (nodal_bcs, nodal_data_ops.cpp:663-766),
+// UDF walls (apply_udf_nodal_bcs, :1061-1175) and level-set bodies
+// (nodal_levelset_bcs, :129-220).  v is updated in place.
+struct NodeBCArgs {
+    const double *udf[2][3];
+    const double *ls[kMaxBodies];
+};
+
+__device__ __forceinline__ double ls_node_value(const Params &P, const double *phi, int i, int j, int k) {
+    int id[3] = {i, j, k};
+    for (int d = 0; d < 3; ++d) {
+        if (P.periodic[d]) {
+            int n = P.nc[d];
+            id[d] %= n;
+            if (id[d] < 0) id[d] += n;
+        } else if (id[d] < 0 || id[d] > P.nc[d]) {
+            return 1.0;
+        }
+    }
+    return phi[((long long)id[2] * P.nn[1] + id[1]) * P.nn[0] + id[0]];
+}
+
+// get_levelset_value / get_levelset_grad (Source/mpm_eb.H:176-288), lsref 1.
+__device__ void ls_sample(const Params &P, const double *phi, const double x[3], double &val, double g[3]) {
+    int idx[3];
+    for (int d = 0; d < 3; ++d) idx[d] = (int)floor((x[d] - P.plo[d] + kTiny) / P.dx[d]);
+    double dv[3][2], w[3][2];
+    for (int d = 0; d < 3; ++d) {
+        double r = (x[d] - (P.plo[d] + idx[d] * P.dx[d])) / P.dx[d];
+        w[d][0] = 1.0 - r;
+        w[d][1] = r;
+        dv[d][0] = -(1.0 / P.dx[d]);
+        dv[d][1] = 1.0 / P.dx[d];
+    }
+    val = 0.0;
+    g[0] = g[1] = g[2] = 0.0;
+    for (int corner = 0; corner < 8; ++corner) {
+        int o[3], c[3];
+        for (int d = 0; d < 3; ++d) {
+            o[d] = (corner >> d) & 1;
+            c[d] = min(max(idx[d] + o[d], -1), P.nc[d] + 1);
+        }
+        double ph = ls_node_value(P, phi, c[0], c[1], c[2]);
+        double bv = w[0][o[0]] * w[1][o[1]] * w[2][o[2]];
+        val += ph * bv;
+        g[0] += ph * (dv[0][o[0]] * w[1][o[1]] * w[2][o[2]]);
+        g[1] += ph * (w[0][o[0]] * dv[1][o[1]] * w[2][o[2]]);
+        g[2] += ph * (w[0][o[0]] * w[1][o[1]] * dv[2][o[2]]);
+    }
+}
+
+__device__ void node_bcs(const Params &P, const NodeBCArgs &bc, int i, int j, int k, double m, double v[3],
+                         unsigned &status) {
+    const int id[3] = {i, j, k};
+    // domain walls: relvel_in accumulates the wall velocity of each face
+    // the node lies on; relvel_out persists across directions.
+    {
+        double rin[3] = {v[0], v[1], v[2]}, rout[3] = {v[0], v[1], v[2]};
+        for (int dir = 0; dir < 3; ++dir) {
+            const bool lo = id[dir] == 0;
+            const bool hi = !lo && id[dir] == P.nc[dir];
+            if (!lo && !hi) continue;
+            double wv[3];
+            for (int d = 0; d < 3; ++d) {
+                wv[d] = lo ? P.wvel_lo[dir * 3 + d] : P.wvel_hi[dir * 3 + d];
+                rin[d] -= wv[d];
+            }
+            double nd[3] = {0, 0, 0};
+            nd[dir] = lo ? 1.0 : -1.0;
+            if (applybc<double>(rin, rout, lo ? P.wmu_lo[dir] : P.wmu_hi[dir], nd, lo ? P.bclo[dir] : P.bchi[dir]) < 0)
+                status |= ST_BC;
+            for (int c = 0; c < 3; ++c) v[c] = rout[c] + wv[c];
+        }
+    }
+    // UDF wall velocity tables
+    for (int dir = 0; dir < 3; ++dir) {
+        const double *tab = nullptr;
+        int bct = -1;
+        if (id[dir] == 0 && bc.udf[0][dir]) {
+            tab = bc.udf[0][dir];
+            bct = P.bclo[dir];
+        } else if (id[dir] == P.nc[dir] && bc.udf[1][dir]) {
+            tab = bc.udf[1][dir];
+            bct = P.bchi[dir];
+        }
+        if (!tab) continue;
+        const int p0 = (dir == 0) ? 1 : 0, p1 = (dir == 2) ? 1 : 2;
+        const long long f = ((long long)id[p0] * (P.nc[p1] + 1) + id[p1]) * 3;
+        if (bct == EXG_BC_NOSLIP) {
+            for (int c = 0; c < 3; ++c) v[c] = tab[f + c];
+        } else {
+            v[dir] = tab[f + dir];
+        }
+    }
+    // level-set bodies
+    if (P.num_bodies > 0 && m > 0.0) {
+        const double xn[3] = {P.plo[0] + i * P.dx[0], P.plo[1] + j * P.dx[1], P.plo[2] + k * P.dx[2]};
+        for (int b = 0; b < P.num_bodies; ++b) {
+            if (!bc.ls[b]) continue;
+            double lv, nd[3];
+            ls_sample(P, bc.ls[b], xn, lv, nd);
+            if (lv >= 0.0) continue;
+            double gm = sqrt(nd[0] * nd[0] + nd[1] * nd[1] + nd[2] * nd[2]);
+            if (!(gm >= 1.0e-10)) continue;
+            for (int d = 0; d < 3; ++d) nd[d] /= gm;
+            const Body &bd = P.body[b];
+            double rin[3], rout[3];
+            for (int d = 0; d < 3; ++d) {
+                rin[d] = v[d] - bd.wall_vel[d];
+                rout[d] = rin[d];
+            }
+            double veln = rin[0] * nd[0] + rin[1] * nd[1] + rin[2] * nd[2];
+            if (veln > 0.0) continue;
+            if (applybc<double>(rin, rout, bd.wall_mu, nd, bd.mom_bc) < 0) status |= ST_BC;
+            for (int d = 0; d < 3; ++d) v[d] = rout[d] + bd.wall_vel[d];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- K3 nodes
+// One CTA per tile; each thread owns nodes of the tile, adds the fixed-point
+// partials of the <= 8 node blocks covering the node (exact integer sums),
+// converts to FP64 and applies the nodal operations of the mode.
+template <class R, bool THERM>
+__global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeBCArgs bc, const int *tiles,
+                                                    const int *slot, const long long *staging, Ctl *ctl, int mode,
+                                                    int flags) {
+    constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
+    const int B = P.B, B3 = B * B * B;
+    const double dt = ctl->dt;
+    unsigned status = 0;
+    double isc[NCH];
+    for (int c = 0; c < NCH; ++c) isc[c] = ctl->inv_scale[c];
+    const int T = P.T;
+    const int nitems = tiles ? ctl->n_touched_tiles : (int)P.ntiles;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    const int t = tiles ? tiles[w] : w;
+    int tc[3];
+    tile_coords(P, t, tc);
+    for (int ln = threadIdx.x; ln < T * T * T; ln += blockDim.x) {
+        const int l[3] = {ln % T, (ln / T) % T, ln / (T * T)};
+        int nid[3];
+        bool ok = true;
+        for (int d = 0; d < 3; ++d) {
+            nid[d] = tc[d] * T + l[d];
+            const int nown = P.periodic[d] ? P.nc[d] : P.nc[d] + 1;
+            ok = ok && nid[d] < nown;
+        }
+        if (!ok) continue;
+        long long accv[NCH];
+        for (int c = 0; c < NCH; ++c) accv[c] = 0;
+        // candidate source tiles per axis
+        int srct[3][3], srcl[3][3], ns[3];
+        for (int d = 0; d < 3; ++d) {
+            ns[d] = 0;
+            for (int dd = -1; dd <= 1; ++dd) {
+                int s = tc[d] + dd;
+                if (s < 0 || s >= P.ntile[d]) {
+                    if (!P.periodic[d]) continue;
+                    s = (s + P.ntile[d]) % P.ntile[d];
+                }
+                int loc = nid[d] - (s * T - P.hlo);
+                if (P.periodic[d]) {
+                    loc %= P.nc[d];
+                    if (loc < 0) loc += P.nc[d];
+                }
+                if (loc < 0 || loc >= B) continue;
+                srct[d][ns[d]] = s;
+                srcl[d][ns[d]] = loc;
+                ns[d]++;
+            }
+        }
+        for (int a = 0; a < ns[2]; ++a)
+            for (int b2 = 0; b2 < ns[1]; ++b2)
+                for (int c2 = 0; c2 < ns[0]; ++c2) {
+                    const int st = (srct[2][a] * P.ntile[1] + srct[1][b2]) * P.ntile[0] + srct[0][c2];
+                    const int sl = slot[st];
+                    if (sl < 0) continue;
+                    const long long base =
+                        (long long)sl * NCH * B3 + ((long long)srcl[2][a] * B + srcl[1][b2]) * B + srcl[0][c2];
+                    for (int c = 0; c < NCH; ++c) accv[c] += staging[base + (long long)c * B3];
+                }
+        const long long ni = ((long long)nid[2] * P.nn[1] + nid[1]) * P.nn[0] + nid[0];
+        double m = (double)accv[CH_M] * isc[CH_M];
+        double p[3], f[3];
+        for (int d = 0; d < 3; ++d) {
+            p[d] = (double)accv[CH_P + d] * isc[CH_P + d];
+            f[d] = (double)accv[CH_F + d] * isc[CH_F + d];
+        }
+        if (mode == NM_MERGE) {
+            // P2G_Momentum: zero + deposit + normalise (mpm_particle_grid_ops.cpp:368-627)
+            if (flags & PF_MASS)
+                Nd.c[EXG_N_MASS][ni] = (R)m;
+            else
+                m = (double)Nd.c[EXG_N_MASS][ni];
+            if (flags & PF_VEL) {
+                double v[3] = {p[0], p[1], p[2]};
+                if (m > 0.0)
+                    for (int d = 0; d < 3; ++d) v[d] = (m >= P.mass_tol) ? p[d] / m : 0.0;
+                for (int d = 0; d < 3; ++d) Nd.c[EXG_N_VEL + d][ni] = (R)v[d];
+            }
+            if (flags & PF_FORCE)
+                for (int d = 0; d < 3; ++d) Nd.c[EXG_N_FRC + d][ni] = (R)f[d];
+        } else if (mode == NM_FUSED) {
+            double v[3] = {p[0], p[1], p[2]};
+            if (m > 0.0)
+                for (int d = 0; d < 3; ++d) v[d] = (m >= P.mass_tol) ? p[d] / m : 0.0;
+            double vold[3] = {0, 0, 0}, mold = 0.0;
+            if (m > 0.0) {  // backup_current_velocity
+                mold = m;
+                for (int d = 0; d < 3; ++d) vold[d] = v[d];
+            }
+            if (m >= P.mass_tol)  // Nodal_Time_Update_Momentum
+                for (int d = 0; d < 3; ++d) v[d] += f[d] / m * dt;
+            else
+                v[0] = v[1] = v[2] = 0.0;
+            node_bcs(P, bc, nid[0], nid[1], nid[2], m, v, status);
+            double dv[3] = {0, 0, 0};
+            if (m > 0.0)  // store_delta_velocity
+                for (int d = 0; d < 3; ++d) dv[d] = v[d] - vold[d];
+            Nd.c[EXG_N_MASS][ni] = (R)m;
+            Nd.c[EXG_N_MASS_OLD][ni] = (R)mold;
+            for (int d = 0; d < 3; ++d) {
+                Nd.c[EXG_N_VEL + d][ni] = (R)v[d];
+                Nd.c[EXG_N_FRC + d][ni] = (R)f[d];
+                Nd.c[EXG_N_DVEL + d][ni] = (R)dv[d];
+            }
+        } else {  // NM_MUSL2: P2G(0,1,0) + Apply_Nodal_BCs (main.cpp:124-127)
+            m = (double)Nd.c[EXG_N_MASS][ni];
+            double v[3] = {p[0], p[1], p[2]};
+            if (m > 0.0)
+                for (int d = 0; d < 3; ++d) v[d] = (m >= P.mass_tol) ? p[d] / m : 0.0;
+            node_bcs(P, bc, nid[0], nid[1], nid[2], m, v, status);
+            for (int d = 0; d < 3; ++d) {
+                Nd.c[EXG_N_VEL + d][ni] = (R)v[d];
+                if (m > 0.0) Nd.c[EXG_N_DVEL + d][ni] = (R)(v[d] - (double)Nd.c[EXG_N_DVEL + d][ni]);
+            }
+        }
+    }
+    }
+    if (status) atomicOr(&ctl->status, status);
+}
+
+// ---------------------------------------------------------------- K4 G2P
+// Node access for the G2P particle update: a shared-memory node block or the
+// dense global arrays.
+template <class R>
+struct SmemNodes {
+    const R *nb;  // [6][B3]: v(3), dv(3)
+    int B, B3;
+    int org[3];   // node coordinate of block element 0
+    __device__ __forceinline__ R get(int c, int i, int j, int k) const {
+        return nb[c * B3 + ((k - org[2]) * B + (j - org[1])) * B + (i - org[0])];
+    }
+};
+template <class R>
+struct GlobalNodes {
+    const R *v[3];
+    const R *dv[3];
+    Params P;
+    __device__ __forceinline__ R get(int c, int i, int j, int k) const {
+        long long n = node_index(P, i, j, k);
+        if (n < 0) return R(0);
+        return c < 3 ? v[c][n] : dv[c - 3][n];
+    }
+};
+
+// Velocity interpolation weights of scheme `sch` along axis d, as
+// bilin_interp_two / quadratic_interp_two / cubic_interp_two build them
+// (interpolants.H:583-656, 863-1006, 1225-1366): scheme 1 is cell-relative
+// linear on offsets 0,1; schemes 2/3 use that spline along every axis over
+// the axis's compute_bounds range.
+template <class R>
+__device__ __forceinline__ void interp_axis(const SplineTables &t, const Params &P, int sch, int d, double x, int i,
+                                            R w[4]) {
+    int bmin, bmax;
+    stencil_bounds(i, P.nc[d], P.order[d], P.periodic[d], bmin, bmax);
+    for (int s = 0; s < 4; ++s) {
+        const int l = s - 1;
+        R val = R(0);
+        if (sch == 1) {
+            R r = (R)((x - (P.plo[d] + i * P.dx[d])) * P.dxi[d]);
+            val = (l == 0) ? R(1) - r : (l == 1 ? r : R(0));
+        } else if (l >= bmin && l < bmax) {
+            int ty = shape_type(i + l, P.nc[d], P.periodic[d]);
+            R r = (R)((x - (P.plo[d] + (i + l) * P.dx[d])) * P.dxi[d]);
+            R der;
+            spline_eval<R>(t, sch, ty, r, val, der);
+        }
+        w[s] = val;
+    }
+}
+
+// interpolate_from_grid for one particle (mpm_particle_grid_ops.cpp:972-1096).
+template <class R, int ORD, class NodeAcc>
+__device__ __forceinline__ void g2p_particle(const SplineTables &tab, const Params &P, const NodeAcc &na,
+                                             const double x[3], const int iv[3], bool upd_vel, bool upd_sr, R v[3],
+                                             R vp[3], R E[9], R sr[6], double dt) {
+    constexpr int W = Stc<ORD>::W, LO = Stc<ORD>::LO;
+    AxisW<R, W> ax, ay, az;
+    axis_weights<R, W, LO>(tab, P, 0, x[0], iv[0], ax);
+    axis_weights<R, W, LO>(tab, P, 1, x[1], iv[1], ay);
+    axis_weights<R, W, LO>(tab, P, 2, x[2], iv[2], az);
+    R vpic[3] = {R(0), R(0), R(0)}, dpic[3] = {R(0), R(0), R(0)};
+    R gv[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
+    const bool generic = (ORD == 0);
+#pragma unroll
+    for (int sz = 0; sz < W; ++sz) {
+#pragma unroll
+        for (int sy = 0; sy < W; ++sy) {
+#pragma unroll
+            for (int sx = 0; sx < W; ++sx) {
+                const R wx = ax.w[sx], wy = ay.w[sy], wz = az.w[sz];
+                const R dx = ax.dw[sx], dy = ay.dw[sy], dz = az.dw[sz];
+                if (wx == R(0) && dx == R(0)) continue;
+                if (wy == R(0) && dy == R(0)) continue;
+                if (wz == R(0) && dz == R(0)) continue;
+                const int ni = iv[0] + LO + sx, nj = iv[1] + LO + sy, nk = iv[2] + LO + sz;
+                const R nv[3] = {na.get(0, ni, nj, nk), na.get(1, ni, nj, nk), na.get(2, ni, nj, nk)};
+                if (upd_vel && !generic) {
+                    const R N = wx * wy * wz;
+                    for (int d = 0; d < 3; ++d) {
+                        vpic[d] += N * nv[d];
+                        dpic[d] += N * na.get(3 + d, ni, nj, nk);
+                    }
+                }
+                if (upd_sr) {
+                    const R g[3] = {dx * wy * wz, wx * dy * wz, wx * wy * dz};
+                    for (int d1 = 0; d1 < 3; ++d1)
+                        for (int d2 = 0; d2 < 3; ++d2) gv[d1][d2] += nv[d1] * g[d2];
+                }
+            }
+        }
+    }
+    if (upd_vel && generic) {
+        // per-component scheme (order of the velocity component's axis)
+        for (int dim = 0; dim < 3; ++dim) {
+            const int sch = P.order[dim];
+            R wx[4], wy[4], wz[4];
+            interp_axis<R>(tab, P, sch, 0, x[0], iv[0], wx);
+            interp_axis<R>(tab, P, sch, 1, x[1], iv[1], wy);
+            interp_axis<R>(tab, P, sch, 2, x[2], iv[2], wz);
+            for (int sz = 0; sz < 4; ++sz)
+                for (int sy = 0; sy < 4; ++sy)
+                    for (int sx = 0; sx < 4; ++sx) {
+                        const R N = wx[sx] * wy[sy] * wz[sz];
+                        if (N == R(0)) continue;
+                        const int ni = iv[0] - 1 + sx, nj = iv[1] - 1 + sy, nk = iv[2] - 1 + sz;
+                        vpic[dim] += N * na.get(dim, ni, nj, nk);
+                        dpic[dim] += N * na.get(3 + dim, ni, nj, nk);
+                    }
+        }
+    }
+    if (upd_vel) {
+        const R a = (R)P.alpha;
+        for (int d = 0; d < 3; ++d) {
+            vp[d] = vpic[d];
+            v[d] = a * v[d] + a * dpic[d] + (R(1) - a) * vpic[d];
+        }
+    }
+    if (upd_sr) {
+        // get_deformation_gradient_tensor (interpolants.H:1732-1787) on
+        // F = I + E: E' = E + (L dt) + (L dt) E.
+        R nrm = R(0);
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) nrm += gv[a][b] * gv[a][b];
+        if (!(nrm >= R(1.0e10))) {
+            R Ld[3][3], En[9];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) Ld[a][b] = gv[a][b] * (R)dt;
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    R acc = E[a * 3 + b] + Ld[a][b];
+                    for (int c = 0; c < 3; ++c) acc += Ld[a][c] * E[c * 3 + b];
+                    En[a * 3 + b] = acc;
+                }
+            for (int q = 0; q < 9; ++q) E[q] = En[q];
+        }
+        int ind = 0;
+        for (int d1 = 0; d1 < 3; ++d1)
+            for (int d2 = d1; d2 < 3; ++d2) sr[ind++] = R(0.5) * (gv[d1][d2] + gv[d2][d1]);
+    }
+}
+
+// moveParticles for one particle (mpm_particle_timestep.cpp:326-576).
+template <class R>
+__device__ __forceinline__ void move_particle(const Params &P, const NodeBCArgs &bc, int phase, double x[3], R v[3],
+                                              const R vp[3], double dt, unsigned &status) {
+    for (int d = 0; d < 3; ++d) x[d] += (double)vp[d] * dt;
+    double rin[3] = {(double)v[0], (double)v[1], (double)v[2]};
+    double rout[3] = {rin[0], rin[1], rin[2]};
+    if (P.num_bodies > 0 && phase == 0) {
+        int hit = -1;
+        double minphi = kTiny;
+        for (int b = 0; b < P.num_bodies; ++b) {
+            if (!bc.ls[b]) continue;
+            double ph, gg[3];
+            ls_sample(P, bc.ls[b], x, ph, gg);
+            if (ph < minphi) {
+                minphi = ph;
+                hit = b;
+            }
+        }
+        if (hit >= 0) {
+            double ph, nd[3];
+            ls_sample(P, bc.ls[hit], x, ph, nd);
+            double gm = sqrt(nd[0] * nd[0] + nd[1] * nd[1] + nd[2] * nd[2]);
+            for (int d = 0; d < 3; ++d) nd[d] /= (gm + kTiny);
+            int mp = applybc<double>(rin, rout, P.body[hit].wall_mu, nd, P.body[hit].mom_bc);
+            if (mp < 0) status |= ST_BC;
+            if (mp > 0)
+                for (int d = 0; d < 3; ++d) x[d] += 2.0 * fabs(minphi) * nd[d];
+            for (int d = 0; d < 3; ++d) v[d] = (R)rout[d];
+        }
+    }
+    for (int dir = 0; dir < 3; ++dir) {
+        const bool lo = x[dir] < P.plo[dir];
+        const bool hi = !lo && x[dir] > P.phi[dir];
+        if (!lo && !hi) continue;
+        double wv[3];
+        for (int d = 0; d < 3; ++d) wv[d] = lo ? P.wvel_lo[dir * 3 + d] : P.wvel_hi[dir * 3 + d];
+        const double *tab = bc.udf[hi ? 1 : 0][dir];
+        if (tab) {
+            const int p0 = (dir == 0) ? 1 : 0, p1 = (dir == 2) ? 1 : 2;
+            double f0 = (x[p0] - P.plo[p0]) / P.dx[p0], f1 = (x[p1] - P.plo[p1]) / P.dx[p1];
+            f0 = fmax(0.0, fmin((double)P.nc[p0], f0));
+            f1 = fmax(0.0, fmin((double)P.nc[p1], f1));
+            int j0 = (int)f0, j1 = min(j0 + 1, P.nc[p0]);
+            int k0 = (int)f1, k1 = min(k0 + 1, P.nc[p1]);
+            double wx1 = f0 - j0, wx0 = 1.0 - wx1, wy1 = f1 - k0, wy0 = 1.0 - wy1;
+            int n1 = P.nc[p1] + 1;
+            for (int c = 0; c < 3; ++c)
+                wv[c] = wx0 * wy0 * tab[(j0 * n1 + k0) * 3 + c] + wx0 * wy1 * tab[(j0 * n1 + k1) * 3 + c] +
+                        wx1 * wy0 * tab[(j1 * n1 + k0) * 3 + c] + wx1 * wy1 * tab[(j1 * n1 + k1) * 3 + c];
+        }
+        for (int d = 0; d < 3; ++d) rin[d] -= wv[d];
+        double nd[3] = {0, 0, 0};
+        nd[dir] = lo ? 1.0 : -1.0;
+        int mp = applybc<double>(rin, rout, lo ? P.wmu_lo[dir] : P.wmu_hi[dir], nd, lo ? P.bclo[dir] : P.bchi[dir]);
+        if (mp < 0) status |= ST_BC;
+        if (mp > 0) x[dir] = lo ? 2.0 * P.plo[dir] - x[dir] : 2.0 * P.phi[dir] - x[dir];
+        for (int c = 0; c < 3; ++c) v[c] = (R)(rout[c] + wv[c]);
+    }
+}
+
+// updateVolume + apply_constitutive_model for one phase-0 particle
+// (mpm_particle_timestep.cpp:131-182, mpm_particle_container.cpp:43-142).
+// J, the Tait pressure and the density division are FP64.
+template <class R>
+__device__ __forceinline__ void volume_stress(const Params &P, const Material &mt, const R E[9], R vol0, R mass,
+                                              const R sr[6], R eps[6], R sig[6], R &vol, R &rho, R &J, R &pres,
+                                              double dt, double asr, bool do_volume, bool do_stress) {
+    if (do_volume) {
+        double e[9];
+        for (int q = 0; q < 9; ++q) e[q] = (double)E[q];
+        double det = det_IpE(e);
+        double V = (double)vol0 * det;
+        J = (R)det;
+        vol = (R)V;
+        rho = (R)((double)mass / V);
+    }
+    if (do_stress) {
+        for (int d = 0; d < 6; ++d) eps[d] += (R)dt * sr[d];
+        eps[0] += (R)(dt * asr);
+        eps[3] += (R)(dt * asr);
+        eps[5] += (R)(dt * asr);
+        if (mt.model == 0) {
+            linear_elastic<R>(eps, sig, (R)mt.E, (R)mt.nu);
+        } else if (mt.model == 1) {
+            double pj = mt.K * (pow(1.0 / (double)J, mt.gamma) - 1.0);
+            pres = (R)pj;
+            newtonian<R>(sr, sig, (R)mt.mu, (R)pj);
+        }
+    }
+}
+
+template <class R>
+__device__ __forceinline__ bool all_finite(const R *a, int n) {
+    bool ok = true;
+    for (int i = 0; i < n; ++i) ok = ok && isfinite((double)a[i]);
+    return ok;
+}
+
+// Fused K4: one CTA per non-empty tile.  The tile's node block (velocity
+// and delta-velocity, halo included) is staged in shared memory once; each
+// particle of the tile is gathered from storage A through the sort
+// permutation and written to storage B at its sorted position, so the
+// particle arrays are physically re-ordered by cell every step at no extra
+// pass.  GM_VEL updates velocity in place in A instead.
+template <class R, int ORD>
+__global__ void __launch_bounds__(kThreads) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
+                                                        const Material *mats, const int *active, const int *start,
+                                                        const int *count, const int32_t *perm, Ctl *ctl, int mode) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
+    R *nb = reinterpret_cast<R *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
+    const int B = P.B, B3 = B * B * B;
+    load_tables(tab);
+    const double dt = ctl->dt, time = ctl->time;
+    const double asr = (time < P.applied_sr_time) ? P.applied_sr : 0.0;
+    unsigned status = 0;
+    const bool upd_vel = (mode != GM_STRAIN);
+    const int nitems = ctl->n_active_tiles;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    const int t = active[w];
+    int tc[3];
+    tile_coords(P, t, tc);
+    SmemNodes<R> na;
+    na.nb = nb;
+    na.B = B;
+    na.B3 = B3;
+    for (int d = 0; d < 3; ++d) na.org[d] = tc[d] * P.T - P.hlo;
+    for (int idx = threadIdx.x; idx < B3; idx += blockDim.x) {
+        const int bx = idx % B, by = (idx / B) % B, bz = idx / (B * B);
+        const long long ni = node_index(P, na.org[0] + bx, na.org[1] + by, na.org[2] + bz);
+        for (int c = 0; c < 3; ++c) {
+            nb[c * B3 + idx] = ni >= 0 ? Nd.c[EXG_N_VEL + c][ni] : R(0);
+            nb[(3 + c) * B3 + idx] = ni >= 0 ? Nd.c[EXG_N_DVEL + c][ni] : R(0);
+        }
+    }
+    __syncthreads();
+    const int s0 = start[t], n = count[t];
+    const int iters = (n + blockDim.x - 1) / blockDim.x;
+    for (int it = 0; it < iters; ++it) {
+        const int k = s0 + it * blockDim.x + threadIdx.x;
+        const bool live = k < s0 + n;
+        double bnd[CH_ALL] = {};
+        double dtp = 0.0;
+        bool red = false;
+        if (live) {
+            const int p = perm[k];
+            const int phase = A.phase[p];
+            double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+            R v[3], vp[3];
+            for (int d = 0; d < 3; ++d) {
+                v[d] = A.v[d][p];
+                vp[d] = A.vp[d][p];
+            }
+            if (mode == GM_VEL) {
+                if (phase == 0) {
+                    int iv[3];
+                    cell_of(P, x, iv);
+                    R E[9], sr[6];
+                    g2p_particle<R, ORD>(*tab, P, na, x, iv, true, false, v, vp, E, sr, dt);
+                    for (int d = 0; d < 3; ++d) {
+                        A.v[d][p] = v[d];
+                        A.vp[d][p] = vp[d];
+                    }
+                }
+            } else {
+                R E[9], sr[6], eps[6], sig[6];
+                for (int q = 0; q < 9; ++q) E[q] = A.E[q][p];
+                for (int c = 0; c < 6; ++c) {
+                    sr[c] = A.sr[c][p];
+                    eps[c] = A.eps[c][p];
+                    sig[c] = A.sig[c][p];
+                }
+                R vol = A.vol[p], rho = A.rho[p], J = A.J[p], pres = A.pres[p];
+                const R mass = A.mass[p], vol0 = A.vol0[p];
+                const int mi = A.mat[p];
+                if (phase == 0) {
+                    int iv[3];
+                    cell_of(P, x, iv);
+                    g2p_particle<R, ORD>(*tab, P, na, x, iv, upd_vel, true, v, vp, E, sr, dt);
+                }
+                move_particle<R>(P, bc, phase, x, v, vp, dt, status);
+                // Redistribute's periodic wrap
+                for (int d = 0; d < 3; ++d)
+                    if (P.periodic[d]) {
+                        double L = P.phi[d] - P.plo[d];
+                        if (x[d] >= P.phi[d])
+                            x[d] -= L;
+                        else if (x[d] < P.plo[d])
+                            x[d] += L;
+                    }
+                const Material mt = mats[mi];
+                if (phase == 0) {
+                    volume_stress<R>(P, mt, E, vol0, mass, sr, eps, sig, vol, rho, J, pres, dt, asr, true, true);
+                    if (!all_finite(v, 3) || !all_finite(sig, 6) || !isfinite((double)J)) status |= ST_NAN;
+                    // reductions for the next step
+                    int iv2[3];
+                    cell_of(P, x, iv2);
+                    bool in = true;
+                    for (int d = 0; d < 3; ++d) in = in && iv2[d] >= 0 && iv2[d] < P.nc[d];
+                    if (in) {
+                        double vd[3] = {(double)v[0], (double)v[1], (double)v[2]};
+                        double sd[6];
+                        for (int c = 0; c < 6; ++c) sd[c] = (double)sig[c];
+                        double q[3] = {0, 0, 0}, cp = 0, T = 0, kc = 0, Q = 0;
+                        if (P.use_temp) {
+                            for (int d = 0; d < 3; ++d) q[d] = (double)A.q[d][p];
+                            cp = A.cp[p];
+                            T = A.T[p];
+                            kc = A.kc[p];
+                            Q = A.Q[p];
+                        }
+                        particle_bounds<R>(P, mt, (double)mass, vd, (double)vol, sd, (double)rho, cp, T, kc, q, Q,
+                                           bnd, dtp);
+                        red = true;
+                    }
+                }
+                // write B at the sorted position k
+                for (int d = 0; d < 3; ++d) {
+                    Bo.x[d][k] = x[d];
+                    Bo.v[d][k] = v[d];
+                    Bo.vp[d][k] = vp[d];
+                }
+                for (int c = 0; c < 6; ++c) {
+                    Bo.sr[c][k] = sr[c];
+                    Bo.eps[c][k] = eps[c];
+                    Bo.sig[c][k] = sig[c];
+                }
+                for (int q = 0; q < 9; ++q) Bo.E[q][k] = E[q];
+                Bo.vol[k] = vol;
+                Bo.rho[k] = rho;
+                Bo.J[k] = J;
+                Bo.pres[k] = pres;
+                Bo.mass[k] = mass;
+                Bo.vol0[k] = vol0;
+                Bo.radius[k] = A.radius[p];
+                Bo.yacc[k] = A.yacc[p];
+                Bo.mat[k] = mi;
+                Bo.phase[k] = (uint8_t)phase;
+                Bo.rigid[k] = A.rigid[p];
+                Bo.pid[k] = A.pid[p];
+                if (P.use_temp) {
+                    Bo.T[k] = A.T[p];
+                    Bo.cp[k] = A.cp[p];
+                    Bo.kc[k] = A.kc[p];
+                    Bo.Q[k] = A.Q[p];
+                    for (int d = 0; d < 3; ++d) Bo.q[d][k] = A.q[d][p];
+                }
+            }
+        }
+        if (mode != GM_VEL) block_reduce_push(&ctl->bound_bits[0], &ctl->dtmin_bits, bnd, dtp, red);
+        __syncthreads();
+    }
+    }
+    if (status) atomicOr(&ctl->status, status);
+}
+
+// Particles outside the domain belong to no tile, so the fused G2P does not
+// write them; they follow the sorted ones in the re-ordered storage
+// (removed particles stay in storage, inert, as AMReX-invalidated ones do).
+template <class R>
+__device__ __forceinline__ void copy_particle(const Parts<R> &A, long long i, Parts<R> &Bo, long long j, bool temp) {
+    for (int d = 0; d < 3; ++d) {
+        Bo.x[d][j] = A.x[d][i];
+        Bo.v[d][j] = A.v[d][i];
+        Bo.vp[d][j] = A.vp[d][i];
+    }
+    for (int c = 0; c < 6; ++c) {
+        Bo.sr[c][j] = A.sr[c][i];
+        Bo.eps[c][j] = A.eps[c][i];
+        Bo.sig[c][j] = A.sig[c][i];
+    }
+    for (int q = 0; q < 9; ++q) Bo.E[q][j] = A.E[q][i];
+    Bo.vol[j] = A.vol[i];
+    Bo.mass[j] = A.mass[i];
+    Bo.rho[j] = A.rho[i];
+    Bo.J[j] = A.J[i];
+    Bo.pres[j] = A.pres[i];
+    Bo.vol0[j] = A.vol0[i];
+    Bo.radius[j] = A.radius[i];
+    Bo.yacc[j] = A.yacc[i];
+    Bo.mat[j] = A.mat[i];
+    Bo.phase[j] = A.phase[i];
+    Bo.rigid[j] = A.rigid[i];
+    Bo.pid[j] = A.pid[i];
+    if (temp) {
+        Bo.T[j] = A.T[i];
+        Bo.cp[j] = A.cp[i];
+        Bo.kc[j] = A.kc[i];
+        Bo.Q[j] = A.Q[i];
+        for (int d = 0; d < 3; ++d) Bo.q[d][j] = A.q[d][i];
+    }
+}
+
+template <class R>
+__global__ void k_copy_lost(Parts<R> A, Parts<R> Bo, const uint32_t *key, long long np, Ctl *ctl, int temp) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= np || key[i] != 0xFFFFFFFFu) return;
+    long long j = ctl->n_sorted + (long long)atomicAdd(&ctl->lost_fill, 1ull);
+    copy_particle<R>(A, i, Bo, j, temp != 0);
+}
+
+// ---------------------------------------------------------------- unfused L5 kernels
+template <class R>
+__global__ void k_node_backup(Params P, Nodes<R> Nd) {  // backup_current_velocity
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= P.nnodes) return;
+    if (Nd.c[EXG_N_MASS][n] > R(0)) {
+        Nd.c[EXG_N_MASS_OLD][n] = Nd.c[EXG_N_MASS][n];
+        for (int d = 0; d < 3; ++d) Nd.c[EXG_N_DVEL + d][n] = Nd.c[EXG_N_VEL + d][n];
+    }
+}
+template <class R>
+__global__ void k_node_time_update(Params P, Nodes<R> Nd, double dt) {  // Nodal_Time_Update_Momentum
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= P.nnodes) return;
+    double m = (double)Nd.c[EXG_N_MASS][n];
+    for (int d = 0; d < 3; ++d) {
+        if (m >= P.mass_tol)
+            Nd.c[EXG_N_VEL + d][n] = (R)((double)Nd.c[EXG_N_VEL + d][n] + (double)Nd.c[EXG_N_FRC + d][n] / m * dt);
+        else
+            Nd.c[EXG_N_VEL + d][n] = R(0);
+    }
+}
+template <class R>
+__global__ void k_node_bcs(Params P, Nodes<R> Nd, NodeBCArgs bc, Ctl *ctl) {  // Apply_Nodal_BCs
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= P.nnodes) return;
+    int i = (int)(n % P.nn[0]), j = (int)((n / P.nn[0]) % P.nn[1]), k = (int)(n / ((long long)P.nn[0] * P.nn[1]));
+    if ((P.periodic[0] && i == P.nc[0]) || (P.periodic[1] && j == P.nc[1]) || (P.periodic[2] && k == P.nc[2])) return;
+    unsigned status = 0;
+    double m = (double)Nd.c[EXG_N_MASS][n];
+    double v[3] = {(double)Nd.c[EXG_N_VEL][n], (double)Nd.c[EXG_N_VEL + 1][n], (double)Nd.c[EXG_N_VEL + 2][n]};
+    node_bcs(P, bc, i, j, k, m, v, status);
+    for (int d = 0; d < 3; ++d) {
+        Nd.c[EXG_N_VEL + d][n] = (R)v[d];
+        if (m > 0.0) Nd.c[EXG_N_DVEL + d][n] = (R)(v[d] - (double)Nd.c[EXG_N_DVEL + d][n]);
+    }
+    if (status) atomicOr(&ctl->status, status);
+}
+
+template <class R, int ORD>
+__global__ void __launch_bounds__(kThreads) k_g2p_simple(Params P, Parts<R> A, Nodes<R> Nd, long long np, int upd_vel,
+                                                         int upd_sr, double dt) {
+    __shared__ SplineTables tab;
+    load_tables(&tab);
+    __syncthreads();
+    long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= np || A.phase[p] != 0) return;
+    GlobalNodes<R> na;
+    for (int d = 0; d < 3; ++d) {
+        na.v[d] = Nd.c[EXG_N_VEL + d];
+        na.dv[d] = Nd.c[EXG_N_DVEL + d];
+    }
+    na.P = P;
+    double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+    int iv[3];
+    cell_of(P, x, iv);
+    R v[3], vp[3], E[9], sr[6];
+    for (int d = 0; d < 3; ++d) {
+        v[d] = A.v[d][p];
+        vp[d] = A.vp[d][p];
+    }
+    for (int q = 0; q < 9; ++q) E[q] = A.E[q][p];
+    for (int c = 0; c < 6; ++c) sr[c] = A.sr[c][p];
+    g2p_particle<R, ORD>(tab, P, na, x, iv, upd_vel != 0, upd_sr != 0, v, vp, E, sr, dt);
+    if (upd_vel)
+        for (int d = 0; d < 3; ++d) {
+            A.v[d][p] = v[d];
+            A.vp[d][p] = vp[d];
+        }
+    if (upd_sr) {
+        for (int q = 0; q < 9; ++q) A.E[q][p] = E[q];
+        for (int c = 0; c < 6; ++c) A.sr[c][p] = sr[c];
+    }
+}
+
+template <class R>
+__global__ void k_move(Params P, Parts<R> A, NodeBCArgs bc, long long np, double dt, Ctl *ctl) {
+    long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    unsigned status = 0;
+    double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+    R v[3], vp[3];
+    for (int d = 0; d < 3; ++d) {
+        v[d] = A.v[d][p];
+        vp[d] = A.vp[d][p];
+    }
+    move_particle<R>(P, bc, A.phase[p], x, v, vp, dt, status);
+    for (int d = 0; d < 3; ++d) {
+        A.x[d][p] = x[d];
+        A.v[d][p] = v[d];
+    }
+    if (status) atomicOr(&ctl->status, status);
+}
+
+template <class R>
+__global__ void k_vol_stress(Params P, Parts<R> A, const Material *mats, long long np, double dt, double asr,
+                             int do_volume, int do_stress) {
+    long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= np || A.phase[p] != 0) return;
+    R E[9], sr[6], eps[6], sig[6];
+    for (int q = 0; q < 9; ++q) E[q] = A.E[q][p];
+    for (int c = 0; c < 6; ++c) {
+        sr[c] = A.sr[c][p];
+        eps[c] = A.eps[c][p];
+        sig[c] = A.sig[c][p];
+    }
+    R vol = A.vol[p], rho = A.rho[p], J = A.J[p], pres = A.pres[p];
+    const Material mt = mats[A.mat[p]];
+    if (do_stress && mt.model != 0 && mt.model != 1) return;
+    volume_stress<R>(P, mt, E, A.vol0[p], A.mass[p], sr, eps, sig, vol, rho, J, pres, dt, asr, do_volume != 0,
+                     do_stress != 0);
+    if (do_volume) {
+        A.vol[p] = vol;
+        A.rho[p] = rho;
+        A.J[p] = J;
+    }
+    if (do_stress) {
+        for (int c = 0; c < 6; ++c) {
+            A.eps[c][p] = eps[c];
+            A.sig[c][p] = sig[c];
+        }
+        A.pres[p] = pres;
+    }
+}
+
+// Do_All_Diagnostics reductions (mpm_diagnostics.cpp:23-216) as one pass with
+// a fixed-shape tree: per-block partials in FP64, summed in block order by a
+// second single-block pass, so the result is deterministic.
+constexpr int kDiagN = 16;  // tke tse mass mom3 mvm min3 max3 np
+template <class R>
+__global__ void __launch_bounds__(kThreads) k_diag_partial(Params P, Parts<R> A, long long np, double *part) {
+    __shared__ double sh[kDiagN][kThreads];
+    long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    double a[kDiagN];
+    for (int c = 0; c < kDiagN; ++c) a[c] = 0.0;
+    a[9] = a[10] = a[11] = 1.7976931348623157e308;
+    a[12] = a[13] = a[14] = -1.7976931348623157e308;
+    if (p < np) {
+        double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+        int iv[3];
+        cell_of(P, x, iv);
+        bool in = true;
+        for (int d = 0; d < 3; ++d) in = in && iv[d] >= 0 && iv[d] < P.nc[d];
+        if (in) {
+            double m = A.mass[p];
+            double v[3] = {(double)A.v[0][p], (double)A.v[1][p], (double)A.v[2][p]};
+            double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            a[0] = 0.5 * m * v2;
+            double s[6], e[6];
+            for (int c = 0; c < 6; ++c) {
+                s[c] = A.sig[c][p];
+                e[c] = A.eps[c][p];
+            }
+            double se = s[0] * e[0] + s[3] * e[3] + s[5] * e[5] + 2.0 * (s[1] * e[1] + s[4] * e[4] + s[2] * e[2]);
+            a[1] = 0.5 * (double)A.vol[p] * se;
+            a[2] = m;
+            for (int d = 0; d < 3; ++d) a[3 + d] = m * v[d];
+            a[6] = m * sqrt(v2);
+            for (int d = 0; d < 3; ++d) {
+                a[9 + d] = x[d];
+                a[12 + d] = x[d];
+            }
+            a[15] = 1.0;
+        }
+    }
+    for (int c = 0; c < kDiagN; ++c) sh[c][threadIdx.x] = a[c];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            for (int c = 0; c < kDiagN; ++c) {
+                double o = sh[c][threadIdx.x + s];
+                if (c >= 9 && c < 12)
+                    sh[c][threadIdx.x] = fmin(sh[c][threadIdx.x], o);
+                else if (c >= 12 && c < 15)
+                    sh[c][threadIdx.x] = fmax(sh[c][threadIdx.x], o);
+                else
+                    sh[c][threadIdx.x] += o;
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x < kDiagN) part[(long long)blockIdx.x * kDiagN + threadIdx.x] = sh[threadIdx.x][0];
+}
+__global__ void k_diag_final(const double *part, int nblk, double *out) {
+    int c = threadIdx.x;
+    if (c >= kDiagN) return;
+    double acc = (c >= 9 && c < 12) ? 1.7976931348623157e308 : ((c >= 12 && c < 15) ? -1.7976931348623157e308 : 0.0);
+    for (int b = 0; b < nblk; ++b) {
+        double v = part[(long long)b * kDiagN + c];
+        if (c >= 9 && c < 12)
+            acc = fmin(acc, v);
+        else if (c >= 12 && c < 15)
+            acc = fmax(acc, v);
+        else
+            acc += v;
+    }
+    out[c] = acc;
+}
+
+}  // namespace
+
+// ====================================================================== launchers
+static int nblocks(long long n, int t = kThreads) { return (int)((n + t - 1) / t); }
+
+// Grid of a persistent kernel: every SM filled to its occupancy limit.
+template <class K>
+static int persistent_grid(K kern, size_t smem) {
+    int dev = 0, nsm = 0, per = 0;
+    EXG_CUDA_OK(cudaGetDevice(&dev));
+    EXG_CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    EXG_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kThreads, smem));
+    if (per < 1) per = 1;
+    return nsm * per;
+}
+
+static NodeBCArgs make_bc(Ctx &c) {
+    NodeBCArgs bc;
+    for (int s = 0; s < 2; ++s)
+        for (int d = 0; d < 3; ++d) bc.udf[s][d] = c.udf_tab[s][d];
+    for (int b = 0; b < kMaxBodies; ++b) bc.ls[b] = c.ls[b];
+    return bc;
+}
+
+#if defined(EXG_R_FP64)
+void launch_keys(Ctx &c) {
+    EXG_CUDA_OK(cudaMemsetAsync(c.sb.tile_count, 0, sizeof(int) * c.P.ntiles, c.stream));
+    EXG_CUDA_OK(cudaMemsetAsync(c.sb.tile_fill, 0, sizeof(int) * c.P.ntiles, c.stream));
+    double **x = c.precision == EXG_PREC_FP64 ? c.A<double>().x : c.A<float>().x;
+    if (c.np > 0)
+        k_keys<<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, x[0], x[1], x[2], c.np, c.sb.key, c.sb.tile_count, c.ctl,
+                                                         1);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void launch_sort_rest(Ctx &c, bool touched_list) {
+    k_tile_scan<<<1, 1024, 0, c.stream>>>((int)c.P.ntiles, c.sb.tile_count, c.sb.tile_start, c.sb.active, c.sb.slot,
+                                          c.ctl);
+    if (c.np > 0)
+        k_scatter<<<nblocks(c.np), kThreads, 0, c.stream>>>(c.np, c.sb.key, 3 * c.P.tshift, c.sb.tile_start,
+                                                            c.sb.tile_fill, c.sb.bucket);
+    const int ncell = c.P.T * c.P.T * c.P.T;
+    size_t sm = sizeof(int) * (3 * ncell + kSortCap);
+    EXG_CUDA_OK(cudaFuncSetAttribute(k_tile_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    static int sgrid = 0;
+    if (!sgrid) sgrid = persistent_grid(k_tile_sort, sm);
+    k_tile_sort<<<sgrid, kThreads, sm, c.stream>>>(c.sb.active, c.sb.tile_start, c.sb.tile_count, c.sb.key,
+                                                    c.sb.bucket, c.sb.bucket + c.cap, c.sb.perm, ncell, c.ctl);
+    if (touched_list)
+        k_touched<<<nblocks(c.P.ntiles), kThreads, 0, c.stream>>>(c.P, c.sb.tile_count, c.sb.touched,
+                                                                  c.sb.touched_step, c.ctl);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void launch_dt_finalize(Ctx &c, bool reset) {
+    k_dt_finalize<<<1, 1, 0, c.stream>>>(c.P, c.ctl, reset ? 1 : 0);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void launch_scales_from(Ctx &c, const unsigned long long *bounds) {
+    const int W = (c.P.uniform_order == 1) ? 2 : 4;
+    k_scales<<<1, 32, 0, c.stream>>>(c.ctl, W * W * W, bounds);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void launch_reset_accum(Ctx &c, unsigned long long *bounds, unsigned long long *dtmin) {
+    k_reset_accum<<<1, 32, 0, c.stream>>>(bounds, dtmin);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void launch_time_advance(Ctx &c) {
+    k_time_advance<<<1, 1, 0, c.stream>>>(c.ctl);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void launch_node_reset(Ctx &c) {
+    const size_t esz = c.precision == EXG_PREC_FP64 ? 8 : 4;
+    for (void *p : c.node_allocs) EXG_CUDA_OK(cudaMemsetAsync(p, 0, esz * c.P.nnodes, c.stream));
+}
+#endif
+
+// ---- precision-specific launchers
+void EXG_SFX(launch_state_reduce)(Ctx &c, unsigned long long *bounds, unsigned long long *dtmin) {
+    using R = EXG_R;
+    if (c.np == 0) return;
+    k_state_reduce<R><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.mat_dev, c.np, bounds, dtmin);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+template <class R, int ORD, bool TH>
+static void p2g_t(Ctx &c, int flags) {
+    const int NCH = TH ? CH_ALL : CH_MOM_END;
+    const int B3 = c.P.B * c.P.B * c.P.B;
+    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * NCH * B3;
+    auto kern = k_p2g<R, ORD, TH>;
+    EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    static int grid = 0;
+    static size_t gsm = 0;
+    if (!grid || gsm != sm) {
+        grid = persistent_grid(kern, sm);
+        gsm = sm;
+    }
+    kern<<<grid, kThreads, sm, c.stream>>>(c.P, c.A<R>(), c.sb.active, c.sb.tile_start, c.sb.tile_count, c.sb.perm,
+                                           c.staging, c.ctl, flags);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+void EXG_SFX(launch_p2g)(Ctx &c, int flags) {
+    using R = EXG_R;
+    const bool th = (flags & (PF_TEMP | PF_SRC)) != 0;
+    switch (c.P.uniform_order) {
+        case 1: th ? p2g_t<R, 1, true>(c, flags) : p2g_t<R, 1, false>(c, flags); break;
+        case 2: th ? p2g_t<R, 2, true>(c, flags) : p2g_t<R, 2, false>(c, flags); break;
+        case 3: th ? p2g_t<R, 3, true>(c, flags) : p2g_t<R, 3, false>(c, flags); break;
+        default: th ? p2g_t<R, 0, true>(c, flags) : p2g_t<R, 0, false>(c, flags); break;
+    }
+}
+
+void EXG_SFX(launch_nodes)(Ctx &c, int mode, int flags, bool all_tiles) {
+    using R = EXG_R;
+    const bool th = (flags & (PF_TEMP | PF_SRC)) != 0;
+    static int pgrid = 0;
+    if (!pgrid) pgrid = persistent_grid(k_nodes<R, true>, 0);
+    int grid = all_tiles ? (int)std::min<long long>(c.P.ntiles, pgrid) : pgrid;
+    const int *tiles = all_tiles ? nullptr : c.sb.touched;
+    NodeBCArgs bc = make_bc(c);
+    if (th)
+        k_nodes<R, true><<<grid, kThreads, 0, c.stream>>>(c.P, c.N<R>(), bc, tiles, c.sb.slot, c.staging, c.ctl, mode,
+                                                          flags);
+    else
+        k_nodes<R, false><<<grid, kThreads, 0, c.stream>>>(c.P, c.N<R>(), bc, tiles, c.sb.slot, c.staging, c.ctl,
+                                                           mode, flags);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+template <class R, int ORD>
+static void g2p_t(Ctx &c, int mode) {
+    const int B3 = c.P.B * c.P.B * c.P.B;
+    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(R) * 6 * B3;
+    auto kern = k_g2p_fused<R, ORD>;
+    EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    static int grid = 0;
+    static size_t gsm = 0;
+    if (!grid || gsm != sm) {
+        grid = persistent_grid(kern, sm);
+        gsm = sm;
+    }
+    kern<<<grid, kThreads, sm, c.stream>>>(c.P, c.A<R>(), c.Bp<R>(), c.N<R>(), make_bc(c), c.mat_dev, c.sb.active,
+                                           c.sb.tile_start, c.sb.tile_count, c.sb.perm, c.ctl, mode);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+void EXG_SFX(launch_g2p_fused)(Ctx &c, int mode) {
+    using R = EXG_R;
+    switch (c.P.uniform_order) {
+        case 1: g2p_t<R, 1>(c, mode); break;
+        case 2: g2p_t<R, 2>(c, mode); break;
+        case 3: g2p_t<R, 3>(c, mode); break;
+        default: g2p_t<R, 0>(c, mode); break;
+    }
+}
+
+void EXG_SFX(launch_copy_lost)(Ctx &c) {
+    if (c.np == 0) return;
+    k_copy_lost<EXG_R><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.A<EXG_R>(), c.Bp<EXG_R>(), c.sb.key, c.np, c.ctl,
+                                                                 c.specs.use_temp);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void EXG_SFX(launch_g2p_simple)(Ctx &c, int uv, int us, double dt) {
+    using R = EXG_R;
+    if (c.np == 0) return;
+    switch (c.P.uniform_order) {
+        case 1: k_g2p_simple<R, 1><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, uv, us, dt); break;
+        case 2: k_g2p_simple<R, 2><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, uv, us, dt); break;
+        case 3: k_g2p_simple<R, 3><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, uv, us, dt); break;
+        default: k_g2p_simple<R, 0><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, uv, us, dt); break;
+    }
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void EXG_SFX(launch_node_backup)(Ctx &c) {
+    k_node_backup<EXG_R><<<nblocks(c.P.nnodes), kThreads, 0, c.stream>>>(c.P, c.N<EXG_R>());
+    EXG_CUDA_OK(cudaGetLastError());
+}
+void EXG_SFX(launch_node_time_update)(Ctx &c, double dt) {
+    k_node_time_update<EXG_R><<<nblocks(c.P.nnodes), kThreads, 0, c.stream>>>(c.P, c.N<EXG_R>(), dt);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+void EXG_SFX(launch_node_bcs)(Ctx &c) {
+    k_node_bcs<EXG_R><<<nblocks(c.P.nnodes), kThreads, 0, c.stream>>>(c.P, c.N<EXG_R>(), make_bc(c), c.ctl);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+void EXG_SFX(launch_move)(Ctx &c, double dt) {
+    if (c.np == 0) return;
+    k_move<EXG_R><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<EXG_R>(), make_bc(c), c.np, dt, c.ctl);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+void EXG_SFX(launch_volume)(Ctx &c) {
+    if (c.np == 0) return;
+    k_vol_stress<EXG_R><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<EXG_R>(), c.mat_dev, c.np, 0.0, 0.0, 1, 0);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+void EXG_SFX(launch_stress)(Ctx &c, double time, double dt) {
+    if (c.np == 0) return;
+    double asr = (time < c.P.applied_sr_time) ? c.P.applied_sr : 0.0;
+    k_vol_stress<EXG_R><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<EXG_R>(), c.mat_dev, c.np, dt, asr, 0, 1);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+void EXG_SFX(launch_diag)(Ctx &c, double *out_dev) {
+    int nb = nblocks(c.np > 0 ? c.np : 1);
+    double *part = out_dev + 32;
+    k_diag_partial<EXG_R><<<nb, kThreads, 0, c.stream>>>(c.P, c.A<EXG_R>(), c.np, part);
+    k_diag_final<<<1, 32, 0, c.stream>>>(part, nb, out_dev);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+}  // namespace exg

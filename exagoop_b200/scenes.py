@@ -1,0 +1,182 @@
+"""Seeded synthetic scenes with the shapes, sizes and parameters of the
+benchmark workloads (no dataset is used; every particle set is generated here).
+
+Particles sit on the regular per-cell lattice of the reference's generator
+(offsets (k + 0.5) / n of a cell per axis, as Tests/*/PreProcess/
+Generate_MPs_Inputfile_Generic.py places them) and get the derived fields
+InitParticles sets (Source/mpm_init.cpp:1120-1160): V = 4/3 pi r^3 with the
+reference's truncated constants, m = rho V, J = 1, F = I.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import native as nt
+
+FOURBYTHREE = 1.3333333333  # Source/constants.H:9
+PI = 3.141592654            # Source/constants.H:10
+
+
+def lattice(lo, hi, dx, ppc):
+    """Lattice points of a box [lo, hi) with ppc points per cell edge."""
+    axes = []
+    for d in range(3):
+        h = dx[d] / ppc[d]
+        n = int(np.floor((hi[d] - lo[d]) / h + 1e-9))
+        start = lo[d] + 0.5 * h
+        pts = start + h * np.arange(n)
+        axes.append(pts[pts < hi[d]])
+    g = np.meshgrid(*axes, indexing="ij")
+    return np.stack([a.ravel(order="F") for a in g])  # x fastest
+
+
+def make_particles(pos: np.ndarray, dx, ppc, density, model: int, E=0.0, nu=0.0, K=0.0, gamma=0.0, visc=0.0):
+    n = pos.shape[1]
+    p = nt.Particles(n)
+    p.pos[:] = pos
+    vol = (dx[0] / ppc[0]) * (dx[1] / ppc[1]) * (dx[2] / ppc[2])
+    radius = (vol / (FOURBYTHREE * PI)) ** (1.0 / 3.0)
+    v = FOURBYTHREE * PI * radius ** 3
+    p.rdata[nt.R_RADIUS] = radius
+    p.rdata[nt.R_DENSITY] = density
+    p.rdata[nt.R_VOLUME] = v
+    p.rdata[nt.R_VOL_INIT] = v
+    p.rdata[nt.R_MASS] = density * v
+    p.rdata[nt.R_JACOBIAN] = 1.0
+    for d in range(3):
+        p.rdata[nt.R_DEFGRAD + 4 * d] = 1.0
+    p.idata[nt.I_MODEL] = model
+    p.idata[nt.I_RIGID_ID] = -1
+    if model == 0:
+        p.rdata[nt.R_E] = E
+        p.rdata[nt.R_NU] = nu
+    else:
+        p.rdata[nt.R_BULK] = K
+        p.rdata[nt.R_GAMMA] = gamma
+        p.rdata[nt.R_VISC] = visc
+    return p
+
+
+def base_specs(plo, phi, ncells, order, precision=nt.PREC_FP64):
+    s = nt.default_specs()
+    for d in range(3):
+        s.plo[d], s.phi[d], s.ncells[d] = plo[d], phi[d], ncells[d]
+        s.gravity[d] = 0.0
+    s.order_scheme = order
+    for d in range(3):
+        s.order[d] = order if (order == 1 or ncells[d] >= 5) else 1
+    s.mass_tolerance = 1e-18
+    s.precision = precision
+    s.max_steps = 1000000
+    s.final_time = 1e30
+    s.applied_strainrate_time = s.final_time
+    return s
+
+
+def axial_bar(nx=64, steps=1000, precision=nt.PREC_FP64):
+    """3-D linear-elastic axial bar: 64x4x4 cells, dx = 1/64, the bar fills
+    x in [0,1], 2x2x2 lattice (8192 particles), E = 100, nu = 0, rho = 1,
+    v_x = 0.1 sin(pi x / 2), x = 0 face fixed (noslip), x = 1 face slip (the
+    reference has no free-end BC), linear shape functions, FLIP 0.99,
+    dt = 0.1 dx / sqrt(E / rho)."""
+    dx = 1.0 / nx
+    ny = 4
+    s = base_specs((0, 0, 0), (1.0, ny * dx, ny * dx), (nx, ny, ny), 1, precision)
+    s.alpha_pic_flip = 0.99
+    s.fixed_timestep = 1
+    s.timestep = 0.1 * dx / np.sqrt(100.0 / 1.0)
+    s.bclo[0] = nt.BC_NOSLIP
+    s.bchi[0] = nt.BC_SLIP
+    pos = lattice((0, 0, 0), (1.0, ny * dx, ny * dx), (dx, dx, dx), (2, 2, 2))
+    p = make_particles(pos, (dx, dx, dx), (2, 2, 2), 1.0, 0, E=100.0, nu=0.0)
+    p.rdata[nt.R_VEL] = 0.1 * np.sin(np.pi * p.pos[0] / 2.0)
+    return s, p
+
+
+def dam_break(n=(256, 128, 128), size=(1.0, 0.5, 0.5), block=(0.4, 0.5, 0.3), seed=1234,
+              precision=nt.PREC_FP64, order=2):
+    """3-D dam break of a weakly compressible fluid: Tait EOS K = 2e6 Pa,
+    gamma = 7, rho0 = 1000, mu = 1e-3; gravity -9.81 in z; the water block in
+    the low corner at 2x2x2 particles per cell, jittered uniformly within
+    +-0.25 dx from a seed; quadratic B-splines, slip walls, CFL dt."""
+    dx = tuple(size[d] / n[d] for d in range(3))
+    s = base_specs((0, 0, 0), size, n, order, precision)
+    s.gravity[2] = -9.81
+    s.cfl = 0.1
+    s.alpha_pic_flip = 0.99
+    pos = lattice((0, 0, 0), block, dx, (2, 2, 2))
+    rng = np.random.default_rng(seed)
+    pos = pos + rng.uniform(-0.25, 0.25, size=pos.shape) * np.array(dx)[:, None]
+    for d in range(3):
+        pos[d] = np.clip(pos[d], 1e-9 * size[d], size[d] * (1 - 1e-9))
+    p = make_particles(pos, dx, (2, 2, 2), 1000.0, 1, K=2e6, gamma=7.0, visc=1e-3)
+    return s, p
+
+
+def sphere_collision(n=256, radius=0.2, precision=nt.PREC_FP64, order=3, speed=0.1):
+    """Two linear-elastic spheres (E = 1e3, nu = 0.3, rho = 1000) of radius
+    0.2 centred at (0.3,0.5,0.5) and (0.7,0.5,0.5) moving at +-0.1 m/s in x,
+    in a unit cube on an n^3 grid, 2x2x2 lattice; cubic B-splines."""
+    dx = 1.0 / n
+    s = base_specs((0, 0, 0), (1, 1, 1), (n, n, n), order, precision)
+    s.alpha_pic_flip = 0.99
+    pos = lattice((0, 0, 0), (1, 1, 1), (dx, dx, dx), (2, 2, 2))
+    c1 = np.array([0.3, 0.5, 0.5])[:, None]
+    c2 = np.array([0.7, 0.5, 0.5])[:, None]
+    in1 = ((pos - c1) ** 2).sum(0) < radius ** 2
+    in2 = ((pos - c2) ** 2).sum(0) < radius ** 2
+    sel = in1 | in2
+    pos = np.ascontiguousarray(pos[:, sel])
+    p = make_particles(pos, (dx, dx, dx), (2, 2, 2), 1000.0, 0, E=1e3, nu=0.3)
+    p.rdata[nt.R_VEL] = np.where(in1[sel], speed, -speed)
+    return s, p
+
+
+def sphere_union_levelset(specs, centers, radii) -> np.ndarray:
+    """One nodal level set, phi = min_i (|x - c_i| - r_i), phi < 0 inside:
+    the union of analytic spheres as one body (the MultiUDF union of
+    Source/mpm_eb_udf_build.cpp:42-68)."""
+    nn = [specs.ncells[d] + 1 for d in range(3)]
+    dx = [(specs.phi[d] - specs.plo[d]) / specs.ncells[d] for d in range(3)]
+    ax = [specs.plo[d] + dx[d] * np.arange(nn[d]) for d in range(3)]
+    z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    phi = np.full(x.shape, np.inf)
+    for c, r in zip(centers, radii):
+        phi = np.minimum(phi, np.sqrt((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) - r)
+    return np.ascontiguousarray(phi.ravel())
+
+
+def twisted_column(n=(64, 64, 384), size=(0.2, 0.2, 1.2), col=(0.1, 0.1, 0.6), seed=4321,
+                   precision=nt.PREC_MIXED, n_obstacles=20, rigid_frac=0.05, order=2):
+    """Twisted elastic column with obstacles: column col (E = 1e5, nu = 0.3,
+    rho = 1000) standing on a noslip base, initial angular velocity 10 rad/s
+    about its axis, seeded analytic sphere obstacles (r in [0.02, 0.05]) as one
+    union level-set body, a seeded fraction of particles flagged rigid,
+    quadratic B-splines.  Returns (specs, particles, phi)."""
+    dx = tuple(size[d] / n[d] for d in range(3))
+    s = base_specs((0, 0, 0), size, n, order, precision)
+    s.bclo[2] = nt.BC_NOSLIP
+    s.alpha_pic_flip = 0.99
+    cx, cy = size[0] / 2, size[1] / 2
+    lo = (cx - col[0] / 2, cy - col[1] / 2, 0.0)
+    hi = (cx + col[0] / 2, cy + col[1] / 2, col[2])
+    pos = lattice(lo, hi, dx, (2, 2, 2))
+    p = make_particles(pos, dx, (2, 2, 2), 1000.0, 0, E=1e5, nu=0.3)
+    omega = 10.0
+    p.rdata[nt.R_VEL + 0] = -omega * (p.pos[1] - cy)
+    p.rdata[nt.R_VEL + 1] = omega * (p.pos[0] - cx)
+    rng = np.random.default_rng(seed)
+    p.idata[nt.I_PHASE] = (rng.random(p.n) < rigid_frac).astype(np.int32)
+    centers, radii = [], []
+    while len(centers) < n_obstacles:
+        r = rng.uniform(0.02, 0.05)
+        c = rng.uniform([r, r, r], [size[0] - r, size[1] - r, size[2] - r])
+        # keep obstacles clear of the column's initial volume
+        if (abs(c[0] - cx) < col[0] / 2 + r and abs(c[1] - cy) < col[1] / 2 + r and c[2] < col[2] + r):
+            continue
+        centers.append(c)
+        radii.append(r)
+    s.num_bodies = 1
+    s.bodies[0].mom_bc = nt.BC_NOSLIP
+    phi = sphere_union_levelset(s, centers, radii)
+    return s, p, phi

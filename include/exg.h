@@ -1,0 +1,291 @@
+/*
+ * exg.h -- C ABI of the B200-native explicit MPM time step.
+ *
+ * This library replaces the per-step particle/grid path of the ExaGOOP MPM
+ * solver (the L5 step functions declared in Source/utilities.H:28-79 and
+ * called from Source/main.cpp:88-146).  Every entry point takes plain
+ * pointers and sizes; no C++ or torch types cross this boundary.  All entry
+ * points return an int status: EXG_OK (0) or a negative EXG_ERR_* code.  The
+ * reference reports errors only through amrex::Abort (process exit); here the
+ * same conditions come back as status codes and exg_last_error() gives the
+ * message.
+ *
+ * Threading: one host thread per context; every device operation of a context
+ * is issued on the context's own CUDA stream.  3-D only (AMREX_SPACEDIM == 3).
+ */
+#ifndef EXG_H_
+#define EXG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define EXG_OK 0
+#define EXG_ERR_CONFIG (-1)      /* bad inputs-file value (reference: amrex::Abort in read_mpm_specs) */
+#define EXG_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define EXG_ERR_ALLOC (-3)       /* device or host allocation failed */
+#define EXG_ERR_NAN (-4)         /* a non-finite value was produced */
+#define EXG_ERR_DOMAIN (-5)      /* particles left a non-periodic domain and were dropped */
+#define EXG_ERR_OVERFLOW (-6)    /* a fixed-size buffer (sort bucket, fixed-point range) overflowed */
+#define EXG_ERR_TIMEOUT (-7)     /* a bounded device-side wait gave up */
+#define EXG_ERR_ARG (-8)         /* invalid argument */
+#define EXG_ERR_UNSUPPORTED (-9) /* feature outside this library's scope */
+#define EXG_ERR_IO (-10)         /* file could not be read or written */
+#define EXG_ERR_NOT_READY (-11)  /* call made before its prerequisite (e.g. no particles uploaded) */
+#define EXG_ERR_BC (-12)         /* outflow wall BC reached applybc (reference: mpm_kernels.H:103-110 aborts) */
+
+/* -------------------------------------------------------- particle fields */
+/* Host particle layout: component-major SoA of doubles whose component index
+ * is the reference's realData enum with USE_TEMP (Source/mpm_specs.H:17-61). */
+#define EXG_NREAL 53
+#define EXG_NINT 3
+enum exg_real_field {
+    EXG_R_RADIUS = 0,
+    EXG_R_VEL = 1,        /* 3 components */
+    EXG_R_VEL_PRIME = 4,  /* 3 */
+    EXG_R_STRAINRATE = 7, /* 6, packed XX XY XZ YY YZ ZZ (constants.H:80-87) */
+    EXG_R_STRAIN = 13,    /* 6 */
+    EXG_R_STRESS = 19,    /* 6 */
+    EXG_R_DEFGRAD = 25,   /* 9, row-major */
+    EXG_R_VOLUME = 34,
+    EXG_R_MASS = 35,
+    EXG_R_DENSITY = 36,
+    EXG_R_JACOBIAN = 37,
+    EXG_R_PRESSURE = 38,
+    EXG_R_VOL_INIT = 39,
+    EXG_R_E = 40,
+    EXG_R_NU = 41,
+    EXG_R_BULK = 42,
+    EXG_R_GAMMA = 43,
+    EXG_R_VISC = 44,
+    EXG_R_YACC = 45,
+    EXG_R_TEMPERATURE = 46,
+    EXG_R_SPHEAT = 47,
+    EXG_R_THERMCOND = 48,
+    EXG_R_HEATFLUX = 49, /* 3 */
+    EXG_R_HEATSRC = 52
+};
+/* intData (Source/mpm_specs.H:63-73) */
+enum exg_int_field { EXG_I_PHASE = 0, EXG_I_RIGID_ID = 1, EXG_I_MODEL = 2 };
+
+typedef struct exg_particle_soa {
+    int64_t np;      /* number of particles */
+    double *pos;     /* [3][np]: x, y, z */
+    double *rdata;   /* [EXG_NREAL][np] */
+    int32_t *idata;  /* [EXG_NINT][np] */
+} exg_particle_soa;
+
+/* --------------------------------------------------------- nodal fields */
+/* Nodal component indices of the reference with USE_TEMP (constants.H:30-64). */
+enum exg_node_comp {
+    EXG_N_MASS = 0,
+    EXG_N_VEL = 1,  /* 3 */
+    EXG_N_FRC = 4,  /* 3 */
+    EXG_N_DVEL = 7, /* 3 */
+    EXG_N_MASS_OLD = 10,
+    EXG_N_MASS_SPHEAT = 20,
+    EXG_N_MASS_SPHEAT_TEMP = 21,
+    EXG_N_TEMPERATURE = 22,
+    EXG_N_SOURCE_TEMP = 23,
+    EXG_N_DELTA_TEMPERATURE = 24,
+    EXG_N_MASS_COND = 25,
+    EXG_N_NCOMP = 26
+};
+
+/* ------------------------------------------------------ boundary codes */
+/* constants.H:89-99 */
+enum exg_bc { EXG_BC_PERIODIC = 0, EXG_BC_NOSLIP = 1, EXG_BC_SLIP = 2, EXG_BC_PARTIALSLIP = 3, EXG_BC_OUTFLOW = 4 };
+enum exg_bc_temp {
+    EXG_BCT_PERIODIC = 0,
+    EXG_BCT_ISOTHERMAL = 1,
+    EXG_BCT_ADIABATIC = 2,
+    EXG_BCT_USERFLUX = 3,
+    EXG_BCT_CONVECTION = 4
+};
+enum exg_precision { EXG_PREC_FP64 = 0, EXG_PREC_MIXED = 1 };
+
+#define EXG_MAX_BODIES 8 /* Source/mpm_eb.H:39 EXAGOOP_MAX_LS_BODIES */
+
+/* User-defined functions loaded from shared libraries, same C signatures as
+ * the reference (Source/mpm_specs.H:12-13, Source/mpm_udf_loader.H:81). */
+typedef void (*exg_wallvel_udf)(double x, double y, double z, double t, double vel[3]);
+typedef void (*exg_temp_udf)(double x, double y, double z, double t, double out[2]);
+typedef double (*exg_levelset_udf)(double x, double y, double z);
+
+typedef struct exg_body {
+    int mom_bc;        /* EXG_BC_NOSLIP / SLIP / PARTIALSLIP (mpm_eb.H:63-73) */
+    double wall_mu;
+    double wall_vel[3];
+    int temp_bc;       /* 0 adiabatic, 1 isothermal, 3 heatflux, 4 convective (mpm_eb.H:92-104) */
+    double T_wall, heat_flux, h_conv, T_inf;
+} exg_body;
+
+/* Run specification: the fields of MPMspecs (Source/mpm_specs.H:75-221) that
+ * the per-step path reads, after read_mpm_specs() and Initialise_Domain()'s
+ * per-direction order fallback (Source/mpm_init.cpp:175-268). */
+typedef struct exg_specs {
+    double plo[3], phi[3];
+    int ncells[3];
+    int periodic[3];
+    double gravity[3];
+    int external_loads;
+    double force_slab_lo[3], force_slab_hi[3], extforce[3];
+    int fixed_timestep;
+    double timestep;
+    double dt_min_limit, dt_max_limit, cfl;
+    double mass_tolerance, alpha_pic_flip;
+    int order_scheme;  /* mpm.order_scheme: 1, 2 or 3 */
+    int order[3];      /* order_scheme_directional */
+    int stress_update_scheme; /* 0 USL, 1 MUSL */
+    int calculate_strain_based_on_delta;
+    double applied_strainrate, applied_strainrate_time;
+    int bclo[3], bchi[3];
+    double wall_mu_lo[3], wall_mu_hi[3];
+    double wall_vel_lo[9], wall_vel_hi[9]; /* [face dir][component] */
+    exg_wallvel_udf udf_wallvel_lo[3], udf_wallvel_hi[3];
+    int use_temp;
+    int bclo_temp[3], bchi_temp[3];
+    double T_wall_lo[3], T_wall_hi[3], flux_lo[3], flux_hi[3], h_lo[3], h_hi[3], Tinf_lo[3], Tinf_hi[3];
+    exg_temp_udf udf_temp_lo[3], udf_temp_hi[3];
+    int num_bodies;
+    exg_body bodies[EXG_MAX_BODIES];
+    /* driver-level keys (main.cpp time loop) */
+    int max_steps;
+    double final_time;
+    int num_redist;
+    double write_output_time, screen_output_time, write_diag_output_time;
+    int print_diagnostics, do_calculate_tke_tse, do_calculate_mwa_velcomp, do_calculate_mwa_velmag,
+        do_calculate_minmaxpos;
+    /* B200 execution keys (exg.* namespace, no counterpart in the reference) */
+    int precision; /* EXG_PREC_FP64 or EXG_PREC_MIXED */
+    int tile;      /* tile edge in cells: 0 = autotune, else 4 or 8 */
+} exg_specs;
+
+typedef struct exg_diag {
+    double tke, tse;          /* mpm_diagnostics.cpp:23-72 */
+    double mass;              /* sum of particle mass (all phases) */
+    double momentum[3];       /* sum m v */
+    double mwa_vel[3];        /* mass-weighted velocity components (:91-127) */
+    double mwa_velmag;        /* (:145-178) */
+    double minpos[3], maxpos[3]; /* (:192-216) */
+    int64_t np;
+} exg_diag;
+
+/* ------------------------------------------------ inputs-file handling */
+typedef struct exg_inputs exg_inputs;
+
+/* Parse a ParmParse-style inputs file plus "key=value" overrides (the CLI of
+ * the reference executable).  path may be NULL. */
+int exg_inputs_parse(const char *path, int argc, const char *const *argv, exg_inputs **out);
+/* Same, from an in-memory text. */
+int exg_inputs_parse_text(const char *text, int argc, const char *const *argv, exg_inputs **out);
+void exg_inputs_free(exg_inputs *in);
+/* Raw value of a key (tokens joined by one space); EXG_ERR_ARG if absent. */
+int exg_inputs_get(const exg_inputs *in, const char *key, char *buf, size_t buflen);
+/* Fill specs from the inputs the way MPMspecs::read_mpm_specs
+ * (Source/mpm_specs.H:223-565), init_eb (Source/mpm_eb.cpp:403-547) and
+ * Initialise_Domain (Source/mpm_init.cpp:108-299) do.  err gets the message. */
+int exg_specs_from_inputs(const exg_inputs *in, exg_specs *specs, char *err, size_t errlen);
+void exg_specs_default(exg_specs *specs);
+/* Nodal level set of body b on the (ncells+1)^3 node grid, from the eb2.* /
+ * <body>.* keys (analytic sphere, plane, box, cylinder or udf_cpp).  The
+ * reference builds these in mpm_ebtools::init_eb (Source/mpm_eb.cpp:100-388). */
+int exg_levelset_build(const exg_inputs *in, const exg_specs *specs, int body, double *phi_nodes);
+
+/* ASCII particle file of InitParticles (Source/mpm_init.cpp:942-1167).
+ * Arrays are allocated with malloc; release with exg_particles_free. */
+int exg_particles_read_ascii(const char *path, int use_temp, exg_particle_soa *out);
+int exg_particles_alloc(int64_t np, exg_particle_soa *out);
+void exg_particles_free(exg_particle_soa *p);
+
+/* ------------------------------------------------------------- context */
+typedef struct exg_ctx exg_ctx;
+
+/* Owns all device memory of one simulation on one GPU. */
+int exg_ctx_create(const exg_specs *specs, int device, exg_ctx **out);
+int exg_ctx_destroy(exg_ctx *ctx);
+const char *exg_last_error(const exg_ctx *ctx);
+/* Device-side status word accumulated by kernels since the last call. */
+int exg_check_status(exg_ctx *ctx);
+int exg_synchronize(exg_ctx *ctx);
+
+/* Level set of body b, nodal (ncells+1)^3, x fastest (replaces the lsphi
+ * MultiFab of LevelSetBody, Source/mpm_eb.H:45-117). */
+int exg_set_levelset(exg_ctx *ctx, int body, const double *phi_nodes);
+
+/* Upload / download particles (host FP64 SoA).  Download returns particles in
+ * upload order. */
+int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p);
+int exg_particles_download(exg_ctx *ctx, exg_particle_soa *p);
+int exg_num_particles(exg_ctx *ctx, int64_t *np);
+/* Dense nodal component (reference component index) as (ncells+1)^3 doubles,
+ * x fastest. */
+int exg_nodes_download(exg_ctx *ctx, int comp, double *out);
+
+/* --- step functions: one per reference L5 function (Source/utilities.H) --- */
+/* Initialise_Internal_Forces (Source/mpm_init.cpp:368-445). */
+int exg_init_internal_forces(exg_ctx *ctx);
+/* Redistribute_Fill_Update (Source/utilities.cpp:420-434): cell-key sort,
+ * periodic wrap and removal of particles outside a non-periodic domain. */
+int exg_redistribute(exg_ctx *ctx);
+/* MPMParticleContainer::Calculate_time_step (mpm_particle_timestep.cpp:38-111). */
+int exg_calculate_time_step(exg_ctx *ctx, double *dt);
+/* Reset_Nodaldata_to_Zero (nodal_data_ops.cpp:924-927). */
+int exg_reset_nodaldata(exg_ctx *ctx);
+/* P2G_Momentum (utilities.cpp:121-133 -> mpm_particle_grid_ops.cpp:333-628). */
+int exg_p2g_momentum(exg_ctx *ctx, int update_mass, int update_vel, int update_forces);
+/* backup_current_velocity (nodal_data_ops.cpp:57-81). */
+int exg_backup_current_velocity(exg_ctx *ctx);
+/* Nodal_Time_Update_Momentum (nodal_data_ops.cpp:451-482). */
+int exg_nodal_time_update_momentum(exg_ctx *ctx, double dt);
+/* Apply_Nodal_BCs (utilities.cpp:183-204): walls, UDF walls, level sets,
+ * then store_delta_velocity. */
+int exg_apply_nodal_bcs(exg_ctx *ctx, double dt, double time);
+/* G2P_Momentum (utilities.cpp:259-269 -> mpm_particle_grid_ops.cpp:924-1098). */
+int exg_g2p_momentum(exg_ctx *ctx, int update_vel, int update_strainrate, double dt);
+/* Update_MP_Positions (utilities.cpp:315-334 -> mpm_particle_timestep.cpp:226-578). */
+int exg_update_mp_positions(exg_ctx *ctx, double dt);
+/* Update_MP_Volume (utilities.cpp:347-350 -> mpm_particle_timestep.cpp:131-182). */
+int exg_update_mp_volume(exg_ctx *ctx);
+/* Calculate_MP_Stress_Strain (utilities.cpp:372-400 -> mpm_particle_container.cpp:43-142). */
+int exg_calculate_mp_stress_strain(exg_ctx *ctx, double time, double dt);
+/* Thermal counterparts (main.cpp:99-106, 129-135). */
+int exg_p2g_temperature(exg_ctx *ctx, int reset, int update_temp, int update_source);
+int exg_backup_current_temperature(exg_ctx *ctx);
+int exg_nodal_time_update_temperature(exg_ctx *ctx, double dt);
+int exg_apply_nodal_bcs_temperature(exg_ctx *ctx, double dt, double time, int dirichlet_only);
+int exg_store_delta_temperature(exg_ctx *ctx);
+int exg_g2p_temperature(exg_ctx *ctx, int update_temperature, int update_heatflux);
+
+/* One or more complete explicit steps of main.cpp:83-171 (without output),
+ * fused into four kernels per step and replayed from a CUDA graph when the
+ * step has no host-side dependency.  dt and time stay on the device. */
+int exg_step(exg_ctx *ctx, int nsteps);
+int exg_get_time(exg_ctx *ctx, double *time, double *last_dt, int64_t *steps);
+int exg_set_time(exg_ctx *ctx, double time, int64_t steps);
+
+/* Deterministic device reductions of Do_All_Diagnostics (utilities.cpp:551-615). */
+int exg_diagnostics(exg_ctx *ctx, exg_diag *out);
+
+/* Cell keys and stable sort permutation of the current particle storage
+ * order (exposed so the sort can be checked against a CPU stable sort). */
+int exg_sort_keys(exg_ctx *ctx, uint32_t *keys, int32_t *perm);
+/* Tile edge (cells) the context uses. */
+int exg_tile_size(exg_ctx *ctx, int *tile);
+/* Per-stage device timing: while enabled, exg_step runs without graph
+ * replay and records CUDA events between its kernel stages.
+ * exg_last_step_timing returns the mean ms per step since it was enabled:
+ * [sort, p2g, nodal, g2p, steps timed]. */
+int exg_set_stage_timing(exg_ctx *ctx, int on);
+int exg_last_step_timing(exg_ctx *ctx, double *ms5);
+/* The CUDA stream (cudaStream_t) the context issues all its work on. */
+int exg_get_stream(exg_ctx *ctx, void **stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EXG_H_ */

@@ -1,0 +1,246 @@
+"""GPU parity: every step function of the C ABI against the FP64 oracle on
+the same seeded inputs.  FP64 tolerance: 1e-10 relative to the field's max
+norm (deterministic fixed-point P2G sums in a different order from the
+oracle's sequential sums); integer binning bit-exact."""
+import numpy as np
+import pytest
+
+from exagoop_b200 import native as nt, scenes
+import orc
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-10
+
+
+def rel(a, b):
+    scale = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() / scale
+
+
+def pair(specs, parts, phi=None):
+    ctx = nt.Context(specs)
+    ctx.upload(parts)
+    o = orc.Oracle(specs)
+    o.upload(parts)
+    if phi is not None:
+        ctx.set_levelset(0, phi)
+        o.set_levelset(0, phi)
+    return ctx, o
+
+
+def check_particles(g, r, tol=TOL64, fields=None):
+    fields = fields or [("vel", nt.R_VEL, 3), ("vel_prime", nt.R_VEL_PRIME, 3), ("strainrate", nt.R_STRAINRATE, 6),
+                        ("strain", nt.R_STRAIN, 6), ("stress", nt.R_STRESS, 6), ("defgrad", nt.R_DEFGRAD, 9),
+                        ("volume", nt.R_VOLUME, 1), ("density", nt.R_DENSITY, 1), ("jacobian", nt.R_JACOBIAN, 1),
+                        ("pressure", nt.R_PRESSURE, 1)]
+    for name, f, k in fields:
+        e = rel(g.rdata[f:f + k], r.rdata[f:f + k])
+        assert e < tol, f"{name}: max rel err {e:.3e}"
+    e = np.abs(g.pos - r.pos).max()
+    assert e < tol * max(1.0, np.abs(r.pos).max()), f"position: max abs err {e:.3e}"
+
+
+def small_dam(order=2, seed=3, n=(32, 16, 16)):
+    return scenes.dam_break(n=n, size=(1.0, 0.5, 0.5), block=(0.4, 0.5, 0.3), seed=seed, order=order)
+
+
+def random_scene(seed, n=(20, 12, 16), npart=4000, order=2, outside=0):
+    rng = np.random.default_rng(seed)
+    s = scenes.base_specs((0.1, -0.2, 0.0), (1.1, 0.4, 0.8), n, order)
+    s.gravity[2] = -3.0
+    dx = [(s.phi[d] - s.plo[d]) / n[d] for d in range(3)]
+    pos = np.stack([rng.uniform(s.plo[d], s.phi[d], npart) for d in range(3)])
+    if outside:
+        pos[0, :outside] = s.phi[0] + 0.01
+    p = scenes.make_particles(pos, dx, (2, 2, 2), 900.0, 0, E=2e3, nu=0.25)
+    p.rdata[nt.R_VEL:nt.R_VEL + 3] = rng.normal(0, 0.3, (3, npart))
+    p.rdata[nt.R_STRESS:nt.R_STRESS + 6] = rng.normal(0, 50.0, (6, npart))
+    return s, p
+
+
+def test_sort_bitexact():
+    s, p = random_scene(11, outside=37)
+    ctx, o = pair(s, p)
+    keys, perm = ctx.sort_keys()
+    okeys, operm = o.sort_keys(ctx.tile())
+    assert np.array_equal(keys, okeys)
+    assert np.array_equal(perm, operm)
+
+
+def test_sort_bitexact_clustered():
+    # many particles per cell and whole empty tiles
+    s, p = random_scene(12, npart=20000)
+    p.pos[:, ::3] = p.pos[:, :1]  # a third of the particles in one cell
+    ctx, o = pair(s, p)
+    keys, perm = ctx.sort_keys()
+    okeys, operm = o.sort_keys(ctx.tile())
+    assert np.array_equal(keys, okeys) and np.array_equal(perm, operm)
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_p2g_momentum(order):
+    s, p = random_scene(20 + order, order=order)
+    s.external_loads = 1
+    for d in range(3):
+        s.force_slab_lo[d] = s.plo[d] + 0.2 * (s.phi[d] - s.plo[d])
+        s.force_slab_hi[d] = s.plo[d] + 0.6 * (s.phi[d] - s.plo[d])
+        s.extforce[d] = 0.5 * (d + 1)
+    ctx, o = pair(s, p)
+    ctx.P2G_Momentum(1, 1, 1)
+    o.p2g_momentum(1, 1, 1)
+    for comp, k in [(nt.N_MASS, 1), (nt.N_VEL, 3), (nt.N_FRC, 3)]:
+        for c in range(k):
+            e = rel(ctx.nodes(comp + c), o.nodes(comp + c))
+            assert e < 1e-12, f"node comp {comp + c}: {e:.3e}"
+
+
+def test_p2g_mixed_orders():
+    # ncells < 5 on one axis: quadratic falls back to linear there
+    s, p = random_scene(31, n=(20, 4, 12), order=2)
+    assert list(s.order) == [2, 1, 2]
+    ctx, o = pair(s, p)
+    ctx.P2G_Momentum(1, 1, 1)
+    o.p2g_momentum(1, 1, 1)
+    for comp in range(7):
+        assert rel(ctx.nodes(comp), o.nodes(comp)) < 1e-12
+
+
+@pytest.mark.parametrize("bc", [nt.BC_NOSLIP, nt.BC_SLIP, nt.BC_PARTIALSLIP])
+def test_nodal_ops_and_bcs(bc):
+    s, p = random_scene(40 + bc, order=2)
+    for d in range(3):
+        s.bclo[d] = bc
+        s.bchi[d] = nt.BC_SLIP if d == 1 else bc
+        s.wall_mu_lo[d] = 0.3
+        s.wall_vel_lo[3 * d + (d + 1) % 3] = 0.05
+    ctx, o = pair(s, p)
+    dt = 1e-4
+    ctx.P2G_Momentum(1, 1, 1)
+    ctx.backup_current_velocity()
+    ctx.Nodal_Time_Update_Momentum(dt)
+    ctx.Apply_Nodal_BCs(dt, 0.0)
+    o.p2g_momentum(1, 1, 1)
+    o.backup_current_velocity()
+    o.nodal_time_update_momentum(dt)
+    o.apply_nodal_bcs(dt, 0.0)
+    for comp in [nt.N_MASS, nt.N_VEL, nt.N_VEL + 1, nt.N_VEL + 2, nt.N_DVEL, nt.N_DVEL + 1, nt.N_DVEL + 2,
+                 nt.N_MASS_OLD]:
+        assert rel(ctx.nodes(comp), o.nodes(comp)) < 1e-11, comp
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_g2p_move_volume_stress(order):
+    s, p = random_scene(50 + order, order=order)
+    p.idata[nt.I_PHASE, ::17] = 1  # rigid particles: advected only
+    ctx, o = pair(s, p)
+    dt = 2e-4
+    for x in (ctx,):
+        x.P2G_Momentum(1, 1, 1)
+        x.backup_current_velocity()
+        x.Nodal_Time_Update_Momentum(dt)
+        x.Apply_Nodal_BCs(dt, 0.0)
+        x.G2P_Momentum(1, 1, dt)
+        x.Update_MP_Positions(dt)
+        x.Update_MP_Volume()
+        x.Calculate_MP_Stress_Strain(0.0, dt)
+    o.p2g_momentum(1, 1, 1)
+    o.backup_current_velocity()
+    o.nodal_time_update_momentum(dt)
+    o.apply_nodal_bcs(dt, 0.0)
+    o.g2p_momentum(1, 1, dt)
+    o.update_mp_positions(dt)
+    o.update_mp_volume()
+    o.calculate_mp_stress_strain(0.0, dt)
+    check_particles(ctx.download(), o.download())
+
+
+def test_init_internal_forces():
+    s, p = small_dam()
+    ctx, o = pair(s, p)
+    ctx.Initialise_Internal_Forces()
+    o.init_internal_forces()
+    check_particles(ctx.download(), o.download())
+
+
+def test_time_step_cfl():
+    s, p = small_dam()
+    ctx, o = pair(s, p)
+    dt = ctx.Calculate_time_step()
+    assert dt == pytest.approx(o.calculate_time_step(), rel=1e-14)
+
+
+def run_both(specs, parts, nsteps, phi=None):
+    ctx, o = pair(specs, parts, phi)
+    ctx.Initialise_Internal_Forces()
+    o.init_internal_forces()
+    ctx.step(nsteps)
+    assert o.step(nsteps) == 0
+    return ctx, o
+
+
+def test_fused_axial_bar():
+    s, p = scenes.axial_bar(nx=32)
+    ctx, o = run_both(s, p, 50)
+    check_particles(ctx.download(), o.download())
+    t, dt, n = ctx.time()
+    to, dto, no = o.time()
+    assert n == no == 50 and t == pytest.approx(to, rel=1e-14)
+
+
+def test_fused_dam_break_quadratic():
+    s, p = small_dam()
+    ctx, o = run_both(s, p, 20)
+    check_particles(ctx.download(), o.download())
+    gd, od = ctx.diagnostics(), o.diagnostics()
+    for k in ("tke", "tse", "mass"):
+        assert gd[k] == pytest.approx(od[k], rel=1e-10, abs=1e-300), k
+
+
+def test_fused_spheres_cubic():
+    s, p = scenes.sphere_collision(n=32)
+    ctx, o = run_both(s, p, 20)
+    check_particles(ctx.download(), o.download())
+
+
+def test_fused_musl():
+    s, p = small_dam(seed=5)
+    s.stress_update_scheme = 1
+    ctx, o = run_both(s, p, 10)
+    check_particles(ctx.download(), o.download())
+
+
+def test_fused_levelset_obstacles():
+    s, p, phi = scenes.twisted_column(n=(16, 16, 48), precision=nt.PREC_FP64, n_obstacles=6)
+    ctx, o = run_both(s, p, 20, phi)
+    check_particles(ctx.download(), o.download())
+
+
+def test_fused_deterministic():
+    s, p = small_dam(seed=9)
+    a, _ = pair(s, p)
+    b, _ = pair(s, p)
+    for x in (a, b):
+        x.Initialise_Internal_Forces()
+        x.step(15)
+    pa, pb = a.download(), b.download()
+    assert np.array_equal(pa.rdata, pb.rdata) and np.array_equal(pa.pos, pb.pos)
+
+
+def test_mixed_precision_error():
+    s, p = small_dam(seed=13)
+    s64 = s.copy()
+    s.precision = nt.PREC_MIXED
+    ctx = nt.Context(s)
+    ctx.upload(p)
+    ctx.Initialise_Internal_Forces()
+    o = orc.Oracle(s64)
+    o.upload(p)
+    o.init_internal_forces()
+    ctx.step(100)
+    o.step(100)
+    g, r = ctx.download(), o.download()
+    for name, f, k in [("vel", nt.R_VEL, 3), ("stress", nt.R_STRESS, 6)]:
+        a, b = g.rdata[f:f + k], r.rdata[f:f + k]
+        l2 = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert l2 < 1e-4, f"{name}: rel L2 {l2:.3e}"
