@@ -124,13 +124,14 @@ class ClockSampler:
 
 def workload(args, precision):
     from exagoop_b200 import native as nt, scenes
+    f = args.scale
     if args.config == "dam_break":
-        s, p = scenes.dam_break(n=(256, 128, 128), size=(1.0, 0.5, 0.5), block=(0.4, 0.5, 0.3), seed=1234,
-                                precision=precision)
-        name = "dam_break_256x128x128_quadratic_tait"
+        n = (int(256 * f), int(128 * f), int(128 * f))
+        s, p = scenes.dam_break(n=n, size=(1.0, 0.5, 0.5), block=(0.4, 0.5, 0.3), seed=1234, precision=precision)
+        name = f"dam_break_{n[0]}x{n[1]}x{n[2]}_quadratic_tait"
     elif args.config == "spheres":
-        s, p = scenes.sphere_collision(n=256, precision=precision)
-        name = "sphere_collision_256^3_cubic_elastic"
+        s, p = scenes.sphere_collision(n=int(256 * f), precision=precision)
+        name = f"sphere_collision_{int(256 * f)}^3_cubic_elastic"
     else:
         s, p = scenes.axial_bar(precision=precision)
         name = "axial_bar_64x4x4_linear_elastic"
@@ -261,6 +262,7 @@ def main():
     ap.add_argument("--config", default="dam_break", choices=["dam_break", "spheres", "axial_bar"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--scale", type=float, default=1.0, help="grid scale factor (1 = the benchmark size)")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")

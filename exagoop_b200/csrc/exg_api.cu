@@ -567,6 +567,9 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
             m.mu = p->rdata[(size_t)EXG_R_VISC * n + i];
             m.model = p->idata[(size_t)EXG_I_MODEL * n + i];
             m.pad = 0;
+            if (m.model != 0 && m.model != 1)
+                return fail(ctx, EXG_ERR_UNSUPPORTED, "constitutive model " + std::to_string(m.model) +
+                                                          " (neo-Hookean) is outside this library's scope");
             auto key = std::make_tuple(m.E, m.nu, m.K, m.gamma, m.mu, m.model);
             auto it = idx.find(key);
             if (it == idx.end()) {

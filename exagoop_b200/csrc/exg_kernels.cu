@@ -487,9 +487,23 @@ struct Stc {
     static constexpr int LO = (ORD == 1) ? 0 : -1;
 };
 
-__device__ __forceinline__ void fx_add(unsigned long long *a, double v, double sc) {
-    long long q = __double2ll_rn(v * sc);
-    if (q) atomicAdd(a, (unsigned long long)q);
+// A 64-bit fixed-point accumulator kept as two 32-bit words (native
+// shared-memory atomics): the low word's returning add yields the carry
+// into the high word, so the pair always holds the exact 64-bit sum.
+__device__ __forceinline__ void fx_add(unsigned *lo, int *hi, int idx, double v, double sc) {
+    const long long q = __double2ll_rn(v * sc);
+    if (!q) return;
+    const unsigned l = (unsigned)(unsigned long long)q;
+    int h = (int)(q >> 32);
+    const unsigned old = atomicAdd(&lo[idx], l);
+    h += (old + l < old) ? 1 : 0;
+    if (h) atomicAdd(&hi[idx], h);
+}
+
+template <int W, class T>
+__device__ __forceinline__ T pick(const T (&a)[W], int i) {
+    if (W == 2) return i ? a[1] : a[0];
+    return i == 0 ? a[0] : (i == 1 ? a[1] : (i == 2 ? a[2] : a[W - 1]));
 }
 
 template <class R, int ORD, bool THERM>
@@ -500,96 +514,117 @@ __global__ void __launch_bounds__(kThreads) k_p2g(Params P, Parts<R> A, const in
     constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
     extern __shared__ __align__(16) unsigned char smraw[];
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
-    unsigned long long *acc = reinterpret_cast<unsigned long long *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
     const int B = P.B, B3 = B * B * B;
+    unsigned *acc_lo = reinterpret_cast<unsigned *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
+    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3);
     load_tables(tab);
     double sc[NCH];
 #pragma unroll
     for (int c = 0; c < NCH; ++c) sc[c] = ctl->scale[c];
-    const int nitems = ctl->n_active_tiles;
-    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
-    for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) acc[i] = 0ull;
-    __syncthreads();
-    const int t = active[w];
-    int tc[3];
-    tile_coords(P, t, tc);
-    const int org[3] = {tc[0] * P.T, tc[1] * P.T, tc[2] * P.T};
-    const int s0 = start[t], n = count[t];
     const bool fm = flags & PF_MASS, fv = flags & PF_VEL, ff = flags & PF_FORCE, fT = flags & PF_TEMP,
                fS = flags & PF_SRC;
-    for (int k = s0 + threadIdx.x; k < s0 + n; k += blockDim.x) {
-        const int p = perm[k];
-        if (A.phase[p] != 0) continue;
-        const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
-        int iv[3];
-        cell_of(P, x, iv);
-        AxisW<R, W> ax, ay, az;
-        axis_weights<R, W, LO>(*tab, P, 0, x[0], iv[0], ax);
-        axis_weights<R, W, LO>(*tab, P, 1, x[1], iv[1], ay);
-        axis_weights<R, W, LO>(*tab, P, 2, x[2], iv[2], az);
-        const int lx = iv[0] - org[0], ly = iv[1] - org[1], lz = iv[2] - org[2];
-        const R m = A.mass[p], vol = A.vol[p];
-        R mv[3], mg[3], ext[3], s[6];
-        for (int d = 0; d < 3; ++d) {
-            mv[d] = m * A.v[d][p];
-            mg[d] = m * (R)P.gravity[d];
+    // lanes of one cell sit next to each other after the sort; rotating the
+    // stencil order by lane keeps them off the same node at the same time
+    const int lane = threadIdx.x & 31;
+    const int rx = lane & (W - 1), ry = (lane / W) & (W - 1), rz = (lane / (W * W)) & (W - 1);
+    const int nitems = ctl->n_active_tiles;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) {
+            acc_lo[i] = 0u;
+            acc_hi[i] = 0;
         }
-        bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] && x[1] > P.slab_lo[1] &&
-                    x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] && x[2] < P.slab_hi[2];
-        for (int d = 0; d < 3; ++d) ext[d] = slab ? (R)P.extforce[d] : R(0);
-        for (int c = 0; c < 6; ++c) s[c] = A.sig[c][p];
-        R mcp = R(0), mcpT = R(0), mk = R(0), qv[3] = {R(0), R(0), R(0)}, VQ = R(0);
-        if (THERM) {
-            mcp = m * A.cp[p];
-            mcpT = mcp * A.T[p];
-            mk = m * A.kc[p];
-            for (int d = 0; d < 3; ++d) qv[d] = A.q[d][p];
-            VQ = vol * A.Q[p];
-        }
+        __syncthreads();
+        const int t = active[w];
+        int tc[3];
+        tile_coords(P, t, tc);
+        const int org[3] = {tc[0] * P.T, tc[1] * P.T, tc[2] * P.T};
+        const int s0 = start[t], n = count[t];
+        for (int k = s0 + threadIdx.x; k < s0 + n; k += blockDim.x) {
+            const int p = perm[k];
+            if (A.phase[p] != 0) continue;
+            const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+            int iv[3];
+            cell_of(P, x, iv);
+            AxisW<R, W> ax, ay, az;
+            axis_weights<R, W, LO>(*tab, P, 0, x[0], iv[0], ax);
+            axis_weights<R, W, LO>(*tab, P, 1, x[1], iv[1], ay);
+            axis_weights<R, W, LO>(*tab, P, 2, x[2], iv[2], az);
+            const int lx = iv[0] - org[0], ly = iv[1] - org[1], lz = iv[2] - org[2];
+            const R m = A.mass[p], vol = A.vol[p];
+            R mv[3], mg[3], ext[3], s[6];
 #pragma unroll
-        for (int sz = 0; sz < W; ++sz) {
-            if (az.w[sz] == R(0) && az.dw[sz] == R(0)) continue;
+            for (int d = 0; d < 3; ++d) {
+                mv[d] = m * A.v[d][p];
+                mg[d] = m * (R)P.gravity[d];
+            }
+            const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
+                              x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] && x[2] < P.slab_hi[2];
 #pragma unroll
-            for (int sy = 0; sy < W; ++sy) {
-                if (ay.w[sy] == R(0) && ay.dw[sy] == R(0)) continue;
-                const R wyz = ay.w[sy] * az.w[sz];
+            for (int d = 0; d < 3; ++d) ext[d] = slab ? (R)P.extforce[d] : R(0);
 #pragma unroll
-                for (int sx = 0; sx < W; ++sx) {
-                    if (ax.w[sx] == R(0) && ax.dw[sx] == R(0)) continue;
-                    const R N = ax.w[sx] * ay.w[sy] * az.w[sz];
-                    const int idx = ((lz + sz) * B + (ly + sy)) * B + (lx + sx);
-                    if (fm) fx_add(&acc[CH_M * B3 + idx], (double)(m * N), sc[CH_M]);
-                    if (fv)
-                        for (int d = 0; d < 3; ++d) fx_add(&acc[(CH_P + d) * B3 + idx], (double)(mv[d] * N), sc[CH_P + d]);
-                    if (ff || (THERM && fS)) {
-                        const R g[3] = {ax.dw[sx] * ay.w[sy] * az.w[sz], ax.w[sx] * ay.dw[sy] * az.w[sz],
-                                        ax.w[sx] * ay.w[sy] * az.dw[sz]};
-                        if (ff) {
-                            const R tv[3] = {s[0] * g[0] + s[1] * g[1] + s[2] * g[2],
-                                             s[1] * g[0] + s[3] * g[1] + s[4] * g[2],
-                                             s[2] * g[0] + s[4] * g[1] + s[5] * g[2]};
+            for (int c = 0; c < 6; ++c) s[c] = A.sig[c][p];
+            R mcp = R(0), mcpT = R(0), mk = R(0), qv[3] = {R(0), R(0), R(0)}, VQ = R(0);
+            if (THERM) {
+                mcp = m * A.cp[p];
+                mcpT = mcp * A.T[p];
+                mk = m * A.kc[p];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) qv[d] = A.q[d][p];
+                VQ = vol * A.Q[p];
+            }
+#pragma unroll
+            for (int iz = 0; iz < W; ++iz) {
+                const int sz = (iz + rz) & (W - 1);
+                const R wz = pick<W>(az.w, sz), dz = pick<W>(az.dw, sz);
+                if (wz == R(0) && dz == R(0)) continue;
+#pragma unroll
+                for (int iy = 0; iy < W; ++iy) {
+                    const int sy = (iy + ry) & (W - 1);
+                    const R wy = pick<W>(ay.w, sy), dy = pick<W>(ay.dw, sy);
+                    if (wy == R(0) && dy == R(0)) continue;
+#pragma unroll
+                    for (int ix = 0; ix < W; ++ix) {
+                        const int sx = (ix + rx) & (W - 1);
+                        const R wx = pick<W>(ax.w, sx), dx = pick<W>(ax.dw, sx);
+                        if (wx == R(0) && dx == R(0)) continue;
+                        const R N = wx * wy * wz;
+                        const int idx = ((lz + sz) * B + (ly + sy)) * B + (lx + sx);
+                        if (fm) fx_add(acc_lo, acc_hi, CH_M * B3 + idx, (double)(m * N), sc[CH_M]);
+                        if (fv) {
+#pragma unroll
                             for (int d = 0; d < 3; ++d)
-                                fx_add(&acc[(CH_F + d) * B3 + idx], (double)((mg[d] * N + ext[d] * N) + (-vol * tv[d])),
-                                       sc[CH_F + d]);
+                                fx_add(acc_lo, acc_hi, (CH_P + d) * B3 + idx, (double)(mv[d] * N), sc[CH_P + d]);
                         }
-                        if (THERM && fS) {
-                            R net = qv[0] * g[0] + qv[1] * g[1] + qv[2] * g[2];
-                            fx_add(&acc[CH_SRC * B3 + idx], (double)(net * vol + VQ * N), sc[CH_SRC]);
+                        if (ff || (THERM && fS)) {
+                            const R g[3] = {dx * wy * wz, wx * dy * wz, wx * wy * dz};
+                            if (ff) {
+                                const R tv[3] = {s[0] * g[0] + s[1] * g[1] + s[2] * g[2],
+                                                 s[1] * g[0] + s[3] * g[1] + s[4] * g[2],
+                                                 s[2] * g[0] + s[4] * g[1] + s[5] * g[2]};
+#pragma unroll
+                                for (int d = 0; d < 3; ++d)
+                                    fx_add(acc_lo, acc_hi, (CH_F + d) * B3 + idx,
+                                           (double)((mg[d] * N + ext[d] * N) + (-vol * tv[d])), sc[CH_F + d]);
+                            }
+                            if (THERM && fS) {
+                                const R net = qv[0] * g[0] + qv[1] * g[1] + qv[2] * g[2];
+                                fx_add(acc_lo, acc_hi, CH_SRC * B3 + idx, (double)(net * vol + VQ * N), sc[CH_SRC]);
+                            }
                         }
-                    }
-                    if (THERM && fT) {
-                        fx_add(&acc[CH_MC * B3 + idx], (double)(mcp * N), sc[CH_MC]);
-                        fx_add(&acc[CH_MCT * B3 + idx], (double)(mcpT * N), sc[CH_MCT]);
-                        fx_add(&acc[CH_MK * B3 + idx], (double)(mk * N), sc[CH_MK]);
+                        if (THERM && fT) {
+                            fx_add(acc_lo, acc_hi, CH_MC * B3 + idx, (double)(mcp * N), sc[CH_MC]);
+                            fx_add(acc_lo, acc_hi, CH_MCT * B3 + idx, (double)(mcpT * N), sc[CH_MCT]);
+                            fx_add(acc_lo, acc_hi, CH_MK * B3 + idx, (double)(mk * N), sc[CH_MK]);
+                        }
                     }
                 }
             }
         }
-    }
-    __syncthreads();
-    long long *dst = staging + (long long)w * NCH * B3;
-    for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) dst[i] = (long long)acc[i];
-    __syncthreads();
+        __syncthreads();
+        long long *dst = staging + (long long)w * NCH * B3;
+        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x)
+            dst[i] = (long long)((((unsigned long long)(unsigned)acc_hi[i]) << 32) + (unsigned long long)acc_lo[i]);
+        __syncthreads();
     }
 }
 
@@ -652,6 +687,7 @@ __device__ void node_bcs(const Params &P, const NodeBCArgs &bc, int i, int j, in
     // the node lies on; relvel_out persists across directions.
     {
         double rin[3] = {v[0], v[1], v[2]}, rout[3] = {v[0], v[1], v[2]};
+#pragma unroll
         for (int dir = 0; dir < 3; ++dir) {
             const bool lo = id[dir] == 0;
             const bool hi = !lo && id[dir] == P.nc[dir];
@@ -669,6 +705,7 @@ __device__ void node_bcs(const Params &P, const NodeBCArgs &bc, int i, int j, in
         }
     }
     // UDF wall velocity tables
+#pragma unroll
     for (int dir = 0; dir < 3; ++dir) {
         const double *tab = nullptr;
         int bct = -1;
@@ -726,6 +763,7 @@ __global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeB
     const double dt = ctl->dt;
     unsigned status = 0;
     double isc[NCH];
+#pragma unroll
     for (int c = 0; c < NCH; ++c) isc[c] = ctl->inv_scale[c];
     const int T = P.T;
     const int nitems = tiles ? ctl->n_touched_tiles : (int)P.ntiles;
@@ -744,36 +782,50 @@ __global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeB
         }
         if (!ok) continue;
         long long accv[NCH];
+#pragma unroll
         for (int c = 0; c < NCH; ++c) accv[c] = 0;
-        // candidate source tiles per axis
-        int srct[3][3], srcl[3][3], ns[3];
+        // Source tiles per axis: the node's own tile, plus the lower
+        // neighbour when the node lies in its high halo (l < hhi) or the
+        // upper neighbour when it lies in its low halo (l >= T - hlo); both
+        // cannot happen since hhi + hlo <= T.
+        int s1[3], l1[3], s2[3], l2[3];
+        bool h2[3];
+#pragma unroll
         for (int d = 0; d < 3; ++d) {
-            ns[d] = 0;
-            for (int dd = -1; dd <= 1; ++dd) {
-                int s = tc[d] + dd;
-                if (s < 0 || s >= P.ntile[d]) {
-                    if (!P.periodic[d]) continue;
-                    s = (s + P.ntile[d]) % P.ntile[d];
-                }
-                int loc = nid[d] - (s * T - P.hlo);
-                if (P.periodic[d]) {
-                    loc %= P.nc[d];
-                    if (loc < 0) loc += P.nc[d];
-                }
-                if (loc < 0 || loc >= B) continue;
-                srct[d][ns[d]] = s;
-                srcl[d][ns[d]] = loc;
-                ns[d]++;
+            s1[d] = tc[d];
+            l1[d] = l[d] + P.hlo;
+            h2[d] = true;
+            if (l[d] < P.hhi) {
+                s2[d] = tc[d] - 1;
+                l2[d] = l[d] + P.hlo + T;
+            } else if (l[d] >= T - P.hlo) {
+                s2[d] = tc[d] + 1;
+                l2[d] = l[d] + P.hlo - T;
+            } else {
+                s2[d] = 0;
+                l2[d] = 0;
+                h2[d] = false;
+            }
+            if (h2[d] && (s2[d] < 0 || s2[d] >= P.ntile[d])) {
+                if (P.periodic[d])
+                    s2[d] = (s2[d] + P.ntile[d]) % P.ntile[d];
+                else
+                    h2[d] = false;
             }
         }
-        for (int a = 0; a < ns[2]; ++a)
-            for (int b2 = 0; b2 < ns[1]; ++b2)
-                for (int c2 = 0; c2 < ns[0]; ++c2) {
-                    const int st = (srct[2][a] * P.ntile[1] + srct[1][b2]) * P.ntile[0] + srct[0][c2];
-                    const int sl = slot[st];
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+                for (int c2 = 0; c2 < 2; ++c2) {
+                    if ((a && !h2[2]) || (b2 && !h2[1]) || (c2 && !h2[0])) continue;
+                    const int sz = a ? s2[2] : s1[2], sy = b2 ? s2[1] : s1[1], sx = c2 ? s2[0] : s1[0];
+                    const int lz = a ? l2[2] : l1[2], ly = b2 ? l2[1] : l1[1], lx = c2 ? l2[0] : l1[0];
+                    const int sl = slot[(sz * P.ntile[1] + sy) * P.ntile[0] + sx];
                     if (sl < 0) continue;
-                    const long long base =
-                        (long long)sl * NCH * B3 + ((long long)srcl[2][a] * B + srcl[1][b2]) * B + srcl[0][c2];
+                    const long long base = (long long)sl * NCH * B3 + ((long long)lz * B + ly) * B + lx;
+#pragma unroll
                     for (int c = 0; c < NCH; ++c) accv[c] += staging[base + (long long)c * B3];
                 }
         const long long ni = ((long long)nid[2] * P.nn[1] + nid[1]) * P.nn[0] + nid[0];
@@ -1009,6 +1061,7 @@ __device__ __forceinline__ void move_particle(const Params &P, const NodeBCArgs 
             for (int d = 0; d < 3; ++d) v[d] = (R)rout[d];
         }
     }
+#pragma unroll
     for (int dir = 0; dir < 3; ++dir) {
         const bool lo = x[dir] < P.plo[dir];
         const bool hi = !lo && x[dir] > P.phi[dir];
@@ -1046,16 +1099,19 @@ template <class R>
 __device__ __forceinline__ void volume_stress(const Params &P, const Material &mt, const R E[9], R vol0, R mass,
                                               const R sr[6], R eps[6], R sig[6], R &vol, R &rho, R &J, R &pres,
                                               double dt, double asr, bool do_volume, bool do_stress) {
+    double e[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) e[q] = (double)E[q];
+    // J = det F in FP64 from F = I + E; the stored J is its rounding
+    const double det = det_IpE(e);
     if (do_volume) {
-        double e[9];
-        for (int q = 0; q < 9; ++q) e[q] = (double)E[q];
-        double det = det_IpE(e);
-        double V = (double)vol0 * det;
+        const double V = (double)vol0 * det;
         J = (R)det;
         vol = (R)V;
         rho = (R)((double)mass / V);
     }
     if (do_stress) {
+#pragma unroll
         for (int d = 0; d < 6; ++d) eps[d] += (R)dt * sr[d];
         eps[0] += (R)(dt * asr);
         eps[3] += (R)(dt * asr);
@@ -1063,7 +1119,8 @@ __device__ __forceinline__ void volume_stress(const Params &P, const Material &m
         if (mt.model == 0) {
             linear_elastic<R>(eps, sig, (R)mt.E, (R)mt.nu);
         } else if (mt.model == 1) {
-            double pj = mt.K * (pow(1.0 / (double)J, mt.gamma) - 1.0);
+            // Tait EOS p = K ((1/J)^gamma - 1) (mpm_particle_container.cpp:113-120), FP64
+            const double pj = mt.K * (pow(1.0 / det, mt.gamma) - 1.0);
             pres = (R)pj;
             newtonian<R>(sr, sig, (R)mt.mu, (R)pj);
         }
@@ -1084,7 +1141,7 @@ __device__ __forceinline__ bool all_finite(const R *a, int n) {
 // particle arrays are physically re-ordered by cell every step at no extra
 // pass.  GM_VEL updates velocity in place in A instead.
 template <class R, int ORD>
-__global__ void __launch_bounds__(kThreads) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
+__global__ void __launch_bounds__(kThreads, 2) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
                                                         const Material *mats, const int *active, const int *start,
                                                         const int *count, const int32_t *perm, Ctl *ctl, int mode) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -1096,6 +1153,13 @@ __global__ void __launch_bounds__(kThreads) k_g2p_fused(Params P, Parts<R> A, Pa
     const double asr = (time < P.applied_sr_time) ? P.applied_sr : 0.0;
     unsigned status = 0;
     const bool upd_vel = (mode != GM_STRAIN);
+    // running per-thread maxima of the P2G bounds (float is enough for a
+    // power-of-two scale with a factor-2 margin; rounded up on conversion)
+    float run_b[CH_ALL];
+#pragma unroll
+    for (int c = 0; c < CH_ALL; ++c) run_b[c] = 0.0f;
+    double run_dt = 1.7976931348623157e308;
+    bool red = false;
     const int nitems = ctl->n_active_tiles;
     for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
     const int t = active[w];
@@ -1116,121 +1180,138 @@ __global__ void __launch_bounds__(kThreads) k_g2p_fused(Params P, Parts<R> A, Pa
     }
     __syncthreads();
     const int s0 = start[t], n = count[t];
-    const int iters = (n + blockDim.x - 1) / blockDim.x;
-    for (int it = 0; it < iters; ++it) {
-        const int k = s0 + it * blockDim.x + threadIdx.x;
-        const bool live = k < s0 + n;
-        double bnd[CH_ALL] = {};
-        double dtp = 0.0;
-        bool red = false;
-        if (live) {
-            const int p = perm[k];
-            const int phase = A.phase[p];
-            double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
-            R v[3], vp[3];
-            for (int d = 0; d < 3; ++d) {
-                v[d] = A.v[d][p];
-                vp[d] = A.vp[d][p];
-            }
-            if (mode == GM_VEL) {
-                if (phase == 0) {
-                    int iv[3];
-                    cell_of(P, x, iv);
-                    R E[9], sr[6];
-                    g2p_particle<R, ORD>(*tab, P, na, x, iv, true, false, v, vp, E, sr, dt);
-                    for (int d = 0; d < 3; ++d) {
-                        A.v[d][p] = v[d];
-                        A.vp[d][p] = vp[d];
-                    }
-                }
-            } else {
-                R E[9], sr[6], eps[6], sig[6];
-                for (int q = 0; q < 9; ++q) E[q] = A.E[q][p];
-                for (int c = 0; c < 6; ++c) {
-                    sr[c] = A.sr[c][p];
-                    eps[c] = A.eps[c][p];
-                    sig[c] = A.sig[c][p];
-                }
-                R vol = A.vol[p], rho = A.rho[p], J = A.J[p], pres = A.pres[p];
-                const R mass = A.mass[p], vol0 = A.vol0[p];
-                const int mi = A.mat[p];
-                if (phase == 0) {
-                    int iv[3];
-                    cell_of(P, x, iv);
-                    g2p_particle<R, ORD>(*tab, P, na, x, iv, upd_vel, true, v, vp, E, sr, dt);
-                }
-                move_particle<R>(P, bc, phase, x, v, vp, dt, status);
-                // Redistribute's periodic wrap
-                for (int d = 0; d < 3; ++d)
-                    if (P.periodic[d]) {
-                        double L = P.phi[d] - P.plo[d];
-                        if (x[d] >= P.phi[d])
-                            x[d] -= L;
-                        else if (x[d] < P.plo[d])
-                            x[d] += L;
-                    }
-                const Material mt = mats[mi];
-                if (phase == 0) {
-                    volume_stress<R>(P, mt, E, vol0, mass, sr, eps, sig, vol, rho, J, pres, dt, asr, true, true);
-                    if (!all_finite(v, 3) || !all_finite(sig, 6) || !isfinite((double)J)) status |= ST_NAN;
-                    // reductions for the next step
-                    int iv2[3];
-                    cell_of(P, x, iv2);
-                    bool in = true;
-                    for (int d = 0; d < 3; ++d) in = in && iv2[d] >= 0 && iv2[d] < P.nc[d];
-                    if (in) {
-                        double vd[3] = {(double)v[0], (double)v[1], (double)v[2]};
-                        double sd[6];
-                        for (int c = 0; c < 6; ++c) sd[c] = (double)sig[c];
-                        double q[3] = {0, 0, 0}, cp = 0, T = 0, kc = 0, Q = 0;
-                        if (P.use_temp) {
-                            for (int d = 0; d < 3; ++d) q[d] = (double)A.q[d][p];
-                            cp = A.cp[p];
-                            T = A.T[p];
-                            kc = A.kc[p];
-                            Q = A.Q[p];
-                        }
-                        particle_bounds<R>(P, mt, (double)mass, vd, (double)vol, sd, (double)rho, cp, T, kc, q, Q,
-                                           bnd, dtp);
-                        red = true;
-                    }
-                }
-                // write B at the sorted position k
+    for (int k = s0 + threadIdx.x; k < s0 + n; k += blockDim.x) {
+        const int p = perm[k];
+        const int phase = A.phase[p];
+        double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+        R v[3], vp[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            v[d] = A.v[d][p];
+            vp[d] = A.vp[d][p];
+        }
+        if (mode == GM_VEL) {
+            if (phase == 0) {
+                int iv[3];
+                cell_of(P, x, iv);
+                R E[9], sr[6];
+                g2p_particle<R, ORD>(*tab, P, na, x, iv, true, false, v, vp, E, sr, dt);
+#pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    Bo.x[d][k] = x[d];
-                    Bo.v[d][k] = v[d];
-                    Bo.vp[d][k] = vp[d];
+                    A.v[d][p] = v[d];
+                    A.vp[d][p] = vp[d];
                 }
-                for (int c = 0; c < 6; ++c) {
-                    Bo.sr[c][k] = sr[c];
-                    Bo.eps[c][k] = eps[c];
-                    Bo.sig[c][k] = sig[c];
-                }
-                for (int q = 0; q < 9; ++q) Bo.E[q][k] = E[q];
-                Bo.vol[k] = vol;
-                Bo.rho[k] = rho;
-                Bo.J[k] = J;
-                Bo.pres[k] = pres;
-                Bo.mass[k] = mass;
-                Bo.vol0[k] = vol0;
-                Bo.radius[k] = A.radius[p];
-                Bo.yacc[k] = A.yacc[p];
-                Bo.mat[k] = mi;
-                Bo.phase[k] = (uint8_t)phase;
-                Bo.rigid[k] = A.rigid[p];
-                Bo.pid[k] = A.pid[p];
+            }
+            continue;
+        }
+        R E[9], sr[6], eps[6], sig[6];
+        R vol, rho, J, pres;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) E[q] = A.E[q][p];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) eps[c] = A.eps[c][p];
+        pres = A.pres[p];
+        if (phase != 0) {
+            // rigid particles are only advected: keep their stored fields
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                sr[c] = A.sr[c][p];
+                sig[c] = A.sig[c][p];
+            }
+            vol = A.vol[p];
+            rho = A.rho[p];
+            J = A.J[p];
+        }
+        const R mass = A.mass[p], vol0 = A.vol0[p];
+        const int mi = A.mat[p];
+        if (phase == 0) {
+            int iv[3];
+            cell_of(P, x, iv);
+            g2p_particle<R, ORD>(*tab, P, na, x, iv, upd_vel, true, v, vp, E, sr, dt);
+        }
+        move_particle<R>(P, bc, phase, x, v, vp, dt, status);
+        // Redistribute's periodic wrap
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (P.periodic[d]) {
+                const double L = P.phi[d] - P.plo[d];
+                if (x[d] >= P.phi[d])
+                    x[d] -= L;
+                else if (x[d] < P.plo[d])
+                    x[d] += L;
+            }
+        const Material mt = mats[mi];
+        if (phase == 0) {
+            volume_stress<R>(P, mt, E, vol0, mass, sr, eps, sig, vol, rho, J, pres, dt, asr, true, true);
+            if (!all_finite(v, 3) || !all_finite(sig, 6) || !isfinite((double)J)) status |= ST_NAN;
+            // reductions for the next step (running per thread)
+            int iv2[3];
+            cell_of(P, x, iv2);
+            const bool in = iv2[0] >= 0 && iv2[0] < P.nc[0] && iv2[1] >= 0 && iv2[1] < P.nc[1] && iv2[2] >= 0 &&
+                            iv2[2] < P.nc[2];
+            if (in) {
+                const double vd[3] = {(double)v[0], (double)v[1], (double)v[2]};
+                double sd[6];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) sd[c] = (double)sig[c];
+                double q[3] = {0, 0, 0}, cp = 0, T = 0, kc = 0, Q = 0;
                 if (P.use_temp) {
-                    Bo.T[k] = A.T[p];
-                    Bo.cp[k] = A.cp[p];
-                    Bo.kc[k] = A.kc[p];
-                    Bo.Q[k] = A.Q[p];
-                    for (int d = 0; d < 3; ++d) Bo.q[d][k] = A.q[d][p];
+                    for (int d = 0; d < 3; ++d) q[d] = (double)A.q[d][p];
+                    cp = A.cp[p];
+                    T = A.T[p];
+                    kc = A.kc[p];
+                    Q = A.Q[p];
                 }
+                double bnd[CH_ALL], dtp;
+                particle_bounds<R>(P, mt, (double)mass, vd, (double)vol, sd, (double)rho, cp, T, kc, q, Q, bnd, dtp);
+#pragma unroll
+                for (int c = 0; c < CH_ALL; ++c) run_b[c] = fmaxf(run_b[c], __double2float_ru(bnd[c]));
+                run_dt = fmin(run_dt, dtp);
+                red = true;
             }
         }
-        if (mode != GM_VEL) block_reduce_push(&ctl->bound_bits[0], &ctl->dtmin_bits, bnd, dtp, red);
-        __syncthreads();
+        // write B at the sorted position k
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            Bo.x[d][k] = x[d];
+            Bo.v[d][k] = v[d];
+            Bo.vp[d][k] = vp[d];
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            Bo.sr[c][k] = sr[c];
+            Bo.eps[c][k] = eps[c];
+            Bo.sig[c][k] = sig[c];
+        }
+#pragma unroll
+        for (int q = 0; q < 9; ++q) Bo.E[q][k] = E[q];
+        Bo.vol[k] = vol;
+        Bo.rho[k] = rho;
+        Bo.J[k] = J;
+        Bo.pres[k] = pres;
+        Bo.mass[k] = mass;
+        Bo.vol0[k] = vol0;
+        Bo.radius[k] = A.radius[p];
+        Bo.yacc[k] = A.yacc[p];
+        Bo.mat[k] = mi;
+        Bo.phase[k] = (uint8_t)phase;
+        Bo.rigid[k] = A.rigid[p];
+        Bo.pid[k] = A.pid[p];
+        if (P.use_temp) {
+            Bo.T[k] = A.T[p];
+            Bo.cp[k] = A.cp[p];
+            Bo.kc[k] = A.kc[p];
+            Bo.Q[k] = A.Q[p];
+            for (int d = 0; d < 3; ++d) Bo.q[d][k] = A.q[d][p];
+        }
     }
+    __syncthreads();
+    }
+    if (mode != GM_VEL) {
+        double rb[CH_ALL];
+#pragma unroll
+        for (int c = 0; c < CH_ALL; ++c) rb[c] = (double)run_b[c];
+        block_reduce_push(&ctl->bound_bits[0], &ctl->dtmin_bits, rb, run_dt, red);
     }
     if (status) atomicOr(&ctl->status, status);
 }

@@ -364,6 +364,27 @@ void ls_eval(const orc_ctx *o, const std::vector<double> &phi, const double x[3]
         for (int d = 0; d < 3; ++d) grad[d] = g[d];
 }
 
+// get_deformation_gradient_tensor (interpolants.H:1732-1787): F <- (I + gv dt) F
+// unless |gv|^2 >= 1e10.
+void defgrad_update(double F[9], const double gv[3][3], double dt) {
+    double nrm = 0.0;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) nrm += gv[a][b] * gv[a][b];
+    if (nrm >= 1.0e10) return;
+    double L[3][3], Fo[3][3];
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            L[a][b] = (a == b) ? 1.0 + gv[a][b] * dt : gv[a][b] * dt;
+            Fo[a][b] = F[3 * a + b];
+        }
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            double acc = 0.0;
+            for (int c = 0; c < 3; ++c) acc += L[a][c] * Fo[c][b];
+            F[3 * a + b] = acc;
+        }
+}
+
 void linear_elastic(const double eps[6], double sig[6], double E, double v) {  // constitutive_models.H:21-54
     double const1 = E / (1.0 + v) / (1.0 - 2.0 * v);
     double const2 = E / (1.0 + v);
@@ -771,23 +792,11 @@ void orc_g2p_momentum(orc_ctx *o, int update_vel, int update_strainrate, double 
                             for (int d2 = 0; d2 < 3; ++d2) gv[d1][d2] += v * g[d2];
                         }
                     }
-            // get_deformation_gradient_tensor (interpolants.H:1732-1787)
-            double nrm = 0.0;
-            for (int a = 0; a < 3; a++)
-                for (int b = 0; b < 3; b++) nrm += gv[a][b] * gv[a][b];
-            if (!(nrm >= 1.0e10)) {
-                double L[3][3], F[3][3];
-                for (int a = 0; a < 3; a++)
-                    for (int b = 0; b < 3; b++) {
-                        L[a][b] = (a == b) ? 1.0 + gv[a][b] * dt : gv[a][b] * dt;
-                        F[a][b] = o->R(EXG_R_DEFGRAD + 3 * a + b, p);
-                    }
-                for (int a = 0; a < 3; ++a)
-                    for (int b = 0; b < 3; ++b) {
-                        double acc = 0.0;
-                        for (int c = 0; c < 3; ++c) acc += L[a][c] * F[c][b];
-                        o->R(EXG_R_DEFGRAD + 3 * a + b, p) = acc;
-                    }
+            {
+                double F[9];
+                for (int q = 0; q < 9; ++q) F[q] = o->R(EXG_R_DEFGRAD + q, p);
+                defgrad_update(F, gv, dt);
+                for (int q = 0; q < 9; ++q) o->R(EXG_R_DEFGRAD + q, p) = F[q];
             }
             int ind = 0;
             for (int d1 = 0; d1 < 3; ++d1)
@@ -1379,6 +1388,12 @@ int orc_fn_applybc(const double *in, double *out, double mu, const double *n, in
 }
 void orc_fn_linear_elastic(const double *eps, double *sig, double E, double nu) { linear_elastic(eps, sig, E, nu); }
 void orc_fn_newtonian(const double *ed, double *sig, double mu, double p) { newtonian_fluid(ed, sig, mu, p); }
+void orc_fn_defgrad(double *F, const double *g, double dt) {
+    double gv[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) gv[a][b] = g[3 * a + b];
+    defgrad_update(F, gv, dt);
+}
 double orc_fn_levelset(orc_ctx *o, int body, const double *x, double *grad) {
     double v;
     ls_eval(o, o->ls[body], x, &v, grad);

@@ -92,7 +92,7 @@ def test_p2g_momentum(order):
     for comp, k in [(nt.N_MASS, 1), (nt.N_VEL, 3), (nt.N_FRC, 3)]:
         for c in range(k):
             e = rel(ctx.nodes(comp + c), o.nodes(comp + c))
-            assert e < 1e-12, f"node comp {comp + c}: {e:.3e}"
+            assert e < TOL64, f"node comp {comp + c}: {e:.3e}"
 
 
 def test_p2g_mixed_orders():
@@ -103,7 +103,7 @@ def test_p2g_mixed_orders():
     ctx.P2G_Momentum(1, 1, 1)
     o.p2g_momentum(1, 1, 1)
     for comp in range(7):
-        assert rel(ctx.nodes(comp), o.nodes(comp)) < 1e-12
+        assert rel(ctx.nodes(comp), o.nodes(comp)) < TOL64
 
 
 @pytest.mark.parametrize("bc", [nt.BC_NOSLIP, nt.BC_SLIP, nt.BC_PARTIALSLIP])
@@ -126,7 +126,7 @@ def test_nodal_ops_and_bcs(bc):
     o.apply_nodal_bcs(dt, 0.0)
     for comp in [nt.N_MASS, nt.N_VEL, nt.N_VEL + 1, nt.N_VEL + 2, nt.N_DVEL, nt.N_DVEL + 1, nt.N_DVEL + 2,
                  nt.N_MASS_OLD]:
-        assert rel(ctx.nodes(comp), o.nodes(comp)) < 1e-11, comp
+        assert rel(ctx.nodes(comp), o.nodes(comp)) < TOL64, comp
 
 
 @pytest.mark.parametrize("order", [1, 2, 3])
