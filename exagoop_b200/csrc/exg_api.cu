@@ -50,9 +50,11 @@ int ilog2(int v) {
     return s;
 }
 
-void build_params(Ctx &c) {
-    const exg_specs &s = c.specs;
-    Params &P = c.P;
+}  // namespace
+
+namespace exg {
+// Kernel parameters of a run specification.
+void build_params_for(const exg_specs &s, Params &P) {
     std::memset(&P, 0, sizeof(P));
     for (int d = 0; d < 3; ++d) {
         P.plo[d] = s.plo[d];
@@ -118,6 +120,11 @@ void build_params(Ctx &c) {
         P.ntile[d] = s.periodic[d] ? s.ncells[d] / T : (s.ncells[d] + 1 + T - 1) / T;
     P.ntiles = (long long)P.ntile[0] * P.ntile[1] * P.ntile[2];
 }
+}  // namespace exg
+
+namespace {
+
+void build_params(Ctx &c) { build_params_for(c.specs, c.P); }
 
 std::string validate(const exg_specs &s) {
     for (int d = 0; d < 3; ++d) {
@@ -474,6 +481,7 @@ int exg_ctx_create(const exg_specs *specs, int device, exg_ctx **out) {
         c.sb.slot = dalloc<int>(nt);
         c.sb.touched = dalloc<int>(nt);
         c.sb.touched_step = dalloc<long long>(nt);
+        c.sb.cell_start = dalloc<int>((size_t)nt * (c.P.T * c.P.T * c.P.T + 1));
         EXG_CUDA_OK(cudaMemset(c.sb.touched_step, 0xff, sizeof(long long) * nt));  // -1: never
         EXG_CUDA_OK(cudaMemset(c.sb.slot, 0xff, sizeof(int) * nt));
         c.nch = specs->use_temp ? CH_ALL : CH_MOM_END;
@@ -513,7 +521,7 @@ int exg_ctx_destroy(exg_ctx *ctx) {
     for (auto &row : c.udf_tab)
         for (double *p : row) cudaFree(p);
     void *bufs[] = {c.sb.key, c.sb.perm, c.sb.bucket, c.sb.tile_count, c.sb.tile_fill, c.sb.tile_start,
-                    c.sb.active, c.sb.slot, c.sb.touched, c.sb.touched_step, c.staging, c.ctl,
+                    c.sb.active, c.sb.slot, c.sb.touched, c.sb.touched_step, c.sb.cell_start, c.staging, c.ctl,
                     c.bounds_cur, c.bounds2, c.dtmin2, c.mat_dev, c.diag_dev};
     for (void *p : bufs) cudaFree(p);
     if (c.ctl_host) cudaFreeHost(c.ctl_host);

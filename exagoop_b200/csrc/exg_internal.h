@@ -33,6 +33,7 @@ struct SortBufs {
     int *slot = nullptr;         // [ntiles] index in active list or -1
     int *touched = nullptr;      // [ntiles] tiles whose nodes the nodal kernel writes
     long long *touched_step = nullptr;  // [ntiles] last step the tile was touched
+    int *cell_start = nullptr;   // [ntiles][T^3 + 1] per-cell particle ranges of each non-empty tile
 };
 
 struct Ctx;

@@ -10,6 +10,7 @@
 // graph without a host round trip.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
 #include "exg_internal.h"
 
@@ -275,7 +276,7 @@ __global__ void k_scatter(long long n, const uint32_t *key, int tshift3, const i
 constexpr int kSortCap = 12288;
 __global__ void __launch_bounds__(kThreads) k_tile_sort(const int *active, const int *start, const int *count,
                                                         const uint32_t *key, const int32_t *bucket, int32_t *scratch,
-                                                        int32_t *perm, int ncell, Ctl *ctl) {
+                                                        int32_t *perm, int *cell_start, int ncell, Ctl *ctl) {
     extern __shared__ int sm[];
     int *cnt = sm, *cst = sm + ncell, *fil = sm + 2 * ncell, *ent_s = sm + 3 * ncell;
     __shared__ int sh[34];
@@ -322,7 +323,14 @@ __global__ void __launch_bounds__(kThreads) k_tile_sort(const int *active, const
             for (int r = b; r < e; ++r) rank += (ent[r] < i);
             perm[s0 + b + rank] = i;
         }
-        if (threadIdx.x == 0) atomicMax(&ctl->maxppc, smax);
+        // cell ranges of this tile (relative to the tile start), for the
+        // per-cell P2G
+        int *cs = cell_start + (long long)w * (ncell + 1);
+        for (int c = threadIdx.x; c < ncell; c += blockDim.x) cs[c] = cst[c];
+        if (threadIdx.x == 0) {
+            cs[ncell] = n;
+            atomicMax(&ctl->maxppc, smax);
+        }
         __syncthreads();
     }
 }
@@ -362,7 +370,8 @@ __global__ void k_scales(Ctl *ctl, int stencil_cells, const unsigned long long *
     if (S > 0.0 && S < 1e300) {
         int ex;
         frexp(S, &ex);  // S < 2^ex
-        sc = ldexp(1.0, 61 - ex);
+        // 2^e stays inside FP32's range; a channel this small contributes 0
+        sc = ldexp(1.0, max(-100, min(100, 61 - ex)));
     }
     ctl->scale[c] = sc;
     ctl->inv_scale[c] = 1.0 / sc;
@@ -617,6 +626,237 @@ __global__ void __launch_bounds__(kThreads) k_p2g(Params P, Parts<R> A, const in
                             fx_add(acc_lo, acc_hi, CH_MK * B3 + idx, (double)(mk * N), sc[CH_MK]);
                         }
                     }
+                }
+            }
+        }
+        __syncthreads();
+        long long *dst = staging + (long long)w * NCH * B3;
+        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x)
+            dst[i] = (long long)((((unsigned long long)(unsigned)acc_hi[i]) << 32) + (unsigned long long)acc_lo[i]);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- K2 per-cell P2G
+// The same deposit with one thread per cell: the thread walks its cell's
+// particles (contiguous after the sort) in storage order and accumulates
+// their contributions to one z-slice of the cell's stencil in registers;
+// only the per-cell sums go to shared memory, as 64-bit fixed point.  The
+// summation order inside a cell is fixed and the cross-cell sums are exact,
+// so the result is deterministic; shared-memory atomics drop by the
+// particles-per-cell factor and lanes never collide (a warp's lanes own
+// different cells and add the same stencil offset at the same time).
+template <class R>
+__device__ __forceinline__ long long to_fixed(R v, R sc);
+template <>
+__device__ __forceinline__ long long to_fixed<float>(float v, float sc) {
+    return __float2ll_rn(v * sc);
+}
+template <>
+__device__ __forceinline__ long long to_fixed<double>(double v, double sc) {
+    return __double2ll_rn(v * sc);
+}
+
+template <class R>
+__device__ __forceinline__ void fx_add_r(unsigned *lo, int *hi, int idx, R v, R sc) {
+    const long long q = to_fixed<R>(v, sc);
+    if (!q) return;
+    const unsigned l = (unsigned)(unsigned long long)q;
+    int h = (int)(q >> 32);
+    const unsigned old = atomicAdd(&lo[idx], l);
+    h += (old + l < old) ? 1 : 0;
+    if (h) atomicAdd(&hi[idx], h);
+}
+
+// Per-axis weights of a cell whose stencil nodes are all interior (shape
+// type 3): the polynomial piece of each stencil offset is fixed (cubic) or
+// picked by f < 1/2 (quadratic); same coefficients as the tables.
+template <class R, int ORD>
+__device__ __forceinline__ void axis_weights_interior(const Params &P, int d, double x, int i,
+                                                      AxisW<R, Stc<ORD>::W> &a) {
+    const R f = (R)((x - (P.plo[d] + i * P.dx[d])) * P.dxi[d]);
+    const R dxinv = (R)P.dxi[d];
+    if (ORD == 1) {
+        a.w[0] = R(1) - f;
+        a.w[1] = f;
+        a.dw[0] = -dxinv;
+        a.dw[1] = dxinv;
+    } else if (ORD == 2) {
+        // type-3 quadratic pieces: p0 = .5z^2+1.5z+1.125, p1 = -z^2+.75, p2 = .5z^2-1.5z+1.125
+        R z = f + R(1);
+        const bool lo = f < R(0.5);
+        a.w[0] = lo ? (R(0.5) * z * z + R(-1.5) * z + R(1.125)) : R(0);
+        a.dw[0] = lo ? (z - R(1.5)) * dxinv : R(0);
+        z = f;
+        a.w[1] = lo ? (R(-1) * z * z + R(0) * z + R(0.75)) : (R(0.5) * z * z + R(-1.5) * z + R(1.125));
+        a.dw[1] = (lo ? (R(-2) * z) : (z - R(1.5))) * dxinv;
+        z = f - R(1);
+        a.w[2] = lo ? (R(0.5) * z * z + R(1.5) * z + R(1.125)) : (R(-1) * z * z + R(0) * z + R(0.75));
+        a.dw[2] = (lo ? (z + R(1.5)) : (R(-2) * z)) * dxinv;
+        z = f - R(2);
+        a.w[3] = lo ? R(0) : (R(0.5) * z * z + R(1.5) * z + R(1.125));
+        a.dw[3] = lo ? R(0) : (z + R(1.5)) * dxinv;
+    } else {
+        // type-3 cubic pieces, interval 3 - s for stencil slot s
+        const R o6 = (R)kOneBySix, t3 = (R)kTwoByThree, f3 = (R)kFourByThree;
+        R z = f + R(1), z2 = z * z;
+        a.w[0] = -o6 * (z2 * z) + R(1) * z2 + R(-2) * z + f3;
+        a.dw[0] = (R(-0.5) * z2 + R(2) * z + R(-2)) * dxinv;
+        z = f;
+        z2 = z * z;
+        a.w[1] = R(0.5) * (z2 * z) + R(-1) * z2 + R(0) * z + t3;
+        a.dw[1] = (R(1.5) * z2 + R(-2) * z + R(0)) * dxinv;
+        z = f - R(1);
+        z2 = z * z;
+        a.w[2] = R(-0.5) * (z2 * z) + R(-1) * z2 + R(0) * z + t3;
+        a.dw[2] = (R(-1.5) * z2 + R(-2) * z + R(0)) * dxinv;
+        z = f - R(2);
+        z2 = z * z;
+        a.w[3] = o6 * (z2 * z) + R(1) * z2 + R(2) * z + f3;
+        a.dw[3] = (R(0.5) * z2 + R(2) * z + R(2)) * dxinv;
+    }
+}
+
+template <class R, int ORD>
+__device__ __forceinline__ void cell_axis_weights(const SplineTables &tab, const Params &P, int d, double x, int i,
+                                                  bool interior, AxisW<R, Stc<ORD>::W> &a) {
+    if (ORD != 0 && interior)
+        axis_weights_interior<R, ORD>(P, d, x, i, a);
+    else
+        axis_weights<R, Stc<ORD>::W, Stc<ORD>::LO>(tab, P, d, x, i, a);
+}
+
+constexpr int kCellThreads = 128;
+
+template <class R, int ORD, bool THERM>
+__global__ void __launch_bounds__(kCellThreads) k_p2g_cell(Params P, Parts<R> A, const int *active, const int *start,
+                                                           const int *cell_start, const int32_t *perm,
+                                                           long long *staging, Ctl *ctl, int flags) {
+    constexpr int W = Stc<ORD>::W;
+    constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
+    // y rows of the stencil slice accumulated per pass (register budget)
+    constexpr int ROWS = (sizeof(R) == 8) ? 1 : ((THERM && W == 4) ? 2 : W);
+    extern __shared__ __align__(16) unsigned char smraw[];
+    SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
+    const int B = P.B, B3 = B * B * B, T = P.T, T3 = T * T * T;
+    unsigned *acc_lo = reinterpret_cast<unsigned *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
+    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3);
+    load_tables(tab);
+    R sc[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) sc[c] = (R)ctl->scale[c];
+    const bool fm = flags & PF_MASS, fv = flags & PF_VEL, ff = flags & PF_FORCE, fT = flags & PF_TEMP,
+               fS = flags & PF_SRC;
+    R grav[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) grav[d] = (R)P.gravity[d];
+    const int nitems = ctl->n_active_tiles;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) {
+            acc_lo[i] = 0u;
+            acc_hi[i] = 0;
+        }
+        __syncthreads();
+        const int t = active[w];
+        int tc[3];
+        tile_coords(P, t, tc);
+        const int s0 = start[t];
+        const int *cs = cell_start + (long long)w * (T3 + 1);
+        for (int c = threadIdx.x; c < T3; c += blockDim.x) {
+            const int ka = cs[c], kb = cs[c + 1];
+            if (ka == kb) continue;
+            const int lx = c % T, ly = (c / T) % T, lz = c / (T * T);
+            const int iv[3] = {tc[0] * T + lx, tc[1] * T + ly, tc[2] * T + lz};
+            bool inter[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                inter[d] = (ORD == 1) || P.periodic[d] || (iv[d] >= 3 && iv[d] <= P.nc[d] - 4);
+            for (int sz = 0; sz < W; ++sz) {
+#pragma unroll
+                for (int sy0 = 0; sy0 < W; sy0 += ROWS) {
+                    R acc[ROWS][W][NCH];
+#pragma unroll
+                    for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+                        for (int sx = 0; sx < W; ++sx)
+#pragma unroll
+                            for (int ch = 0; ch < NCH; ++ch) acc[r][sx][ch] = R(0);
+                    bool any = false;
+                    for (int k = ka; k < kb; ++k) {
+                        const int p = perm[s0 + k];
+                        if (A.phase[p] != 0) continue;
+                        const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+                        AxisW<R, W> az;
+                        cell_axis_weights<R, ORD>(*tab, P, 2, x[2], iv[2], inter[2], az);
+                        const R wz = pick<W>(az.w, sz), dzw = pick<W>(az.dw, sz);
+                        if (wz == R(0) && dzw == R(0)) continue;
+                        any = true;
+                        AxisW<R, W> ax, ay;
+                        cell_axis_weights<R, ORD>(*tab, P, 0, x[0], iv[0], inter[0], ax);
+                        cell_axis_weights<R, ORD>(*tab, P, 1, x[1], iv[1], inter[1], ay);
+                        const R m = A.mass[p], vol = A.vol[p];
+                        R mv[3], bf[3], s[6];
+                        const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
+                                          x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] &&
+                                          x[2] < P.slab_hi[2];
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            mv[d] = m * A.v[d][p];
+                            bf[d] = m * grav[d];
+                        }
+#pragma unroll
+                        for (int c6 = 0; c6 < 6; ++c6) s[c6] = -vol * A.sig[c6][p];
+                        R ext[3];
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) ext[d] = slab ? (R)P.extforce[d] : R(0);
+                        R mcp = R(0), mcpT = R(0), mk = R(0), qv[3] = {R(0), R(0), R(0)}, VQ = R(0);
+                        if (THERM) {
+                            mcp = m * A.cp[p];
+                            mcpT = mcp * A.T[p];
+                            mk = m * A.kc[p];
+#pragma unroll
+                            for (int d = 0; d < 3; ++d) qv[d] = vol * A.q[d][p];
+                            VQ = vol * A.Q[p];
+                        }
+#pragma unroll
+                        for (int r = 0; r < ROWS; ++r) {
+                            const R wy = ay.w[sy0 + r], dyw = ay.dw[sy0 + r];
+                            const R wyz = wy * wz;
+#pragma unroll
+                            for (int sx = 0; sx < W; ++sx) {
+                                const R N = ax.w[sx] * wyz;
+                                R *a = acc[r][sx];
+                                if (fm) a[CH_M] += m * N;
+                                if (fv) {
+#pragma unroll
+                                    for (int d = 0; d < 3; ++d) a[CH_P + d] += mv[d] * N;
+                                }
+                                if (ff || (THERM && fS)) {
+                                    const R g0 = ax.dw[sx] * wyz, g1 = ax.w[sx] * dyw * wz, g2 = ax.w[sx] * wy * dzw;
+                                    if (ff) {
+                                        a[CH_F + 0] += (bf[0] * N + ext[0] * N) + (s[0] * g0 + s[1] * g1 + s[2] * g2);
+                                        a[CH_F + 1] += (bf[1] * N + ext[1] * N) + (s[1] * g0 + s[3] * g1 + s[4] * g2);
+                                        a[CH_F + 2] += (bf[2] * N + ext[2] * N) + (s[2] * g0 + s[4] * g1 + s[5] * g2);
+                                    }
+                                    if (THERM && fS) a[CH_SRC] += (qv[0] * g0 + qv[1] * g1 + qv[2] * g2) + VQ * N;
+                                }
+                                if (THERM && fT) {
+                                    a[CH_MC] += mcp * N;
+                                    a[CH_MCT] += mcpT * N;
+                                    a[CH_MK] += mk * N;
+                                }
+                            }
+                        }
+                    }
+                    if (!any) continue;
+#pragma unroll
+                    for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+                        for (int sx = 0; sx < W; ++sx) {
+                            const int idx = ((lz + sz) * B + (ly + sy0 + r)) * B + (lx + sx);
+#pragma unroll
+                            for (int ch = 0; ch < NCH; ++ch) fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, acc[r][sx][ch], sc[ch]);
+                        }
                 }
             }
         }
@@ -1606,7 +1846,8 @@ void launch_sort_rest(Ctx &c, bool touched_list) {
     static int sgrid = 0;
     if (!sgrid) sgrid = persistent_grid(k_tile_sort, sm);
     k_tile_sort<<<sgrid, kThreads, sm, c.stream>>>(c.sb.active, c.sb.tile_start, c.sb.tile_count, c.sb.key,
-                                                    c.sb.bucket, c.sb.bucket + c.cap, c.sb.perm, ncell, c.ctl);
+                                                    c.sb.bucket, c.sb.bucket + c.cap, c.sb.perm, c.sb.cell_start, ncell,
+                                                    c.ctl);
     if (touched_list)
         k_touched<<<nblocks(c.P.ntiles), kThreads, 0, c.stream>>>(c.P, c.sb.tile_count, c.sb.touched,
                                                                   c.sb.touched_step, c.ctl);
@@ -1649,7 +1890,33 @@ void EXG_SFX(launch_state_reduce)(Ctx &c, unsigned long long *bounds, unsigned l
 }
 
 template <class R, int ORD, bool TH>
+static void p2g_cell_t(Ctx &c, int flags) {
+    const int NCH = TH ? CH_ALL : CH_MOM_END;
+    const int B3 = c.P.B * c.P.B * c.P.B;
+    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * NCH * B3;
+    auto kern = k_p2g_cell<R, ORD, TH>;
+    EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    static int grid = 0;
+    static size_t gsm = 0;
+    if (!grid || gsm != sm) {
+        int dev = 0, nsm = 0, per = 0;
+        EXG_CUDA_OK(cudaGetDevice(&dev));
+        EXG_CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        EXG_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kCellThreads, sm));
+        grid = nsm * (per < 1 ? 1 : per);
+        gsm = sm;
+    }
+    kern<<<grid, kCellThreads, sm, c.stream>>>(c.P, c.A<R>(), c.sb.active, c.sb.tile_start, c.sb.cell_start,
+                                               c.sb.perm, c.staging, c.ctl, flags);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+template <class R, int ORD, bool TH>
 static void p2g_t(Ctx &c, int flags) {
+    if (!std::getenv("EXG_P2G_ATOMIC")) {
+        p2g_cell_t<R, ORD, TH>(c, flags);
+        return;
+    }
     const int NCH = TH ? CH_ALL : CH_MOM_END;
     const int B3 = c.P.B * c.P.B * c.P.B;
     size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * NCH * B3;
@@ -1773,5 +2040,7 @@ void EXG_SFX(launch_diag)(Ctx &c, double *out_dev) {
     k_diag_final<<<1, 32, 0, c.stream>>>(part, nb, out_dev);
     EXG_CUDA_OK(cudaGetLastError());
 }
+
+
 
 }  // namespace exg

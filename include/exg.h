@@ -285,6 +285,7 @@ int exg_last_step_timing(exg_ctx *ctx, double *ms5);
 /* The CUDA stream (cudaStream_t) the context issues all its work on. */
 int exg_get_stream(exg_ctx *ctx, void **stream);
 
+
 #ifdef __cplusplus
 }
 #endif
