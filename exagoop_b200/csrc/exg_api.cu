@@ -120,6 +120,8 @@ void build_params_for(const exg_specs &s, Params &P) {
         P.ntile[d] = s.periodic[d] ? s.ncells[d] / T : (s.ncells[d] + 1 + T - 1) / T;
     P.ntiles = (long long)P.ntile[0] * P.ntile[1] * P.ntile[2];
 }
+int noalloc_p2g(const exg_specs *specs, const exg_particle_soa *dev, double *mass, double *vel, double *frc,
+                cudaStream_t stream, std::string &err);
 }  // namespace exg
 
 namespace {
@@ -1001,6 +1003,20 @@ int exg_last_step_timing(exg_ctx *ctx, double *ms5) {
     for (int k = 0; k < 4; ++k) ms5[k] = ctx->c.stage_ms[k] / n;
     ms5[4] = ctx->c.stage_ms[4];
     return EXG_OK;
+}
+
+int exg_p2g_momentum_noalloc(const exg_specs *specs, const exg_particle_soa *dev_particles, double *node_mass,
+                             double *node_vel, double *node_frc, void *stream) {
+    if (!specs || !dev_particles || !node_mass || !node_vel || !node_frc || dev_particles->np < 0) return EXG_ERR_ARG;
+    const std::string v = validate(*specs);
+    if (!v.empty()) {
+        fprintf(stderr, "exg_p2g_momentum_noalloc: %s\n", v.c_str());
+        return EXG_ERR_CONFIG;
+    }
+    std::string err;
+    const int rc = noalloc_p2g(specs, dev_particles, node_mass, node_vel, node_frc, (cudaStream_t)stream, err);
+    if (rc) fprintf(stderr, "%s\n", err.c_str());
+    return rc;
 }
 
 int exg_get_stream(exg_ctx *ctx, void **stream) {

@@ -2042,5 +2042,230 @@ void EXG_SFX(launch_diag)(Ctx &c, double *out_dev) {
 }
 
 
+#if defined(EXG_R_FP64)
+// ====================================================================== no-alloc P2G
+// exg_p2g_momentum_noalloc: P2G of mass, momentum and force for callers that
+// must not allocate device memory (see include/exg.h).  Its scratch -- the
+// 64-bit fixed-point node sums, the per-channel bounds and scales -- lives in
+// this file-scope device array instead of cudaMalloc'd buffers.  Every GPU
+// that loads the library holds the array until the process exits.
+namespace {
+constexpr long long kNaNodes = EXG_NOALLOC_MAX_NODES;
+constexpr int kNaCh = CH_MOM_END;  // mass, momentum(3), force(3)
+// [kNaCh * kNaNodes] node sums, 8 bound words, 8 scale words, one word for
+// the largest particle count of a cell, then kNaNodes 32-bit cell counts
+constexpr long long kNaWords = kNaCh * kNaNodes + 17 + kNaNodes / 2;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNaWords];
+
+struct NaArgs {
+    const double *pos;
+    const double *rdata;
+    const int32_t *idata;
+    long long np;
+    double *mass, *vel, *frc;
+    unsigned long long *acc;  // device address of g_noalloc_scratch
+};
+
+__global__ void k_na_clear(unsigned long long *acc, long long n) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) acc[i] = 0ull;
+}
+
+// particles per cell, and the largest count (the fixed-point range bound
+// uses it as the context path uses the sort's maximum)
+__global__ void k_na_count(Params P, NaArgs a) {
+    long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= a.np || a.idata[(long long)EXG_I_PHASE * a.np + p] != 0) return;
+    const double x[3] = {a.pos[p], a.pos[a.np + p], a.pos[2 * a.np + p]};
+    int iv[3];
+    cell_of(P, x, iv);
+    if (iv[0] < 0 || iv[0] >= P.nc[0] || iv[1] < 0 || iv[1] >= P.nc[1] || iv[2] < 0 || iv[2] >= P.nc[2]) return;
+    unsigned *cnt = reinterpret_cast<unsigned *>(a.acc + kNaCh * kNaNodes + 17);
+    const unsigned old = atomicAdd(&cnt[((long long)iv[2] * P.nc[1] + iv[1]) * P.nc[0] + iv[0]], 1u);
+    atomicMax(a.acc + kNaCh * kNaNodes + 16, (unsigned long long)(old + 1u));
+}
+
+// per-channel largest |term| (as ordered bits) over phase-0 particles
+__global__ void k_na_bounds(Params P, NaArgs a) {
+    long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= a.np || a.idata[(long long)EXG_I_PHASE * a.np + p] != 0) return;
+    auto R = [&](int f) { return a.rdata[(long long)f * a.np + p]; };
+    unsigned long long *bnd = a.acc + kNaCh * kNaNodes;
+    const double m = R(EXG_R_MASS), vol = R(EXG_R_VOLUME);
+    double b[kNaCh];
+    b[CH_M] = fabs(m);
+    const int rowi[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    for (int d = 0; d < 3; ++d) {
+        b[CH_P + d] = fabs(m * R(EXG_R_VEL + d));
+        double s = 0.0;
+        for (int j = 0; j < 3; ++j) s += fabs(R(EXG_R_STRESS + rowi[d][j])) * 2.0 * P.dxi[j];
+        b[CH_F + d] = fabs(m * P.gravity[d]) + (P.external_loads ? fabs(P.extforce[d]) : 0.0) + fabs(vol) * s;
+    }
+    for (int c = 0; c < kNaCh; ++c) atomicMax(&bnd[c], dbits(b[c]));
+}
+
+// scale 2^e per channel so that (particles per cell) x (stencil cells) x
+// (largest term) x 2 < 2^61, the bound of the context path's k_scales
+__global__ void k_na_scale(NaArgs a, int stencil_cells) {
+    const int c = threadIdx.x;
+    if (c >= kNaCh) return;
+    unsigned long long *bnd = a.acc + kNaCh * kNaNodes;
+    const unsigned long long ppc = bnd[16];
+    const double S = bitsd(bnd[c]) * (double)(ppc > 0 ? ppc : 1) * (double)stencil_cells * 2.0;
+    double sc = 1.0;
+    if (S > 0.0 && S < 1e300) {
+        int ex;
+        frexp(S, &ex);
+        sc = ldexp(1.0, max(-100, min(100, 61 - ex)));
+    }
+    bnd[8 + c] = dbits(sc);
+}
+
+template <int ORD>
+__global__ void __launch_bounds__(kThreads) k_na_deposit(Params P, NaArgs a) {
+    constexpr int W = Stc<ORD>::W, LO = Stc<ORD>::LO;
+    __shared__ SplineTables tab;
+    load_tables(&tab);
+    __syncthreads();
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= a.np || a.idata[(long long)EXG_I_PHASE * a.np + p] != 0) return;
+    auto R = [&](int f) { return a.rdata[(long long)f * a.np + p]; };
+    const unsigned long long *bnd = a.acc + kNaCh * kNaNodes;
+    double sc[kNaCh];
+    for (int c = 0; c < kNaCh; ++c) sc[c] = bitsd(bnd[8 + c]);
+    const double x[3] = {a.pos[p], a.pos[a.np + p], a.pos[2 * a.np + p]};
+    int iv[3];
+    cell_of(P, x, iv);
+    if (iv[0] < 0 || iv[0] >= P.nc[0] || iv[1] < 0 || iv[1] >= P.nc[1] || iv[2] < 0 || iv[2] >= P.nc[2]) return;
+    AxisW<double, W> ax, ay, az;
+    axis_weights<double, W, LO>(tab, P, 0, x[0], iv[0], ax);
+    axis_weights<double, W, LO>(tab, P, 1, x[1], iv[1], ay);
+    axis_weights<double, W, LO>(tab, P, 2, x[2], iv[2], az);
+    const double m = R(EXG_R_MASS), vol = R(EXG_R_VOLUME);
+    double mv[3], s[6];
+    for (int d = 0; d < 3; ++d) mv[d] = m * R(EXG_R_VEL + d);
+    for (int c = 0; c < 6; ++c) s[c] = R(EXG_R_STRESS + c);
+    const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] && x[1] > P.slab_lo[1] &&
+                      x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] && x[2] < P.slab_hi[2];
+    for (int sz = 0; sz < W; ++sz)
+        for (int sy = 0; sy < W; ++sy)
+            for (int sx = 0; sx < W; ++sx) {
+                const double wx = ax.w[sx], wy = ay.w[sy], wz = az.w[sz];
+                const double dx = ax.dw[sx], dy = ay.dw[sy], dz = az.dw[sz];
+                if ((wx == 0.0 && dx == 0.0) || (wy == 0.0 && dy == 0.0) || (wz == 0.0 && dz == 0.0)) continue;
+                const long long ni = node_index(P, iv[0] + LO + sx, iv[1] + LO + sy, iv[2] + LO + sz);
+                if (ni < 0) continue;
+                const double N = wx * wy * wz;
+                const double g[3] = {dx * wy * wz, wx * dy * wz, wx * wy * dz};
+                double v[kNaCh];
+                v[CH_M] = m * N;
+                for (int d = 0; d < 3; ++d) {
+                    v[CH_P + d] = mv[d] * N;
+                    const double tv = s[d == 0 ? 0 : (d == 1 ? 1 : 2)] * g[0] +
+                                      s[d == 0 ? 1 : (d == 1 ? 3 : 4)] * g[1] + s[d == 0 ? 2 : (d == 1 ? 4 : 5)] * g[2];
+                    v[CH_F + d] = (m * P.gravity[d] * N + (slab ? P.extforce[d] * N : 0.0)) + (-vol * tv);
+                }
+                for (int c = 0; c < kNaCh; ++c) {
+                    const long long q = __double2ll_rn(v[c] * sc[c]);
+                    if (q) atomicAdd(&a.acc[(long long)c * kNaNodes + ni], (unsigned long long)q);
+                }
+            }
+}
+
+// node sums -> the caller's arrays: mass, velocity p/m (m >= mass_tolerance,
+// as deposit_onto_grid_momentum normalises, mpm_particle_grid_ops.cpp:602-615),
+// force
+__global__ void k_na_finish(Params P, NaArgs a) {
+    const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= P.nnodes) return;
+    const unsigned long long *bnd = a.acc + kNaCh * kNaNodes;
+    // periodic axes: node ncells reads node 0
+    int id[3] = {(int)(n % P.nn[0]), (int)((n / P.nn[0]) % P.nn[1]), (int)(n / ((long long)P.nn[0] * P.nn[1]))};
+    const long long src = node_index(P, id[0], id[1], id[2]);
+    double v[kNaCh];
+    for (int c = 0; c < kNaCh; ++c)
+        v[c] = (double)(long long)a.acc[(long long)c * kNaNodes + src] * (1.0 / bitsd(bnd[8 + c]));
+    const double m = v[CH_M];
+    a.mass[n] = m;
+    for (int d = 0; d < 3; ++d) {
+        double vel = v[CH_P + d];
+        if (m > 0.0) vel = (m >= P.mass_tol) ? v[CH_P + d] / m : 0.0;
+        a.vel[(long long)d * P.nnodes + n] = vel;
+        a.frc[(long long)d * P.nnodes + n] = v[CH_F + d];
+    }
+}
+
+unsigned long long *g_na_addr[64] = {};
+}  // namespace
+
+// Builds the kernel parameters of a specs (also used by the context).
+void build_params_for(const exg_specs &s, Params &P);
+
+int noalloc_p2g(const exg_specs *specs, const exg_particle_soa *dev, double *mass, double *vel, double *frc,
+                cudaStream_t stream, std::string &err) {
+    Params P;
+    build_params_for(*specs, P);
+    if (P.nnodes > kNaNodes) {
+        err = "exg_p2g_momentum_noalloc: the grid has " + std::to_string(P.nnodes) +
+              " nodes; this entry point's static scratch holds at most " + std::to_string(kNaNodes) +
+              " (EXG_NOALLOC_MAX_NODES)";
+        return EXG_ERR_OVERFLOW;
+    }
+    int dev_id = 0;
+    if (cudaGetDevice(&dev_id) != cudaSuccess || dev_id < 0 || dev_id >= 64) {
+        err = "exg_p2g_momentum_noalloc: no current CUDA device";
+        return EXG_ERR_CUDA;
+    }
+    if (!g_na_addr[dev_id]) {
+        // one-time set-up on this device (outside any stream capture): the
+        // device address of the scratch array and the spline tables
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) {
+            err = std::string("exg_p2g_momentum_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
+            return EXG_ERR_CUDA;
+        }
+        try {
+            upload_tables_fp64();
+        } catch (const std::exception &ex) {
+            err = ex.what();
+            return EXG_ERR_CUDA;
+        }
+        g_na_addr[dev_id] = reinterpret_cast<unsigned long long *>(ptr);
+    }
+    NaArgs a;
+    a.pos = dev->pos;
+    a.rdata = dev->rdata;
+    a.idata = dev->idata;
+    a.np = dev->np;
+    a.mass = mass;
+    a.vel = vel;
+    a.frc = frc;
+    a.acc = g_na_addr[dev_id];
+    const long long nclear = kNaWords;
+    k_na_clear<<<nblocks(nclear), kThreads, 0, stream>>>(a.acc, nclear);
+    if (a.np > 0) {
+        k_na_bounds<<<nblocks(a.np), kThreads, 0, stream>>>(P, a);
+        k_na_count<<<nblocks(a.np), kThreads, 0, stream>>>(P, a);
+    }
+    const int W = (P.uniform_order == 1) ? 2 : 4;
+    k_na_scale<<<1, 32, 0, stream>>>(a, W * W * W);
+    if (a.np > 0) {
+        switch (P.uniform_order) {
+            case 1: k_na_deposit<1><<<nblocks(a.np), kThreads, 0, stream>>>(P, a); break;
+            case 2: k_na_deposit<2><<<nblocks(a.np), kThreads, 0, stream>>>(P, a); break;
+            case 3: k_na_deposit<3><<<nblocks(a.np), kThreads, 0, stream>>>(P, a); break;
+            default: k_na_deposit<0><<<nblocks(a.np), kThreads, 0, stream>>>(P, a); break;
+        }
+    }
+    k_na_finish<<<nblocks(P.nnodes), kThreads, 0, stream>>>(P, a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        err = std::string("exg_p2g_momentum_noalloc: ") + cudaGetErrorString(e);
+        return EXG_ERR_CUDA;
+    }
+    return EXG_OK;
+}
+#endif  // EXG_R_FP64
 
 }  // namespace exg

@@ -25,6 +25,7 @@ EXG_NREAL = 53
 EXG_NINT = 3
 EXG_N_NCOMP = 26
 EXG_MAX_BODIES = 8
+EXG_NOALLOC_MAX_NODES = 262144
 PREC_FP64, PREC_MIXED = 0, 1
 
 # realData (Source/mpm_specs.H:17-61) and intData indices
@@ -115,7 +116,7 @@ EXPORTED = [
     "exg_backup_current_temperature", "exg_nodal_time_update_temperature", "exg_apply_nodal_bcs_temperature",
     "exg_store_delta_temperature", "exg_g2p_temperature", "exg_step", "exg_get_time", "exg_set_time",
     "exg_diagnostics", "exg_sort_keys", "exg_tile_size", "exg_set_stage_timing", "exg_last_step_timing",
-    "exg_get_stream",
+    "exg_get_stream", "exg_p2g_momentum_noalloc",
 ]
 
 _lib = None
@@ -179,6 +180,7 @@ def lib() -> C.CDLL:
         "exg_set_stage_timing": (i, [vp, i]),
         "exg_last_step_timing": (i, [vp, pd]),
         "exg_get_stream": (i, [vp, C.POINTER(vp)]),
+        "exg_p2g_momentum_noalloc": (i, [C.POINTER(Specs), C.POINTER(ParticleSoA), pd, pd, pd, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -285,6 +285,34 @@ int exg_last_step_timing(exg_ctx *ctx, double *ms5);
 /* The CUDA stream (cudaStream_t) the context issues all its work on. */
 int exg_get_stream(exg_ctx *ctx, void **stream);
 
+/* ------------------------------------------------ P2G without allocation */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code running while another component captures a CUDA graph in global
+ * capture mode (cudaMalloc is not permitted then), hosts that hand all
+ * device memory to their own pool or enforce a fixed device-memory budget,
+ * and real-time loops that forbid allocation after start-up.  It computes
+ * what exg_p2g_momentum(ctx, 1, 1, 1) computes -- nodal mass, velocity (momentum
+ * over mass, zero below mass_tolerance) and force, deterministically in
+ * 64-bit fixed point -- without a context and without allocating: its
+ * scratch is a static device array of EXG_NOALLOC_MAX_NODES nodes x 7
+ * channels x 8 bytes plus one 32-bit count per cell (about 16 MB) that every GPU which loads the library
+ * holds until the process exits.
+ *   specs          host pointer; grids of more than EXG_NOALLOC_MAX_NODES
+ *                  nodes ((ncells+1)^3) are rejected with EXG_ERR_OVERFLOW
+ *                  and a message on stderr
+ *   dev_particles  host struct whose pos/rdata/idata point to DEVICE arrays
+ *                  in the exg_particle_soa layout
+ *   node_mass      device, (ncells+1)^3 doubles, x fastest
+ *   node_vel, node_frc  device, 3 x (ncells+1)^3 doubles (component-major)
+ *   stream         cudaStream_t the work is issued on (NULL = legacy stream)
+ * The first call on a device looks up the scratch array's device address and
+ * loads the spline tables there; make that first call before any stream
+ * capture begins.  All calls share the one array: it is cleared at the start
+ * of every call, and calls that overlap on the GPU (different streams, no
+ * ordering between them) race on it. */
+#define EXG_NOALLOC_MAX_NODES 262144
+int exg_p2g_momentum_noalloc(const exg_specs *specs, const exg_particle_soa *dev_particles, double *node_mass,
+                             double *node_vel, double *node_frc, void *stream);
 
 #ifdef __cplusplus
 }
