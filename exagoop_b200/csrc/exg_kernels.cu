@@ -1180,8 +1180,45 @@ __device__ __forceinline__ void interp_axis(const SplineTables &t, const Params 
 }
 
 // interpolate_from_grid for one particle (mpm_particle_grid_ops.cpp:972-1096).
+// FLIP blend, F update and strain rate from the interpolated velocity,
+// velocity increment and velocity gradient (mpm_particle_grid_ops.cpp:1030-1094).
+template <class R>
+__device__ __forceinline__ void g2p_finish(const Params &P, bool upd_vel, bool upd_sr, const R vpic[3],
+                                           const R dpic[3], const R gv[3][3], R v[3], R vp[3], R E[9], R sr[6],
+                                           double dt) {
+    if (upd_vel) {
+        const R a = (R)P.alpha;
+        for (int d = 0; d < 3; ++d) {
+            vp[d] = vpic[d];
+            v[d] = a * v[d] + a * dpic[d] + (R(1) - a) * vpic[d];
+        }
+    }
+    if (upd_sr) {
+        // get_deformation_gradient_tensor (interpolants.H:1732-1787) on
+        // F = I + E: E' = E + (L dt) + (L dt) E.
+        R nrm = R(0);
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) nrm += gv[a][b] * gv[a][b];
+        if (!(nrm >= R(1.0e10))) {
+            R Ld[3][3], En[9];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) Ld[a][b] = gv[a][b] * (R)dt;
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    R acc = E[a * 3 + b] + Ld[a][b];
+                    for (int c = 0; c < 3; ++c) acc += Ld[a][c] * E[c * 3 + b];
+                    En[a * 3 + b] = acc;
+                }
+            for (int q = 0; q < 9; ++q) E[q] = En[q];
+        }
+        int ind = 0;
+        for (int d1 = 0; d1 < 3; ++d1)
+            for (int d2 = d1; d2 < 3; ++d2) sr[ind++] = R(0.5) * (gv[d1][d2] + gv[d2][d1]);
+    }
+}
+
 template <class R, int ORD, class NodeAcc>
-__device__ __forceinline__ void g2p_particle(const SplineTables &tab, const Params &P, const NodeAcc &na,
+__device__ __forceinline__ void g2p_particle_generic(const SplineTables &tab, const Params &P, const NodeAcc &na,
                                              const double x[3], const int iv[3], bool upd_vel, bool upd_sr, R v[3],
                                              R vp[3], R E[9], R sr[6], double dt) {
     constexpr int W = Stc<ORD>::W, LO = Stc<ORD>::LO;
@@ -1239,36 +1276,122 @@ __device__ __forceinline__ void g2p_particle(const SplineTables &tab, const Para
                     }
         }
     }
-    if (upd_vel) {
-        const R a = (R)P.alpha;
-        for (int d = 0; d < 3; ++d) {
-            vp[d] = vpic[d];
-            v[d] = a * v[d] + a * dpic[d] + (R(1) - a) * vpic[d];
-        }
-    }
-    if (upd_sr) {
-        // get_deformation_gradient_tensor (interpolants.H:1732-1787) on
-        // F = I + E: E' = E + (L dt) + (L dt) E.
-        R nrm = R(0);
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) nrm += gv[a][b] * gv[a][b];
-        if (!(nrm >= R(1.0e10))) {
-            R Ld[3][3], En[9];
-            for (int a = 0; a < 3; ++a)
-                for (int b = 0; b < 3; ++b) Ld[a][b] = gv[a][b] * (R)dt;
-            for (int a = 0; a < 3; ++a)
-                for (int b = 0; b < 3; ++b) {
-                    R acc = E[a * 3 + b] + Ld[a][b];
-                    for (int c = 0; c < 3; ++c) acc += Ld[a][c] * E[c * 3 + b];
-                    En[a * 3 + b] = acc;
+    g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt);
+}
+
+// Quadratic interior weights on the 3-node window that holds the support:
+// offsets -1..1 when f < 1/2, else 0..2 (the fourth offset's weight is 0).
+// Returns the stencil offset of window entry 0.
+template <class R>
+__device__ __forceinline__ int quad_window(const Params &P, int d, double x, int i, R w[3], R dw[3]) {
+    const R f = (R)((x - (P.plo[d] + i * P.dx[d])) * P.dxi[d]);
+    const R dxinv = (R)P.dxi[d];
+    const bool lo = f < R(0.5);
+    const R u = lo ? f : f - R(1);
+    R z = u + R(1);
+    w[0] = R(0.5) * z * z + R(-1.5) * z + R(1.125);
+    dw[0] = (z - R(1.5)) * dxinv;
+    z = u;
+    w[1] = R(-1) * z * z + R(0) * z + R(0.75);
+    dw[1] = (R(-2) * z) * dxinv;
+    z = u - R(1);
+    w[2] = R(0.5) * z * z + R(1.5) * z + R(1.125);
+    dw[2] = (z + R(1.5)) * dxinv;
+    return lo ? -1 : 0;
+}
+
+// Interpolation over a WN^3 window of the shared-memory node block.
+template <class R, int WN>
+__device__ __forceinline__ void g2p_window(const SmemNodes<R> &na, const int base[3], const R wx[WN], const R dwx[WN],
+                                           const R wy[WN], const R dwy[WN], const R wz[WN], const R dwz[WN],
+                                           bool upd_vel, bool upd_sr, R vpic[3], R dpic[3], R gv[3][3]) {
+    const int B = na.B, B3 = na.B3;
+    const int i0 = ((base[2] - na.org[2]) * B + (base[1] - na.org[1])) * B + (base[0] - na.org[0]);
+    const R *nb = na.nb;
+#pragma unroll
+    for (int sz = 0; sz < WN; ++sz) {
+#pragma unroll
+        for (int sy = 0; sy < WN; ++sy) {
+            const R wyz = wy[sy] * wz[sz], dyz = dwy[sy] * wz[sz], wdz = wy[sy] * dwz[sz];
+            const int row = i0 + (sz * B + sy) * B;
+#pragma unroll
+            for (int sx = 0; sx < WN; ++sx) {
+                const int idx = row + sx;
+                const R v0 = nb[idx], v1 = nb[B3 + idx], v2 = nb[2 * B3 + idx];
+                if (upd_vel) {
+                    const R N = wx[sx] * wyz;
+                    vpic[0] += N * v0;
+                    vpic[1] += N * v1;
+                    vpic[2] += N * v2;
+                    dpic[0] += N * nb[3 * B3 + idx];
+                    dpic[1] += N * nb[4 * B3 + idx];
+                    dpic[2] += N * nb[5 * B3 + idx];
                 }
-            for (int q = 0; q < 9; ++q) E[q] = En[q];
+                if (upd_sr) {
+                    const R g0 = dwx[sx] * wyz, g1 = wx[sx] * dyz, g2 = wx[sx] * wdz;
+                    gv[0][0] += v0 * g0;
+                    gv[0][1] += v0 * g1;
+                    gv[0][2] += v0 * g2;
+                    gv[1][0] += v1 * g0;
+                    gv[1][1] += v1 * g1;
+                    gv[1][2] += v1 * g2;
+                    gv[2][0] += v2 * g0;
+                    gv[2][1] += v2 * g1;
+                    gv[2][2] += v2 * g2;
+                }
+            }
         }
-        int ind = 0;
-        for (int d1 = 0; d1 < 3; ++d1)
-            for (int d2 = d1; d2 < 3; ++d2) sr[ind++] = R(0.5) * (gv[d1][d2] + gv[d2][d1]);
     }
 }
+
+// G2P of one particle from the shared-memory node block: the interior fast
+// path (fixed spline pieces; quadratic on its 3-node window) when every
+// stencil node of the particle's cell has the interior shape type, else the
+// table-driven path.
+template <class R, int ORD>
+__device__ __forceinline__ void g2p_particle_smem(const SplineTables &tab, const Params &P, const SmemNodes<R> &na,
+                                                  const double x[3], const int iv[3], bool upd_vel, bool upd_sr,
+                                                  R v[3], R vp[3], R E[9], R sr[6], double dt) {
+    bool inter = (ORD != 0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        inter = inter && ((ORD == 1) || P.periodic[d] || (iv[d] >= 3 && iv[d] <= P.nc[d] - 4));
+    if (!inter) {
+        g2p_particle_generic<R, ORD>(tab, P, na, x, iv, upd_vel, upd_sr, v, vp, E, sr, dt);
+        return;
+    }
+    R vpic[3] = {R(0), R(0), R(0)}, dpic[3] = {R(0), R(0), R(0)};
+    R gv[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
+    if (ORD == 2) {
+        R w[3][3], dw[3][3];
+        int base[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) base[d] = iv[d] + quad_window<R>(P, d, x[d], iv[d], w[d], dw[d]);
+        g2p_window<R, 3>(na, base, w[0], dw[0], w[1], dw[1], w[2], dw[2], upd_vel, upd_sr, vpic, dpic, gv);
+    } else if (ORD == 1 || ORD == 3) {
+        constexpr int WN = (ORD == 1) ? 2 : 4;
+        constexpr int OW = (ORD == 0) ? 3 : ORD;  // keeps the template argument valid when ORD == 0
+        AxisW<R, WN> a[3];
+        int base[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            axis_weights_interior<R, OW>(P, d, x[d], iv[d], a[d]);
+            base[d] = iv[d] + Stc<OW>::LO;
+        }
+        g2p_window<R, WN>(na, base, a[0].w, a[0].dw, a[1].w, a[1].dw, a[2].w, a[2].dw, upd_vel, upd_sr, vpic, dpic,
+                          gv);
+    }
+    g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt);
+}
+
+// G2P of one particle through any node accessor (the unfused L5 path).
+template <class R, int ORD, class NodeAcc>
+__device__ __forceinline__ void g2p_particle(const SplineTables &tab, const Params &P, const NodeAcc &na,
+                                             const double x[3], const int iv[3], bool upd_vel, bool upd_sr, R v[3],
+                                             R vp[3], R E[9], R sr[6], double dt) {
+    g2p_particle_generic<R, ORD>(tab, P, na, x, iv, upd_vel, upd_sr, v, vp, E, sr, dt);
+}
+
 
 // moveParticles for one particle (mpm_particle_timestep.cpp:326-576).
 template <class R>
@@ -1435,7 +1558,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_g2p_fused(Params P, Parts<R> A,
                 int iv[3];
                 cell_of(P, x, iv);
                 R E[9], sr[6];
-                g2p_particle<R, ORD>(*tab, P, na, x, iv, true, false, v, vp, E, sr, dt);
+                g2p_particle_smem<R, ORD>(*tab, P, na, x, iv, true, false, v, vp, E, sr, dt);
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     A.v[d][p] = v[d];
@@ -1467,7 +1590,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_g2p_fused(Params P, Parts<R> A,
         if (phase == 0) {
             int iv[3];
             cell_of(P, x, iv);
-            g2p_particle<R, ORD>(*tab, P, na, x, iv, upd_vel, true, v, vp, E, sr, dt);
+            g2p_particle_smem<R, ORD>(*tab, P, na, x, iv, upd_vel, true, v, vp, E, sr, dt);
         }
         move_particle<R>(P, bc, phase, x, v, vp, dt, status);
         // Redistribute's periodic wrap
