@@ -108,6 +108,20 @@ void build_params_for(const exg_specs &s, Params &P) {
         o.T_inf = e.T_inf;
     }
     P.use_temp = s.use_temp;
+    for (int d = 0; d < 3; ++d) {
+        P.bclo_temp[d] = s.bclo_temp[d];
+        P.bchi_temp[d] = s.bchi_temp[d];
+        P.Twall_lo[d] = s.T_wall_lo[d];
+        P.Twall_hi[d] = s.T_wall_hi[d];
+        P.qflux_lo[d] = s.flux_lo[d];
+        P.qflux_hi[d] = s.flux_hi[d];
+        P.hc_lo[d] = s.h_lo[d];
+        P.hc_hi[d] = s.h_hi[d];
+        P.Tinf_lo[d] = s.Tinf_lo[d];
+        P.Tinf_hi[d] = s.Tinf_hi[d];
+        P.udfT_lo[d] = s.udf_temp_lo[d] != nullptr;
+        P.udfT_hi[d] = s.udf_temp_hi[d] != nullptr;
+    }
     // tile geometry
     int T = s.tile > 0 ? s.tile : 8;
     P.T = T;
@@ -220,7 +234,8 @@ void upload_parts(Ctx &c, const exg_particle_soa *h, const std::vector<int32_t> 
     put_r(P.radius, EXG_R_RADIUS);
     put_r(P.yacc, EXG_R_YACC);
     if (c.specs.use_temp) {
-        put_r(P.T, EXG_R_TEMPERATURE);
+        EXG_CUDA_OK(cudaMemcpy(P.T, h->rdata + (size_t)EXG_R_TEMPERATURE * n, sizeof(double) * n,
+                               cudaMemcpyHostToDevice));
         put_r(P.cp, EXG_R_SPHEAT);
         put_r(P.kc, EXG_R_THERMCOND);
         for (int d = 0; d < 3; ++d) put_r(P.q[d], EXG_R_HEATFLUX + d);
@@ -273,7 +288,8 @@ void download_parts(Ctx &c, exg_particle_soa *h) {
     get_r(P.radius, EXG_R_RADIUS);
     get_r(P.yacc, EXG_R_YACC);
     if (c.specs.use_temp) {
-        get_r(P.T, EXG_R_TEMPERATURE);
+        EXG_CUDA_OK(cudaMemcpy(xb.data(), P.T, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        for (long long i = 0; i < n; ++i) h->rdata[(size_t)EXG_R_TEMPERATURE * n + pid[i]] = xb[i];
         get_r(P.cp, EXG_R_SPHEAT);
         get_r(P.kc, EXG_R_THERMCOND);
         for (int d = 0; d < 3; ++d) get_r(P.q[d], EXG_R_HEATFLUX + d);
@@ -343,6 +359,40 @@ bool has_udf(const Ctx &c) {
     return false;
 }
 
+// UDF wall-temperature tables of compute_udf_temp_at_nodes
+// (nodal_data_ops.cpp:1178-1293): two values per face node.
+void tabulate_udf_temp(Ctx &c, double t) {
+    for (int side = 0; side < 2; ++side)
+        for (int d = 0; d < 3; ++d) {
+            exg_temp_udf fn = side ? c.specs.udf_temp_hi[d] : c.specs.udf_temp_lo[d];
+            if (!fn) continue;
+            const int p0 = (d == 0) ? 1 : 0, p1 = (d == 2) ? 1 : 2;
+            const int n0 = c.P.nc[p0] + 1, n1 = c.P.nc[p1] + 1;
+            std::vector<double> &tab = c.udfT_host[side][d];
+            tab.assign((size_t)n0 * n1 * 2, 0.0);
+            for (int j = 0; j < n0; ++j)
+                for (int k = 0; k < n1; ++k) {
+                    double xc[3] = {0, 0, 0};
+                    xc[d] = side ? c.P.phi[d] : c.P.plo[d];
+                    xc[p0] = c.P.plo[p0] + j * c.P.dx[p0];
+                    xc[p1] = c.P.plo[p1] + k * c.P.dx[p1];
+                    double out[2] = {0, 0};
+                    fn(xc[0], xc[1], xc[2], t, out);
+                    tab[((size_t)j * n1 + k) * 2] = out[0];
+                    tab[((size_t)j * n1 + k) * 2 + 1] = out[1];
+                }
+            if (!c.udfT_tab[side][d]) c.udfT_tab[side][d] = dalloc<double>(tab.size());
+            EXG_CUDA_OK(cudaMemcpyAsync(c.udfT_tab[side][d], tab.data(), sizeof(double) * tab.size(),
+                                        cudaMemcpyHostToDevice, c.stream));
+            sync(c);
+        }
+}
+bool has_udf_temp(const Ctx &c) {
+    for (int d = 0; d < 3; ++d)
+        if (c.specs.udf_temp_lo[d] || c.specs.udf_temp_hi[d]) return true;
+    return false;
+}
+
 int status_from_ctl(Ctx &c) {
     ctl_pull(c);
     unsigned st = c.ctl_host->status;
@@ -391,19 +441,35 @@ void enqueue_step(Ctx &c) {
     launch_sort_rest(c, true);
     if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[1], c.stream));
     launch_scales_from(c, c.bounds_cur);
-    DISPATCH(launch_p2g, c, PF_MASS | PF_VEL | PF_FORCE);
+    const bool th = c.specs.use_temp != 0;
+    const bool musl = c.specs.stress_update_scheme != 0;
+    const int tflags = th ? (PF_TEMP | PF_SRC) : 0;
+    const int udfT = has_udf_temp(c) ? 1 : 0;
+    DISPATCH(launch_p2g, c, PF_MASS | PF_VEL | PF_FORCE | tflags);
     if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[2], c.stream));
-    DISPATCH(launch_nodes, c, NM_FUSED, PF_MASS | PF_VEL | PF_FORCE, false);
+    DISPATCH(launch_nodes, c, NM_FUSED, PF_MASS | PF_VEL | PF_FORCE | tflags, false);
+    if (th) {
+        // Apply_Nodal_BCs_Temperature + store_delta_temperature (main.cpp:103-106)
+        DISPATCH(launch_temp_bcs, c, TW_MASKED, udfT, 1, musl ? 1 : 0);
+        DISPATCH(launch_temp_node_op, c, TN_DELTA, 0.0);
+    }
     if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[3], c.stream));
-    if (c.specs.stress_update_scheme == 0) {
+    if (!musl) {
+        if (th) DISPATCH(launch_g2p_temp, c, 1, 1);  // G2P_Temperature(1,1) (main.cpp:113)
         DISPATCH(launch_g2p_fused, c, GM_FULL);
     } else {
+        if (th) DISPATCH(launch_g2p_temp, c, 1, 0);  // G2P_Temperature(1,0) (main.cpp:132)
         DISPATCH(launch_g2p_fused, c, GM_VEL);
         launch_reset_accum(c, c.bounds2, c.dtmin2);
         DISPATCH(launch_state_reduce, c, c.bounds2, c.dtmin2);
         launch_scales_from(c, c.bounds2);
-        DISPATCH(launch_p2g, c, PF_VEL);
-        DISPATCH(launch_nodes, c, NM_MUSL2, PF_VEL, false);
+        // P2G_Momentum(0,1,0) and P2G_Temperature(1,0,1) in one deposit
+        DISPATCH(launch_p2g, c, PF_VEL | (th ? PF_SRC : 0));
+        DISPATCH(launch_nodes, c, NM_MUSL2, PF_VEL | (th ? PF_SRC : 0), false);
+        if (th) {
+            DISPATCH(launch_temp_bcs, c, TW_ON, udfT, 1, 0);  // main.cpp:134-135
+            DISPATCH(launch_g2p_temp, c, 0, 1);               // G2P_Temperature(0,1) (main.cpp:136)
+        }
         DISPATCH(launch_g2p_fused, c, GM_STRAIN);
     }
     DISPATCH(launch_copy_lost, c);
@@ -490,6 +556,19 @@ int exg_ctx_create(const exg_specs *specs, int device, exg_ctx **out) {
         const long long B3 = (long long)c.P.B * c.P.B * c.P.B;
         c.staging_cap = (size_t)nt;
         c.staging = dalloc<long long>((size_t)nt * c.nch * B3);
+        if (specs->use_temp) {
+            // thermal wall pass: one entry per node of each non-periodic face
+            c.n_tface = 0;
+            for (int d = 0; d < 3; ++d) {
+                if (c.P.periodic[d]) continue;
+                const int p0 = (d == 0) ? 1 : 0, p1 = (d == 2) ? 1 : 2;
+                const long long n0 = c.P.periodic[p0] ? c.P.nc[p0] : c.P.nc[p0] + 1;
+                const long long n1 = c.P.periodic[p1] ? c.P.nc[p1] : c.P.nc[p1] + 1;
+                c.n_tface += 2 * n0 * n1;
+            }
+            if (c.n_tface) c.tface = dalloc<double>(c.n_tface);
+            c.ttmp = dalloc<unsigned char>(esz * c.P.nnodes);
+        }
         for (int k = 0; k < 6; ++k) EXG_CUDA_OK(cudaEventCreate(&c.ev[k]));
         // initial dt accumulators: "no particles"
         launch_reset_accum(c, &c.ctl->bound_bits[0], &c.ctl->dtmin_bits);
@@ -522,6 +601,10 @@ int exg_ctx_destroy(exg_ctx *ctx) {
     for (double *p : c.ls) cudaFree(p);
     for (auto &row : c.udf_tab)
         for (double *p : row) cudaFree(p);
+    for (auto &row : c.udfT_tab)
+        for (double *p : row) cudaFree(p);
+    cudaFree(c.tface);
+    cudaFree(c.ttmp);
     void *bufs[] = {c.sb.key, c.sb.perm, c.sb.bucket, c.sb.tile_count, c.sb.tile_fill, c.sb.tile_start,
                     c.sb.active, c.sb.slot, c.sb.touched, c.sb.touched_step, c.sb.cell_start, c.staging, c.ctl,
                     c.bounds_cur, c.bounds2, c.dtmin2, c.mat_dev, c.diag_dev};
@@ -809,7 +892,6 @@ int exg_calculate_mp_stress_strain(exg_ctx *ctx, double time, double dt) {
 int exg_init_internal_forces(exg_ctx *ctx) {
     if (!ctx) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
-    if (c.specs.use_temp) return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
     int rc = exg_p2g_momentum(ctx, 1, 1, 1);
     if (rc) return rc;
     rc = exg_backup_current_velocity(ctx);
@@ -823,26 +905,93 @@ int exg_init_internal_forces(exg_ctx *ctx) {
         c.reduce_stale = true;
         sync(c);
     });
-    return EXG_OK;
+    if (!c.specs.use_temp) return EXG_OK;
+    // thermal prologue (mpm_init.cpp:411-441): deposit without source,
+    // backup, domain-wall BCs only (nodal_bcs_temperature), store delta, G2P
+    if ((rc = exg_p2g_temperature(ctx, 1, 1, 0))) return rc;
+    if ((rc = exg_backup_current_temperature(ctx))) return rc;
+    EXG_TRY(ctx, {
+        DISPATCH(launch_temp_bcs, c, TW_ON, 0, 0, 0);
+        rc = status_from_ctl(c);
+    });
+    if (rc) return rc;
+    if ((rc = exg_store_delta_temperature(ctx))) return rc;
+    return exg_g2p_temperature(ctx, 1, 1);
 }
 
-int exg_p2g_temperature(exg_ctx *ctx, int, int, int) {
-    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+static int need_temp(exg_ctx *ctx) {
+    return ctx->c.specs.use_temp ? EXG_OK
+                                 : fail(ctx, EXG_ERR_NOT_READY, "thermal step function without mpm.use_temp");
+}
+
+int exg_p2g_temperature(exg_ctx *ctx, int reset, int update_temp, int update_source) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (int rc = need_temp(ctx)) return rc;
+    if (c.np == 0) return fail(ctx, EXG_ERR_NOT_READY, "no particles");
+    if (!reset)
+        return fail(ctx, EXG_ERR_UNSUPPORTED, "P2G_Temperature without reset (the reference always resets)");
+    EXG_TRY(ctx, {
+        const int flags = (update_temp ? PF_TEMP : 0) | (update_source ? PF_SRC : 0);
+        EXG_CUDA_OK(cudaMemsetAsync(&c.ctl->maxppc, 0, sizeof(int), c.stream));
+        do_sort(c, false);
+        launch_reset_accum(c, c.bounds2, c.dtmin2);
+        DISPATCH(launch_state_reduce, c, c.bounds2, c.dtmin2);
+        launch_scales_from(c, c.bounds2);
+        if (flags) {
+            DISPATCH(launch_p2g, c, flags);
+            DISPATCH(launch_nodes, c, NM_MERGE, flags, true);
+        } else {  // reset only
+            const size_t esz = fp64(c) ? 8 : 4;
+            for (int comp : {EXG_N_MASS_SPHEAT, EXG_N_MASS_SPHEAT_TEMP, EXG_N_SOURCE_TEMP}) {
+                void *a = fp64(c) ? (void *)c.N<double>().c[comp] : (void *)c.N<float>().c[comp];
+                EXG_CUDA_OK(cudaMemsetAsync(a, 0, esz * c.P.nnodes, c.stream));
+            }
+        }
+        return status_from_ctl(c);
+    });
 }
 int exg_backup_current_temperature(exg_ctx *ctx) {
-    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (int rc = need_temp(ctx)) return rc;
+    EXG_TRY(ctx, DISPATCH(launch_temp_node_op, c, TN_BACKUP, 0.0));
+    return EXG_OK;
 }
-int exg_nodal_time_update_temperature(exg_ctx *ctx, double) {
-    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+int exg_nodal_time_update_temperature(exg_ctx *ctx, double dt) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (int rc = need_temp(ctx)) return rc;
+    EXG_TRY(ctx, DISPATCH(launch_temp_node_op, c, TN_TIME_UPDATE, dt));
+    return EXG_OK;
 }
-int exg_apply_nodal_bcs_temperature(exg_ctx *ctx, double, double, int) {
-    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+int exg_apply_nodal_bcs_temperature(exg_ctx *ctx, double dt, double time, int dirichlet_only) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (int rc = need_temp(ctx)) return rc;
+    (void)dt;
+    EXG_TRY(ctx, {
+        tabulate_udf_temp(c, time);
+        DISPATCH(launch_temp_bcs, c, TW_ON, has_udf_temp(c) ? 1 : 0, 1, dirichlet_only ? 1 : 0);
+        return status_from_ctl(c);
+    });
 }
 int exg_store_delta_temperature(exg_ctx *ctx) {
-    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (int rc = need_temp(ctx)) return rc;
+    EXG_TRY(ctx, DISPATCH(launch_temp_node_op, c, TN_DELTA, 0.0));
+    return EXG_OK;
 }
-int exg_g2p_temperature(exg_ctx *ctx, int, int) {
-    return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
+int exg_g2p_temperature(exg_ctx *ctx, int update_temperature, int update_heatflux) {
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (int rc = need_temp(ctx)) return rc;
+    EXG_TRY(ctx, {
+        DISPATCH(launch_g2p_temp, c, update_temperature, update_heatflux);
+        c.reduce_stale = true;
+    });
+    return EXG_OK;
 }
 
 // ------------------------------------------------------------ fused step
@@ -850,10 +999,9 @@ int exg_step(exg_ctx *ctx, int nsteps) {
     if (!ctx || nsteps < 0) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     if (c.np == 0) return fail(ctx, EXG_ERR_NOT_READY, "no particles");
-    if (c.specs.use_temp) return fail(ctx, EXG_ERR_UNSUPPORTED, "thermal path not built in this version");
     EXG_TRY(ctx, {
         if (c.reduce_stale) do_reduce(c);
-        const bool host_dep = has_udf(c);
+        const bool host_dep = has_udf(c) || (c.specs.use_temp && has_udf_temp(c));
         const bool use_graph = !host_dep && !c.timing && std::getenv("EXG_NO_GRAPH") == nullptr;
         for (int s = 0; s < nsteps; ++s) {
             if (host_dep) {
@@ -861,6 +1009,7 @@ int exg_step(exg_ctx *ctx, int nsteps) {
                 // the host before the step's kernels.
                 ctl_pull(c);
                 tabulate_udf(c, c.ctl_host->time);
+                if (c.specs.use_temp) tabulate_udf_temp(c, c.ctl_host->time);
             }
             if (use_graph) {
                 cudaGraphExec_t &g = c.gexec[c.orient];

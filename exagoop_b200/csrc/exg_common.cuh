@@ -93,6 +93,10 @@ struct Params {
     int num_bodies;
     Body body[kMaxBodies];
     int use_temp;
+    // domain-wall thermal BCs (mpm_specs.H bc_temp_* arrays)
+    int bclo_temp[3], bchi_temp[3];
+    double Twall_lo[3], Twall_hi[3], qflux_lo[3], qflux_hi[3], hc_lo[3], hc_hi[3], Tinf_lo[3], Tinf_hi[3];
+    int udfT_lo[3], udfT_hi[3];  // wall-temperature table present
 };
 
 // Particle storage (structure of arrays).  Positions are FP64 in both
@@ -105,7 +109,9 @@ struct Parts {
     R *sr[6], *eps[6], *sig[6];
     R *E[9];
     R *vol, *mass, *rho, *J, *pres, *vol0, *radius, *yacc;
-    R *T, *cp, *kc, *q[3], *Q;
+    double *T;        // temperature: FP64 in both precisions (per-step increments
+                      // are far below FP32 resolution at a few hundred kelvin)
+    R *cp, *kc, *q[3], *Q;
     int32_t *mat;     // index into the material table
     uint8_t *phase;
     int32_t *rigid;

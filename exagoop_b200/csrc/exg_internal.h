@@ -15,6 +15,18 @@ enum NodeMode {
     NM_FUSED = 1,      // merge + backup + time update + BCs + store delta (one USL step)
     NM_MUSL2 = 2,      // merge momentum, normalise with the stored mass, BCs, store delta (MUSL pass 2)
 };
+// Thermal nodal operations (launch_temp_node_op).
+enum TempNodeOp {
+    TN_BACKUP = 0,     // backup_current_temperature
+    TN_TIME_UPDATE = 1,  // Nodal_Time_Update_Temperature
+    TN_DELTA = 2,      // store_delta_temperature
+};
+// walls_mask of launch_temp_bcs
+enum TempWalls {
+    TW_OFF = 0,        // no domain-wall pass
+    TW_ON = 1,         // wall pass reading the stored temperatures
+    TW_MASKED = 2,     // wall pass in a fused step: nodes below the mass tolerance read as 0
+};
 // Fused G2P modes.
 enum G2PMode {
     GM_FULL = 0,       // G2P vel + strain rate + F, move, volume, stress, reductions (USL)
@@ -62,7 +74,10 @@ void launch_node_reset(Ctx &c);
     void launch_move##sfx(Ctx &c, double dt);                                    \
     void launch_volume##sfx(Ctx &c);                                             \
     void launch_stress##sfx(Ctx &c, double time, double dt);                     \
-    void launch_diag##sfx(Ctx &c, double *out_dev);
+    void launch_diag##sfx(Ctx &c, double *out_dev);                              \
+    void launch_temp_node_op##sfx(Ctx &c, int op, double dt);                     \
+    void launch_temp_bcs##sfx(Ctx &c, int walls_mask, int udf, int ls, int dirichlet_only); \
+    void launch_g2p_temp##sfx(Ctx &c, int upd_T, int upd_q);
 EXG_DECL_PREC(_fp64)
 EXG_DECL_PREC(_fp32)
 
@@ -87,6 +102,12 @@ struct Ctx {
     // UDF wall tables [lo/hi][dir] (FP64)
     double *udf_tab[2][3] = {};
     std::vector<double> udf_host[2][3];
+    // UDF wall-temperature tables [lo/hi][dir] (FP64, two values per face node)
+    double *udfT_tab[2][3] = {};
+    std::vector<double> udfT_host[2][3];
+    double *tface = nullptr;           // thermal wall pass: one value per face-node entry
+    long long n_tface = 0;
+    void *ttmp = nullptr;              // thermal level-set pass: node-sized scratch (R)
     // sort
     SortBufs sb;
     long long *staging = nullptr;      // P2G partial node blocks (fixed point)

@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(kThreads) k_p2g(Params P, Parts<R> A, const in
             R mcp = R(0), mcpT = R(0), mk = R(0), qv[3] = {R(0), R(0), R(0)}, VQ = R(0);
             if (THERM) {
                 mcp = m * A.cp[p];
-                mcpT = mcp * A.T[p];
+                mcpT = (R)(mcp * A.T[p]);
                 mk = m * A.kc[p];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) qv[d] = A.q[d][p];
@@ -812,7 +812,7 @@ __global__ void __launch_bounds__(kCellThreads) k_p2g_cell(Params P, Parts<R> A,
                         R mcp = R(0), mcpT = R(0), mk = R(0), qv[3] = {R(0), R(0), R(0)}, VQ = R(0);
                         if (THERM) {
                             mcp = m * A.cp[p];
-                            mcpT = mcp * A.T[p];
+                            mcpT = (R)(mcp * A.T[p]);
                             mk = m * A.kc[p];
 #pragma unroll
                             for (int d = 0; d < 3; ++d) qv[d] = vol * A.q[d][p];
@@ -875,6 +875,7 @@ __global__ void __launch_bounds__(kCellThreads) k_p2g_cell(Params P, Parts<R> A,
 struct NodeBCArgs {
     const double *udf[2][3];
     const double *ls[kMaxBodies];
+    const double *udfT[2][3];  // wall-temperature tables: (value, second value) per face node
 };
 
 __device__ __forceinline__ double ls_node_value(const Params &P, const double *phi, int i, int j, int k) {
@@ -1089,6 +1090,21 @@ __global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeB
             }
             if (flags & PF_FORCE)
                 for (int d = 0; d < 3; ++d) Nd.c[EXG_N_FRC + d][ni] = (R)f[d];
+            if (THERM && (flags & (PF_TEMP | PF_SRC))) {
+                // P2G_Temperature with reset: m cp, m cp T and the source are
+                // zeroed, m k only when temperatures are deposited, and T is
+                // normalised where m cp > 0 (mpm_particle_grid_ops.cpp:680-884)
+                const bool fT = flags & PF_TEMP;
+                const double mc = fT ? (double)accv[CH_MC] * isc[CH_MC] : 0.0;
+                const double mct = fT ? (double)accv[CH_MCT] * isc[CH_MCT] : 0.0;
+                Nd.c[EXG_N_MASS_SPHEAT][ni] = (R)mc;
+                Nd.c[EXG_N_MASS_SPHEAT_TEMP][ni] = (R)mct;
+                Nd.c[EXG_N_SOURCE_TEMP][ni] = (R)((flags & PF_SRC) ? (double)accv[CH_SRC] * isc[CH_SRC] : 0.0);
+                if (fT) {
+                    Nd.c[EXG_N_MASS_COND][ni] = (R)((double)accv[CH_MK] * isc[CH_MK]);
+                    if (mc > 0.0) Nd.c[EXG_N_TEMPERATURE][ni] = (R)((mc >= P.mass_tol) ? mct / mc : 0.0);
+                }
+            }
         } else if (mode == NM_FUSED) {
             double v[3] = {p[0], p[1], p[2]};
             if (m > 0.0)
@@ -1113,6 +1129,26 @@ __global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeB
                 Nd.c[EXG_N_FRC + d][ni] = (R)f[d];
                 Nd.c[EXG_N_DVEL + d][ni] = (R)dv[d];
             }
+            if (THERM && (flags & PF_TEMP)) {
+                // P2G_Temperature(1,1,1), backup_current_temperature and
+                // Nodal_Time_Update_Temperature (main.cpp:100-102) on a node
+                // that Reset_Nodaldata_to_Zero left at 0
+                const double mc = (double)accv[CH_MC] * isc[CH_MC], mct = (double)accv[CH_MCT] * isc[CH_MCT];
+                const double src = (double)accv[CH_SRC] * isc[CH_SRC];
+                double Tn = 0.0;
+                if (mc > 0.0) Tn = (mc >= P.mass_tol) ? mct / mc : 0.0;
+                const double Told = (mc > 0.0) ? Tn : 0.0;
+                if (mc >= P.mass_tol)
+                    Tn += src / mc * dt;
+                else
+                    Tn = 0.0;
+                Nd.c[EXG_N_MASS_SPHEAT][ni] = (R)mc;
+                Nd.c[EXG_N_MASS_SPHEAT_TEMP][ni] = (R)mct;
+                Nd.c[EXG_N_MASS_COND][ni] = (R)((double)accv[CH_MK] * isc[CH_MK]);
+                Nd.c[EXG_N_SOURCE_TEMP][ni] = (R)src;
+                Nd.c[EXG_N_TEMPERATURE][ni] = (R)Tn;
+                Nd.c[EXG_N_DELTA_TEMPERATURE][ni] = (R)Told;
+            }
         } else {  // NM_MUSL2: P2G(0,1,0) + Apply_Nodal_BCs (main.cpp:124-127)
             m = (double)Nd.c[EXG_N_MASS][ni];
             double v[3] = {p[0], p[1], p[2]};
@@ -1122,6 +1158,13 @@ __global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeB
             for (int d = 0; d < 3; ++d) {
                 Nd.c[EXG_N_VEL + d][ni] = (R)v[d];
                 if (m > 0.0) Nd.c[EXG_N_DVEL + d][ni] = (R)(v[d] - (double)Nd.c[EXG_N_DVEL + d][ni]);
+            }
+            if (THERM && (flags & PF_SRC)) {
+                // P2G_Temperature(1,0,1) of MUSL (main.cpp:133): the reset
+                // zeroes m cp and m cp T, only the source is deposited
+                Nd.c[EXG_N_MASS_SPHEAT][ni] = R(0);
+                Nd.c[EXG_N_MASS_SPHEAT_TEMP][ni] = R(0);
+                Nd.c[EXG_N_SOURCE_TEMP][ni] = (R)((double)accv[CH_SRC] * isc[CH_SRC]);
             }
         }
     }
@@ -1849,6 +1892,358 @@ __global__ void k_vol_stress(Params P, Parts<R> A, const Material *mats, long lo
     }
 }
 
+// ---------------------------------------------------------------- thermal
+// backup_current_temperature (nodal_data_ops.cpp:95-114),
+// Nodal_Time_Update_Temperature (:500-527), store_delta_temperature
+// (:409-430): one pass over the dense node arrays.
+template <class R>
+__global__ void k_temp_node_op(Params P, Nodes<R> Nd, int op, double dt) {
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= P.nnodes) return;
+    const double mc = (double)Nd.c[EXG_N_MASS_SPHEAT][n];
+    if (op == TN_BACKUP) {
+        if (mc > 0.0) Nd.c[EXG_N_DELTA_TEMPERATURE][n] = Nd.c[EXG_N_TEMPERATURE][n];
+    } else if (op == TN_TIME_UPDATE) {
+        if (mc >= P.mass_tol)
+            Nd.c[EXG_N_TEMPERATURE][n] =
+                (R)((double)Nd.c[EXG_N_TEMPERATURE][n] + (double)Nd.c[EXG_N_SOURCE_TEMP][n] / mc * dt);
+        else
+            Nd.c[EXG_N_TEMPERATURE][n] = R(0);
+    } else {
+        if (mc > 0.0)
+            Nd.c[EXG_N_DELTA_TEMPERATURE][n] =
+                (R)((double)Nd.c[EXG_N_TEMPERATURE][n] - (double)Nd.c[EXG_N_DELTA_TEMPERATURE][n]);
+    }
+}
+
+// Domain-wall thermal BCs, nodal_bcs_temperature (nodal_data_ops.cpp:786-910)
+// then apply_udf_nodal_bcs_temperature (:1296-1446).  Both are in-place
+// sweeps in node order (x fastest): a node on a high face reads its inward
+// neighbour after that neighbour's own update in the same sweep, a node on a
+// low face reads it before.  Only the last direction that writes a node
+// decides its value, so the sweep result of a node is a chain of at most
+// three links (one per high face), each a function of the next node's
+// value; every thread evaluates its node's chain from the values stored
+// before the pass, which gives the sweep result without ordering.
+struct TLink {
+    signed char dir, side, kind;
+    double a, b;  // wall constants of the link (value, second value)
+};
+
+template <class R>
+struct TempView {
+    const R *T, *mc, *mk, *m;
+    bool mask;  // fused step: nodes below the mass tolerance hold 0 before the pass
+    double mass_tol;
+    __device__ __forceinline__ double pre(long long n) const {
+        if (mask && !((double)mc[n] >= mass_tol)) return 0.0;
+        return (double)T[n];
+    }
+    // specific conductance k = (m k) / m, 1 on massless nodes
+    __device__ __forceinline__ double kn(long long n) const {
+        const double mm = (double)m[n];
+        return (mm > 0.0) ? (double)mk[n] / mm : 1.0;
+    }
+};
+
+__device__ __forceinline__ bool temp_wall_link(const Params &P, const int id[3], TLink &L) {
+    bool applied = false, any = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const bool lo = id[d] == 0;
+        const bool hi = !lo && id[d] == P.nc[d];
+        if (!lo && !hi) continue;
+        const int bc = lo ? P.bclo_temp[d] : P.bchi_temp[d];
+        const bool writes = bc == EXG_BCT_ISOTHERMAL || bc == EXG_BCT_USERFLUX || bc == EXG_BCT_CONVECTION ||
+                            (bc == EXG_BCT_ADIABATIC && !applied);
+        if (bc == EXG_BCT_PERIODIC || writes) applied = true;
+        if (!writes) continue;
+        any = true;
+        L.dir = (signed char)d;
+        L.side = hi ? 1 : 0;
+        L.kind = (signed char)bc;
+        L.a = L.b = 0.0;
+        if (bc == EXG_BCT_ISOTHERMAL) {
+            L.a = lo ? P.Twall_lo[d] : P.Twall_hi[d];
+        } else if (bc == EXG_BCT_USERFLUX) {
+            L.a = lo ? P.qflux_lo[d] : P.qflux_hi[d];
+        } else if (bc == EXG_BCT_CONVECTION) {
+            L.a = lo ? P.hc_lo[d] : P.hc_hi[d];
+            L.b = lo ? P.Tinf_lo[d] : P.Tinf_hi[d];
+        }
+    }
+    return any;
+}
+
+__device__ __forceinline__ bool temp_udf_link(const Params &P, const NodeBCArgs &bc, const int id[3], TLink &L) {
+    bool any = false;
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir) {
+        const double *tab = nullptr;
+        int code = -1, side = 0;
+        if (id[dir] == 0 && bc.udfT[0][dir]) {
+            tab = bc.udfT[0][dir];
+            code = P.bclo_temp[dir];
+        } else if (id[dir] == P.nc[dir] && bc.udfT[1][dir]) {
+            tab = bc.udfT[1][dir];
+            code = P.bchi_temp[dir];
+            side = 1;
+        }
+        if (!tab) continue;
+        if (code != EXG_BCT_ISOTHERMAL && code != EXG_BCT_USERFLUX && code != EXG_BCT_CONVECTION) continue;
+        const int p0 = (dir == 0) ? 1 : 0, p1 = (dir == 2) ? 1 : 2;
+        const long long f = ((long long)id[p0] * (P.nc[p1] + 1) + id[p1]) * 2;
+        any = true;
+        L.dir = (signed char)dir;
+        L.side = (signed char)side;
+        L.kind = (signed char)code;
+        L.a = tab[f];
+        L.b = tab[f + 1];
+    }
+    return any;
+}
+
+// Value written by one link given its neighbour's value.
+__device__ __forceinline__ double temp_link_apply(const Params &P, const TLink &L, double Tnb, double kn) {
+    const double h = P.dx[L.dir];
+    if (L.kind == EXG_BCT_ISOTHERMAL) return L.a;
+    if (L.kind == EXG_BCT_ADIABATIC) return Tnb;
+    if (L.kind == EXG_BCT_USERFLUX) return Tnb + L.a * h / kn;
+    const double Bi = L.a * h / kn;
+    return (Tnb + Bi * L.b) / (1.0 + Bi);
+}
+
+__device__ __forceinline__ long long node_lin(const Params &P, const int id[3]) {
+    return ((long long)id[2] * P.nn[1] + id[1]) * P.nn[0] + id[0];
+}
+
+// Result of the wall sweep at node id.
+template <class R>
+__device__ double temp_wall_value(const Params &P, const TempView<R> &tv, const int id0[3], unsigned &status) {
+    TLink L[3];
+    long long ln[3];
+    int nl = 0;
+    int id[3] = {id0[0], id0[1], id0[2]};
+    double val = 0.0;
+    for (int it = 0;; ++it) {
+        TLink l;
+        const long long n = node_lin(P, id);
+        if (!temp_wall_link(P, id, l)) {
+            val = tv.pre(n);
+            break;
+        }
+        if (l.kind == EXG_BCT_ISOTHERMAL) {
+            val = l.a;
+            break;
+        }
+        int nb[3] = {id[0], id[1], id[2]};
+        nb[l.dir] += l.side ? -1 : 1;
+        if (!l.side) {  // low face: the neighbour is swept later
+            val = temp_link_apply(P, l, tv.pre(node_lin(P, nb)), tv.kn(n));
+            break;
+        }
+        if (nl == 3) {  // at most three high faces: unreachable
+            status |= ST_BC;
+            break;
+        }
+        L[nl] = l;
+        ln[nl++] = n;
+        id[0] = nb[0];
+        id[1] = nb[1];
+        id[2] = nb[2];
+    }
+    for (int k = nl - 1; k >= 0; --k) val = temp_link_apply(P, L[k], val, tv.kn(ln[k]));
+    return val;
+}
+
+// Result of the wall sweep followed by the UDF sweep at node id.
+template <class R>
+__device__ double temp_face_value(const Params &P, const NodeBCArgs &bc, const TempView<R> &tv, const int id0[3],
+                                  bool walls, bool udf, unsigned &status) {
+    TLink L[3];
+    long long ln[3];
+    int nl = 0;
+    int id[3] = {id0[0], id0[1], id0[2]};
+    double val = 0.0;
+    for (int it = 0;; ++it) {
+        TLink l;
+        const long long n = node_lin(P, id);
+        if (!udf || !temp_udf_link(P, bc, id, l)) {
+            val = walls ? temp_wall_value<R>(P, tv, id, status) : tv.pre(n);
+            break;
+        }
+        if (l.kind == EXG_BCT_ISOTHERMAL) {
+            val = l.a;
+            break;
+        }
+        int nb[3] = {id[0], id[1], id[2]};
+        nb[l.dir] += l.side ? -1 : 1;
+        if (!l.side) {
+            const double before = walls ? temp_wall_value<R>(P, tv, nb, status) : tv.pre(node_lin(P, nb));
+            val = temp_link_apply(P, l, before, tv.kn(n));
+            break;
+        }
+        if (nl == 3) {
+            status |= ST_BC;
+            break;
+        }
+        L[nl] = l;
+        ln[nl++] = n;
+        id[0] = nb[0];
+        id[1] = nb[1];
+        id[2] = nb[2];
+    }
+    for (int k = nl - 1; k >= 0; --k) val = temp_link_apply(P, L[k], val, tv.kn(ln[k]));
+    return val;
+}
+
+// Face-node entries: for each non-periodic axis d and side, the owned nodes
+// of that face; a node on an edge or corner appears once per face and every
+// entry computes the same value.
+__device__ __forceinline__ bool face_entry(const Params &P, long long e, int id[3]) {
+    for (int d = 0; d < 3; ++d) {
+        if (P.periodic[d]) continue;
+        const int p0 = (d == 0) ? 1 : 0, p1 = (d == 2) ? 1 : 2;
+        const long long n0 = P.periodic[p0] ? P.nc[p0] : P.nc[p0] + 1;
+        const long long n1 = P.periodic[p1] ? P.nc[p1] : P.nc[p1] + 1;
+        const long long per = n0 * n1;
+        if (e < 2 * per) {
+            const int side = (int)(e / per);
+            const long long r = e % per;
+            id[d] = side ? P.nc[d] : 0;
+            id[p0] = (int)(r % n0);
+            id[p1] = (int)(r / n0);
+            return true;
+        }
+        e -= 2 * per;
+    }
+    return false;
+}
+
+template <class R>
+__global__ void k_temp_faces(Params P, Nodes<R> Nd, NodeBCArgs bc, double *out, long long nface, int walls, int mask,
+                             int udf, Ctl *ctl) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= nface) return;
+    int id[3];
+    if (!face_entry(P, e, id)) return;
+    TempView<R> tv{Nd.c[EXG_N_TEMPERATURE], Nd.c[EXG_N_MASS_SPHEAT], Nd.c[EXG_N_MASS_COND], Nd.c[EXG_N_MASS],
+                   mask != 0, P.mass_tol};
+    unsigned status = 0;
+    out[e] = temp_face_value<R>(P, bc, tv, id, walls != 0, udf != 0, status);
+    if (status) atomicOr(&ctl->status, status);
+}
+
+template <class R>
+__global__ void k_temp_faces_store(Params P, Nodes<R> Nd, const double *in, long long nface) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= nface) return;
+    int id[3];
+    if (!face_entry(P, e, id)) return;
+    Nd.c[EXG_N_TEMPERATURE][node_lin(P, id)] = (R)in[e];
+}
+
+// nodal_levelset_bcs_temperature (nodal_data_ops.cpp:235-349) for one body:
+// nodes inside the body (phi < 0) that carry heat capacity take the wall
+// temperature, or the flux / convective value from the neighbour one step
+// along the dominant axis of the outward normal, read as it was before the
+// body's pass.  Writes every node of dst.
+template <class R>
+__global__ void k_temp_levelset(Params P, Nodes<R> Nd, const double *phi, int b, const R *src, R *dst) {
+    const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= P.nnodes) return;
+    const int id[3] = {(int)(n % P.nn[0]), (int)((n / P.nn[0]) % P.nn[1]), (int)(n / ((long long)P.nn[0] * P.nn[1]))};
+    R out = src[n];
+    bool owned = true;
+    for (int d = 0; d < 3; ++d) owned = owned && !(P.periodic[d] && id[d] == P.nc[d]);
+    if (owned && (double)Nd.c[EXG_N_MASS_SPHEAT][n] > 0.0) {
+        const double xn[3] = {P.plo[0] + id[0] * P.dx[0], P.plo[1] + id[1] * P.dx[1], P.plo[2] + id[2] * P.dx[2]};
+        double lv, nd[3];
+        ls_sample(P, phi, xn, lv, nd);
+        const double gm = sqrt(nd[0] * nd[0] + nd[1] * nd[1] + nd[2] * nd[2]);
+        if (lv < 0.0 && !(gm < 1.0e-10)) {
+            for (int d = 0; d < 3; ++d) nd[d] /= gm;
+            const Body &bd = P.body[b];
+            if (bd.temp_bc == 1) {
+                out = (R)bd.T_wall;
+            } else if (bd.temp_bc == 3 || bd.temp_bc == 4) {
+                int dd = 0;
+                for (int d = 1; d < 3; ++d)
+                    if (fabs(nd[d]) > fabs(nd[dd])) dd = d;
+                int nb[3] = {id[0], id[1], id[2]};
+                nb[dd] += (nd[dd] > 0.0) ? 1 : -1;
+                const double mm = (double)Nd.c[EXG_N_MASS][n];
+                const double kn = (mm > 0.0) ? (double)Nd.c[EXG_N_MASS_COND][n] / mm : 1.0;
+                const long long q = node_index(P, nb[0], nb[1], nb[2]);
+                const double Tnb = q < 0 ? 0.0 : (double)src[q];  // ghost nodes hold 0
+                if (bd.temp_bc == 3) {
+                    out = (R)(Tnb + bd.heat_flux * P.dx[dd] / kn);
+                } else {
+                    const double Bi = bd.h_conv * P.dx[dd] / kn;
+                    out = (R)((Tnb + Bi * bd.T_inf) / (1.0 + Bi));
+                }
+            }
+        }
+    }
+    dst[n] = out;
+}
+
+// interpolate_from_grid_temperature (mpm_particle_grid_ops.cpp:1129-1270):
+// T += interpolated nodal temperature increment (scheme of the x order, as
+// the reference selects it) and q = -k grad T from the nodal temperatures.
+template <class R, int ORD>
+__global__ void __launch_bounds__(kThreads) k_g2p_temp(Params P, Parts<R> A, Nodes<R> Nd, long long np, int upd_T,
+                                                       int upd_q) {
+    __shared__ SplineTables tab;
+    load_tables(&tab);
+    __syncthreads();
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= np || A.phase[p] != 0) return;
+    const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+    int iv[3];
+    cell_of(P, x, iv);
+    if (upd_T) {
+        const R *dT = Nd.c[EXG_N_DELTA_TEMPERATURE];
+        R wx[4], wy[4], wz[4];
+        interp_axis<R>(tab, P, P.order[0], 0, x[0], iv[0], wx);
+        interp_axis<R>(tab, P, P.order[0], 1, x[1], iv[1], wy);
+        interp_axis<R>(tab, P, P.order[0], 2, x[2], iv[2], wz);
+        R acc = R(0);
+        for (int sz = 0; sz < 4; ++sz)
+            for (int sy = 0; sy < 4; ++sy)
+                for (int sx = 0; sx < 4; ++sx) {
+                    const R N = wx[sx] * wy[sy] * wz[sz];
+                    if (N == R(0)) continue;
+                    const long long q = node_index(P, iv[0] - 1 + sx, iv[1] - 1 + sy, iv[2] - 1 + sz);
+                    if (q >= 0) acc += N * dT[q];
+                }
+        A.T[p] = A.T[p] + (double)acc;
+    }
+    if (upd_q) {
+        constexpr int W = Stc<ORD>::W, LO = Stc<ORD>::LO;
+        const R *Tn = Nd.c[EXG_N_TEMPERATURE];
+        AxisW<R, W> ax, ay, az;
+        axis_weights<R, W, LO>(tab, P, 0, x[0], iv[0], ax);
+        axis_weights<R, W, LO>(tab, P, 1, x[1], iv[1], ay);
+        axis_weights<R, W, LO>(tab, P, 2, x[2], iv[2], az);
+        R g[3] = {R(0), R(0), R(0)};
+        for (int sz = 0; sz < W; ++sz)
+            for (int sy = 0; sy < W; ++sy)
+                for (int sx = 0; sx < W; ++sx) {
+                    const R gx = ax.dw[sx] * ay.w[sy] * az.w[sz], gy = ax.w[sx] * ay.dw[sy] * az.w[sz],
+                            gz = ax.w[sx] * ay.w[sy] * az.dw[sz];
+                    if (gx == R(0) && gy == R(0) && gz == R(0)) continue;
+                    const long long q = node_index(P, iv[0] + LO + sx, iv[1] + LO + sy, iv[2] + LO + sz);
+                    const R t = q >= 0 ? Tn[q] : R(0);
+                    g[0] += t * gx;
+                    g[1] += t * gy;
+                    g[2] += t * gz;
+                }
+        const R k = A.kc[p];
+        for (int d = 0; d < 3; ++d) A.q[d][p] = -k * g[d];
+    }
+}
+
 // Do_All_Diagnostics reductions (mpm_diagnostics.cpp:23-216) as one pass with
 // a fixed-shape tree: per-block partials in FP64, summed in block order by a
 // second single-block pass, so the result is deterministic.
@@ -1941,7 +2336,10 @@ static int persistent_grid(K kern, size_t smem) {
 static NodeBCArgs make_bc(Ctx &c) {
     NodeBCArgs bc;
     for (int s = 0; s < 2; ++s)
-        for (int d = 0; d < 3; ++d) bc.udf[s][d] = c.udf_tab[s][d];
+        for (int d = 0; d < 3; ++d) {
+            bc.udf[s][d] = c.udf_tab[s][d];
+            bc.udfT[s][d] = c.udfT_tab[s][d];
+        }
     for (int b = 0; b < kMaxBodies; ++b) bc.ls[b] = c.ls[b];
     return bc;
 }
@@ -2124,6 +2522,48 @@ void EXG_SFX(launch_g2p_simple)(Ctx &c, int uv, int us, double dt) {
         case 2: k_g2p_simple<R, 2><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, uv, us, dt); break;
         case 3: k_g2p_simple<R, 3><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, uv, us, dt); break;
         default: k_g2p_simple<R, 0><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, uv, us, dt); break;
+    }
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void EXG_SFX(launch_temp_node_op)(Ctx &c, int op, double dt) {
+    k_temp_node_op<EXG_R><<<nblocks(c.P.nnodes), kThreads, 0, c.stream>>>(c.P, c.N<EXG_R>(), op, dt);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void EXG_SFX(launch_temp_bcs)(Ctx &c, int walls, int udf, int ls, int dirichlet_only) {
+    using R = EXG_R;
+    const NodeBCArgs bc = make_bc(c);
+    Nodes<R> &Nd = c.N<R>();
+    if ((walls != TW_OFF || udf) && c.n_tface > 0) {
+        k_temp_faces<R><<<nblocks(c.n_tface), kThreads, 0, c.stream>>>(c.P, Nd, bc, c.tface, c.n_tface, walls != TW_OFF,
+                                                                       walls == TW_MASKED, udf, c.ctl);
+        EXG_CUDA_OK(cudaGetLastError());
+        k_temp_faces_store<R><<<nblocks(c.n_tface), kThreads, 0, c.stream>>>(c.P, Nd, c.tface, c.n_tface);
+        EXG_CUDA_OK(cudaGetLastError());
+    }
+    if (!ls) return;
+    for (int b = 0; b < c.P.num_bodies; ++b) {
+        const int tb = c.P.body[b].temp_bc;
+        if (!c.ls[b] || tb == 0 || (dirichlet_only && tb != 1)) continue;
+        R *tmp = reinterpret_cast<R *>(c.ttmp);
+        k_temp_levelset<R><<<nblocks(c.P.nnodes), kThreads, 0, c.stream>>>(c.P, Nd, c.ls[b], b,
+                                                                           Nd.c[EXG_N_TEMPERATURE], tmp);
+        EXG_CUDA_OK(cudaGetLastError());
+        EXG_CUDA_OK(cudaMemcpyAsync(Nd.c[EXG_N_TEMPERATURE], tmp, sizeof(R) * c.P.nnodes, cudaMemcpyDeviceToDevice,
+                                    c.stream));
+    }
+}
+
+void EXG_SFX(launch_g2p_temp)(Ctx &c, int ut, int uq) {
+    using R = EXG_R;
+    if (c.np == 0) return;
+    const int nb = nblocks(c.np);
+    switch (c.P.uniform_order) {
+        case 1: k_g2p_temp<R, 1><<<nb, kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, ut, uq); break;
+        case 2: k_g2p_temp<R, 2><<<nb, kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, ut, uq); break;
+        case 3: k_g2p_temp<R, 3><<<nb, kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, ut, uq); break;
+        default: k_g2p_temp<R, 0><<<nb, kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, ut, uq); break;
     }
     EXG_CUDA_OK(cudaGetLastError());
 }

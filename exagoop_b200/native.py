@@ -36,6 +36,9 @@ R_TEMPERATURE, R_SPHEAT, R_THERMCOND, R_HEATFLUX, R_HEATSRC = 46, 47, 48, 49, 52
 I_PHASE, I_RIGID_ID, I_MODEL = 0, 1, 2
 # nodal components (constants.H:30-64)
 N_MASS, N_VEL, N_FRC, N_DVEL, N_MASS_OLD = 0, 1, 4, 7, 10
+N_MASS_SPHEAT, N_MASS_SPHEAT_TEMP, N_TEMPERATURE, N_SOURCE_TEMP, N_DELTA_TEMPERATURE, N_MASS_COND = 20, 21, 22, 23, 24, 25
+# thermal wall BC codes (mpm_specs.H bc_temp_*)
+BCT_PERIODIC, BCT_ISOTHERMAL, BCT_ADIABATIC, BCT_USERFLUX, BCT_CONVECTION = 0, 1, 2, 3, 4
 BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_PARTIALSLIP, BC_OUTFLOW = 0, 1, 2, 3, 4
 
 
@@ -374,6 +377,26 @@ class Context:
 
     def Calculate_MP_Stress_Strain(self, time: float, dt: float):
         self._ck(self.L.exg_calculate_mp_stress_strain(self.h, time, dt), "exg_calculate_mp_stress_strain")
+
+    # --- thermal step functions (Source/utilities.H, USE_TEMP)
+    def P2G_Temperature(self, reset=1, update_temp=1, update_source=1):
+        self._ck(self.L.exg_p2g_temperature(self.h, reset, update_temp, update_source), "exg_p2g_temperature")
+
+    def backup_current_temperature(self):
+        self._ck(self.L.exg_backup_current_temperature(self.h), "exg_backup_current_temperature")
+
+    def Nodal_Time_Update_Temperature(self, dt: float):
+        self._ck(self.L.exg_nodal_time_update_temperature(self.h, dt), "exg_nodal_time_update_temperature")
+
+    def Apply_Nodal_BCs_Temperature(self, dt: float, time: float, dirichlet_only: int = 0):
+        self._ck(self.L.exg_apply_nodal_bcs_temperature(self.h, dt, time, dirichlet_only),
+                 "exg_apply_nodal_bcs_temperature")
+
+    def store_delta_temperature(self):
+        self._ck(self.L.exg_store_delta_temperature(self.h), "exg_store_delta_temperature")
+
+    def G2P_Temperature(self, update_temperature: int, update_heatflux: int):
+        self._ck(self.L.exg_g2p_temperature(self.h, update_temperature, update_heatflux), "exg_g2p_temperature")
 
     # --- fused path
     def step(self, nsteps: int = 1):

@@ -180,3 +180,53 @@ def twisted_column(n=(64, 64, 384), size=(0.2, 0.2, 1.2), col=(0.1, 0.1, 0.6), s
     s.bodies[0].mom_bc = nt.BC_NOSLIP
     phi = sphere_union_levelset(s, centers, radii)
     return s, p, phi
+
+
+def heated_block(n=(24, 16, 20), size=(1.2, 0.8, 1.0), fill=0.7, order=2, seed=7, precision=nt.PREC_FP64,
+                 body_bc=0):
+    """Thermo-mechanical block (mpm.use_temp = 1): a linear-elastic block
+    (E = 1e4, nu = 0.25, rho = 2000) filling x, y and the lower `fill` of z,
+    2x2x2 particles per cell jittered by +-0.2 dx; seeded temperatures
+    300 +- 20 K, cp = 900, k = 50, heat sources 1e5 W/m^3 +- 50 %, heat
+    fluxes and velocities of seeded noise; gravity -9.81 in z, slip walls.
+    Thermal walls: x-lo isothermal 350 K, x-hi convective (h = 20,
+    T_inf = 290 K), y-lo user flux 500 W/m^2, y-hi adiabatic, z-lo
+    isothermal 280 K, z-hi convective.  body_bc > 0 adds a sphere body
+    (r = 0.25 at the block centre) with that thermal BC (1 isothermal
+    320 K, 3 heat flux 2e3 W/m^2, 4 convective h = 50, T_inf = 310 K).
+    Returns (specs, particles, phi or None)."""
+    dx = tuple(size[d] / n[d] for d in range(3))
+    s = base_specs((0, 0, 0), size, n, order, precision)
+    s.gravity[2] = -9.81
+    s.alpha_pic_flip = 0.95
+    s.cfl = 0.2
+    s.use_temp = 1
+    s.bclo_temp[0], s.T_wall_lo[0] = nt.BCT_ISOTHERMAL, 350.0
+    s.bchi_temp[0], s.h_hi[0], s.Tinf_hi[0] = nt.BCT_CONVECTION, 20.0, 290.0
+    s.bclo_temp[1], s.flux_lo[1] = nt.BCT_USERFLUX, 500.0
+    s.bchi_temp[1] = nt.BCT_ADIABATIC
+    s.bclo_temp[2], s.T_wall_lo[2] = nt.BCT_ISOTHERMAL, 280.0
+    s.bchi_temp[2], s.h_hi[2], s.Tinf_hi[2] = nt.BCT_CONVECTION, 5.0, 300.0
+    hi = (size[0], size[1], fill * size[2])
+    pos = lattice((0, 0, 0), hi, dx, (2, 2, 2))
+    rng = np.random.default_rng(seed)
+    pos = pos + rng.uniform(-0.2, 0.2, size=pos.shape) * np.array(dx)[:, None]
+    for d in range(3):
+        pos[d] = np.clip(pos[d], 1e-9 * size[d], size[d] * (1 - 1e-9))
+    p = make_particles(pos, dx, (2, 2, 2), 2000.0, 0, E=1e4, nu=0.25)
+    p.rdata[nt.R_VEL:nt.R_VEL + 3] = rng.normal(0, 0.02, (3, p.n))
+    p.rdata[nt.R_TEMPERATURE] = 300.0 + rng.uniform(-20.0, 20.0, p.n)
+    p.rdata[nt.R_SPHEAT] = 900.0
+    p.rdata[nt.R_THERMCOND] = 50.0
+    p.rdata[nt.R_HEATSRC] = 1e5 * (1.0 + rng.uniform(-0.5, 0.5, p.n))
+    p.rdata[nt.R_HEATFLUX:nt.R_HEATFLUX + 3] = rng.normal(0, 100.0, (3, p.n))
+    phi = None
+    if body_bc:
+        s.num_bodies = 1
+        b = s.bodies[0]
+        b.mom_bc = nt.BC_SLIP
+        b.temp_bc = body_bc
+        b.T_wall, b.heat_flux, b.h_conv, b.T_inf = 320.0, 2e3, 50.0, 310.0
+        c = (size[0] / 2, size[1] / 2, fill * size[2] / 2)
+        phi = sphere_union_levelset(s, [c], [0.25])
+    return s, p, phi

@@ -1146,13 +1146,17 @@ void orc_apply_nodal_bcs_temperature(orc_ctx *o, double dt, double time, int dir
                 }
             }
         });
-    // nodal_levelset_bcs_temperature, nodal_data_ops.cpp:235-349
+    // nodal_levelset_bcs_temperature, nodal_data_ops.cpp:235-349.  The
+    // heat-flux and convective forms read a neighbour node that the same
+    // pass may write (the reference's ParallelFor races there); neighbours
+    // are read as they were before the body's pass.
     for (int b = 0; b < s.num_bodies; ++b) {
         if (!o->has_ls[b]) continue;
         const exg_body &body = s.bodies[b];
         int bc = body.temp_bc;
         if (bc == 0) continue;
         if (dirichlet_only && bc != 1) continue;
+        const std::vector<double> Tsnap = o->node[EXG_N_TEMPERATURE];
         for_nodes(o, [&](int i, int j, int k, int64_t n) {
             double xp[3] = {o->plo[0] + i * o->dx[0], o->plo[1] + j * o->dx[1], o->plo[2] + k * o->dx[2]};
             double lsval;
@@ -1180,7 +1184,7 @@ void orc_apply_nodal_bcs_temperature(orc_ctx *o, double dt, double time, int dir
             if (!o->s.periodic[dd] && (nb[dd] < -1 || nb[dd] > o->nc[dd] + 1)) return;
             double kn = k_node(n);
             bool ghost = !o->s.periodic[dd] && (nb[dd] < 0 || nb[dd] > o->nc[dd]);
-            double Tnb = ghost ? 0.0 : o->N(EXG_N_TEMPERATURE, o->nidx_w(nb[0], nb[1], nb[2]));
+            double Tnb = ghost ? 0.0 : Tsnap[o->nidx_w(nb[0], nb[1], nb[2])];
             if (bc == 3)
                 o->N(EXG_N_TEMPERATURE, n) = Tnb + body.heat_flux * o->dx[dd] / kn;
             else if (bc == 4) {
