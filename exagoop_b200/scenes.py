@@ -147,12 +147,15 @@ def sphere_union_levelset(specs, centers, radii) -> np.ndarray:
 
 
 def twisted_column(n=(64, 64, 384), size=(0.2, 0.2, 1.2), col=(0.1, 0.1, 0.6), seed=4321,
-                   precision=nt.PREC_MIXED, n_obstacles=20, rigid_frac=0.05, order=2):
-    """Twisted elastic column with obstacles: column col (E = 1e5, nu = 0.3,
-    rho = 1000) standing on a noslip base, initial angular velocity 10 rad/s
-    about its axis, seeded analytic sphere obstacles (r in [0.02, 0.05]) as one
-    union level-set body, a seeded fraction of particles flagged rigid,
-    quadratic B-splines.  Returns (specs, particles, phi)."""
+                   precision=nt.PREC_MIXED, n_obstacles=20, rigid_frac=0.05, order=2, heat=True):
+    """Twisted elastic column with obstacles and heat: column col (E = 1e5,
+    nu = 0.3, rho = 1000) standing on a noslip base, initial angular velocity
+    10 rad/s about its axis, seeded analytic sphere obstacles (r in
+    [0.02, 0.05]) as one union level-set body, a seeded fraction of particles
+    flagged rigid, quadratic B-splines; with heat, mpm.use_temp = 1 and
+    temperatures 300 K plus a seeded Gaussian perturbation of 1e-2 K,
+    conductivity 1 W/m/K, cp 1000 J/kg/K, adiabatic walls.  Returns (specs,
+    particles, phi)."""
     dx = tuple(size[d] / n[d] for d in range(3))
     s = base_specs((0, 0, 0), size, n, order, precision)
     s.bclo[2] = nt.BC_NOSLIP
@@ -167,6 +170,11 @@ def twisted_column(n=(64, 64, 384), size=(0.2, 0.2, 1.2), col=(0.1, 0.1, 0.6), s
     p.rdata[nt.R_VEL + 1] = omega * (p.pos[0] - cx)
     rng = np.random.default_rng(seed)
     p.idata[nt.I_PHASE] = (rng.random(p.n) < rigid_frac).astype(np.int32)
+    if heat:
+        s.use_temp = 1
+        p.rdata[nt.R_TEMPERATURE] = 300.0 + 1e-2 * rng.standard_normal(p.n)
+        p.rdata[nt.R_SPHEAT] = 1000.0
+        p.rdata[nt.R_THERMCOND] = 1.0
     centers, radii = [], []
     while len(centers) < n_obstacles:
         r = rng.uniform(0.02, 0.05)

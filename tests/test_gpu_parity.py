@@ -211,9 +211,20 @@ def test_fused_musl():
 
 
 def test_fused_levelset_obstacles():
-    s, p, phi = scenes.twisted_column(n=(16, 16, 48), precision=nt.PREC_FP64, n_obstacles=6)
+    s, p, phi = scenes.twisted_column(n=(16, 16, 48), precision=nt.PREC_FP64, n_obstacles=6, heat=False)
     ctx, o = run_both(s, p, 20, phi)
     check_particles(ctx.download(), o.download())
+
+
+def test_fused_twisted_column_heat():
+    # the twisted column with its temperature field (rigid particles,
+    # obstacles, noslip base, thermal deposit and G2P every step)
+    s, p, phi = scenes.twisted_column(n=(16, 16, 48), precision=nt.PREC_FP64, n_obstacles=6, heat=True)
+    ctx, o = run_both(s, p, 20, phi)
+    g, r = ctx.download(), o.download()
+    check_particles(g, r, fields=[("vel", nt.R_VEL, 3), ("stress", nt.R_STRESS, 6), ("heatflux", nt.R_HEATFLUX, 3)])
+    e = np.abs(g.rdata[nt.R_TEMPERATURE] - r.rdata[nt.R_TEMPERATURE]).max()
+    assert e < TOL64 * 300.0, f"temperature: max abs err {e:.3e}"
 
 
 def test_fused_deterministic():

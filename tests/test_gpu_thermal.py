@@ -187,7 +187,14 @@ def test_fused_thermal_step(scheme, body_bc):
     ctx.step(10)
     assert o.step(10) == 0
     check_parts(ctx.download(), o.download(), FUSED_FIELDS)
-    check_nodes(ctx, o, [("temperature", nt.N_TEMPERATURE), ("delta_temperature", nt.N_DELTA_TEMPERATURE)])
+    # nodal T = (m cp T) / (m cp): the fixed-point deposit has absolute, not
+    # relative, precision, so nodes at the rim of the support (m cp below
+    # 1e-6 of its maximum, which particles weight by ~N as well) are left out
+    mc = o.nodes(nt.N_MASS_SPHEAT)
+    sel = mc >= 1e-6 * mc.max()
+    for name, comp in [("temperature", nt.N_TEMPERATURE), ("delta_temperature", nt.N_DELTA_TEMPERATURE)]:
+        e = rel(ctx.nodes(comp)[sel], o.nodes(comp)[sel])
+        assert e < TOL64, f"node {name}: max rel err {e:.3e}"
 
 
 def test_fused_thermal_udf():
