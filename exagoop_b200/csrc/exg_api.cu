@@ -127,8 +127,9 @@ void build_params_for(const exg_specs &s, Params &P) {
     P.T = T;
     P.tshift = ilog2(T);
     const bool lin = (P.uniform_order == 1);
+    P.dual = (P.uniform_order == 2);
     P.hlo = lin ? 0 : 1;
-    P.hhi = lin ? 1 : 2;
+    P.hhi = lin ? 1 : (P.dual ? 1 : 2);
     P.B = T + P.hlo + P.hhi;
     for (int d = 0; d < 3; ++d)
         P.ntile[d] = s.periodic[d] ? s.ncells[d] / T : (s.ncells[d] + 1 + T - 1) / T;

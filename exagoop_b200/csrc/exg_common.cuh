@@ -55,6 +55,8 @@ struct Ctl {
     int n_touched_tiles;
     long long n_sorted;                // particles inside the domain after the sort
     unsigned long long lost_fill;      // next slot for out-of-domain particles in the re-ordered storage
+    int next_p2g;                      // dynamic tile counter of the P2G kernel (reset by k_scales)
+    int next_g2p;                      // dynamic tile counter of the fused G2P (reset by k_nodes)
 };
 
 struct Body {
@@ -74,7 +76,8 @@ struct Params {
     int periodic[3];
     int order[3];
     int uniform_order;  // 1,2,3 when all axes share it, else 0
-    int T;              // tile edge (cells)
+    int dual;           // quadratic: particles binned by nearest node (3-node window per axis)
+    int T;              // tile edge (cells, or nearest-node bins when dual)
     int tshift;         // log2(T)
     int ntile[3];
     long long ntiles;
@@ -346,6 +349,22 @@ EXG_HD long long node_index(const Params &P, int i, int j, int k) {
 // Cell of a position: floor((x - plo) * dxi) (AMReX getParticleCell).
 EXG_HD void cell_of(const Params &P, const double x[3], int iv[3]) {
     for (int d = 0; d < 3; ++d) iv[d] = (int)floor((x[d] - P.plo[d]) * P.dxi[d]);
+}
+
+// Nearest-node bin along axis d: every node a quadratic B-spline of the
+// particle touches (support 1.5 dx for all boundary types) is bin-1..bin+1.
+// Periodic axes wrap bin ncells onto 0.
+EXG_HD int dual_bin_raw(const Params &P, int d, double x) { return (int)floor((x - P.plo[d]) * P.dxi[d] + 0.5); }
+EXG_HD int dual_bin(const Params &P, int d, double x) {
+    int b = dual_bin_raw(P, d, x);
+    if (P.periodic[d] && b >= P.nc[d]) b -= P.nc[d];
+    return b;
+}
+// Position used for the weights of a particle whose bin wrapped: shifted
+// one period down, so its window bin-1..bin+1 (and the bin's node block)
+// holds it.
+EXG_HD double dual_x(const Params &P, int d, double x) {
+    return (P.dual && P.periodic[d] && dual_bin_raw(P, d, x) >= P.nc[d]) ? x - (P.phi[d] - P.plo[d]) : x;
 }
 
 }  // namespace exg

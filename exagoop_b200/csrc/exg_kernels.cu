@@ -132,7 +132,10 @@ __device__ __forceinline__ void tile_coords(const Params &P, int t, int tc[3]) {
 // ---------------------------------------------------------------- K1 sort
 // Cell key per particle, with the periodic wrap of Redistribute.  Keys are
 // tile-major: (tile index << 3 log2 T) | (cell inside tile), so one tile's
-// particles are contiguous after a stable sort by key.
+// particles are contiguous after a stable sort by key.  With quadratic
+// B-splines the key's "cell" is the nearest-node bin (dual_bin): particles
+// of one bin share a 3x3x3 node window.  Particles outside the domain's
+// cells are dropped either way.
 __global__ void k_keys(Params P, double *x0, double *x1, double *x2, long long n, uint32_t *key, int *tile_count,
                        Ctl *ctl, int wrap) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -163,6 +166,8 @@ __global__ void k_keys(Params P, double *x0, double *x1, double *x2, long long n
             key[i] = 0xFFFFFFFFu;
             atomicAdd(&ctl->lost, 1ull);
         } else {
+            if (P.dual)
+                for (int d = 0; d < 3; ++d) iv[d] = dual_bin(P, d, x[d]);
             const int ts = P.tshift, m = P.T - 1;
             t = ((iv[2] >> ts) * P.ntile[1] + (iv[1] >> ts)) * P.ntile[0] + (iv[0] >> ts);
             uint32_t loc = (uint32_t)((((iv[2] & m) << ts) | (iv[1] & m)) << ts | (iv[0] & m));
@@ -360,9 +365,10 @@ __global__ void k_dt_finalize(Params P, Ctl *ctl, int reset) {
 
 // Fixed-point scales: a channel's node sum is bounded by
 // (particles per cell) x (stencil cells) x (largest per-particle term);
-// the scale 2^e keeps that bound below 2^61.
+// the scale 2^e keeps twice that bound below 2^55 (see fx_add_r).
 __global__ void k_scales(Ctl *ctl, int stencil_cells, const unsigned long long *bounds) {
     int c = threadIdx.x;
+    if (c == 0) ctl->next_p2g = 0;  // the P2G launch that follows takes tiles from 0
     if (c >= CH_ALL) return;
     double b = bitsd(bounds[c]);
     double S = b * (double)(ctl->maxppc > 0 ? ctl->maxppc : 1) * (double)stencil_cells * 2.0;
@@ -371,7 +377,7 @@ __global__ void k_scales(Ctl *ctl, int stencil_cells, const unsigned long long *
         int ex;
         frexp(S, &ex);  // S < 2^ex
         // 2^e stays inside FP32's range; a channel this small contributes 0
-        sc = ldexp(1.0, max(-100, min(100, 61 - ex)));
+        sc = ldexp(1.0, max(-100, min(100, 55 - ex)));
     }
     ctl->scale[c] = sc;
     ctl->inv_scale[c] = 1.0 / sc;
@@ -496,156 +502,22 @@ struct Stc {
     static constexpr int LO = (ORD == 1) ? 0 : -1;
 };
 
-// A 64-bit fixed-point accumulator kept as two 32-bit words (native
-// shared-memory atomics): the low word's returning add yields the carry
-// into the high word, so the pair always holds the exact 64-bit sum.
-__device__ __forceinline__ void fx_add(unsigned *lo, int *hi, int idx, double v, double sc) {
-    const long long q = __double2ll_rn(v * sc);
-    if (!q) return;
-    const unsigned l = (unsigned)(unsigned long long)q;
-    int h = (int)(q >> 32);
-    const unsigned old = atomicAdd(&lo[idx], l);
-    h += (old + l < old) ? 1 : 0;
-    if (h) atomicAdd(&hi[idx], h);
-}
-
 template <int W, class T>
 __device__ __forceinline__ T pick(const T (&a)[W], int i) {
     if (W == 2) return i ? a[1] : a[0];
     return i == 0 ? a[0] : (i == 1 ? a[1] : (i == 2 ? a[2] : a[W - 1]));
 }
 
-template <class R, int ORD, bool THERM>
-__global__ void __launch_bounds__(kThreads) k_p2g(Params P, Parts<R> A, const int *active, const int *start,
-                                                  const int *count, const int32_t *perm, long long *staging, Ctl *ctl,
-                                                  int flags) {
-    constexpr int W = Stc<ORD>::W, LO = Stc<ORD>::LO;
-    constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
-    const int B = P.B, B3 = B * B * B;
-    unsigned *acc_lo = reinterpret_cast<unsigned *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
-    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3);
-    load_tables(tab);
-    double sc[NCH];
-#pragma unroll
-    for (int c = 0; c < NCH; ++c) sc[c] = ctl->scale[c];
-    const bool fm = flags & PF_MASS, fv = flags & PF_VEL, ff = flags & PF_FORCE, fT = flags & PF_TEMP,
-               fS = flags & PF_SRC;
-    // lanes of one cell sit next to each other after the sort; rotating the
-    // stencil order by lane keeps them off the same node at the same time
-    const int lane = threadIdx.x & 31;
-    const int rx = lane & (W - 1), ry = (lane / W) & (W - 1), rz = (lane / (W * W)) & (W - 1);
-    const int nitems = ctl->n_active_tiles;
-    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
-        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) {
-            acc_lo[i] = 0u;
-            acc_hi[i] = 0;
-        }
-        __syncthreads();
-        const int t = active[w];
-        int tc[3];
-        tile_coords(P, t, tc);
-        const int org[3] = {tc[0] * P.T, tc[1] * P.T, tc[2] * P.T};
-        const int s0 = start[t], n = count[t];
-        for (int k = s0 + threadIdx.x; k < s0 + n; k += blockDim.x) {
-            const int p = perm[k];
-            if (A.phase[p] != 0) continue;
-            const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
-            int iv[3];
-            cell_of(P, x, iv);
-            AxisW<R, W> ax, ay, az;
-            axis_weights<R, W, LO>(*tab, P, 0, x[0], iv[0], ax);
-            axis_weights<R, W, LO>(*tab, P, 1, x[1], iv[1], ay);
-            axis_weights<R, W, LO>(*tab, P, 2, x[2], iv[2], az);
-            const int lx = iv[0] - org[0], ly = iv[1] - org[1], lz = iv[2] - org[2];
-            const R m = A.mass[p], vol = A.vol[p];
-            R mv[3], mg[3], ext[3], s[6];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                mv[d] = m * A.v[d][p];
-                mg[d] = m * (R)P.gravity[d];
-            }
-            const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
-                              x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] && x[2] < P.slab_hi[2];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) ext[d] = slab ? (R)P.extforce[d] : R(0);
-#pragma unroll
-            for (int c = 0; c < 6; ++c) s[c] = A.sig[c][p];
-            R mcp = R(0), mcpT = R(0), mk = R(0), qv[3] = {R(0), R(0), R(0)}, VQ = R(0);
-            if (THERM) {
-                mcp = m * A.cp[p];
-                mcpT = (R)(mcp * A.T[p]);
-                mk = m * A.kc[p];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) qv[d] = A.q[d][p];
-                VQ = vol * A.Q[p];
-            }
-#pragma unroll
-            for (int iz = 0; iz < W; ++iz) {
-                const int sz = (iz + rz) & (W - 1);
-                const R wz = pick<W>(az.w, sz), dz = pick<W>(az.dw, sz);
-                if (wz == R(0) && dz == R(0)) continue;
-#pragma unroll
-                for (int iy = 0; iy < W; ++iy) {
-                    const int sy = (iy + ry) & (W - 1);
-                    const R wy = pick<W>(ay.w, sy), dy = pick<W>(ay.dw, sy);
-                    if (wy == R(0) && dy == R(0)) continue;
-#pragma unroll
-                    for (int ix = 0; ix < W; ++ix) {
-                        const int sx = (ix + rx) & (W - 1);
-                        const R wx = pick<W>(ax.w, sx), dx = pick<W>(ax.dw, sx);
-                        if (wx == R(0) && dx == R(0)) continue;
-                        const R N = wx * wy * wz;
-                        const int idx = ((lz + sz) * B + (ly + sy)) * B + (lx + sx);
-                        if (fm) fx_add(acc_lo, acc_hi, CH_M * B3 + idx, (double)(m * N), sc[CH_M]);
-                        if (fv) {
-#pragma unroll
-                            for (int d = 0; d < 3; ++d)
-                                fx_add(acc_lo, acc_hi, (CH_P + d) * B3 + idx, (double)(mv[d] * N), sc[CH_P + d]);
-                        }
-                        if (ff || (THERM && fS)) {
-                            const R g[3] = {dx * wy * wz, wx * dy * wz, wx * wy * dz};
-                            if (ff) {
-                                const R tv[3] = {s[0] * g[0] + s[1] * g[1] + s[2] * g[2],
-                                                 s[1] * g[0] + s[3] * g[1] + s[4] * g[2],
-                                                 s[2] * g[0] + s[4] * g[1] + s[5] * g[2]};
-#pragma unroll
-                                for (int d = 0; d < 3; ++d)
-                                    fx_add(acc_lo, acc_hi, (CH_F + d) * B3 + idx,
-                                           (double)((mg[d] * N + ext[d] * N) + (-vol * tv[d])), sc[CH_F + d]);
-                            }
-                            if (THERM && fS) {
-                                const R net = qv[0] * g[0] + qv[1] * g[1] + qv[2] * g[2];
-                                fx_add(acc_lo, acc_hi, CH_SRC * B3 + idx, (double)(net * vol + VQ * N), sc[CH_SRC]);
-                            }
-                        }
-                        if (THERM && fT) {
-                            fx_add(acc_lo, acc_hi, CH_MC * B3 + idx, (double)(mcp * N), sc[CH_MC]);
-                            fx_add(acc_lo, acc_hi, CH_MCT * B3 + idx, (double)(mcpT * N), sc[CH_MCT]);
-                            fx_add(acc_lo, acc_hi, CH_MK * B3 + idx, (double)(mk * N), sc[CH_MK]);
-                        }
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        long long *dst = staging + (long long)w * NCH * B3;
-        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x)
-            dst[i] = (long long)((((unsigned long long)(unsigned)acc_hi[i]) << 32) + (unsigned long long)acc_lo[i]);
-        __syncthreads();
-    }
-}
-
 // ---------------------------------------------------------------- K2 per-cell P2G
-// The same deposit with one thread per cell: the thread walks its cell's
-// particles (contiguous after the sort) in storage order and accumulates
-// their contributions to one z-slice of the cell's stencil in registers;
-// only the per-cell sums go to shared memory, as 64-bit fixed point.  The
-// summation order inside a cell is fixed and the cross-cell sums are exact,
-// so the result is deterministic; shared-memory atomics drop by the
-// particles-per-cell factor and lanes never collide (a warp's lanes own
-// different cells and add the same stencil offset at the same time).
+// P2G with one thread per cell (nearest-node bin for quadratic): the thread
+// walks its cell's particles (contiguous after the sort) in storage order
+// and accumulates their contributions to rows of one z-slice of the cell's
+// stencil in registers; only the per-cell sums go to the tile's node block
+// in shared memory, as 64-bit fixed point.  The summation order inside a
+// cell is fixed and the cross-cell sums are exact, so the result is
+// deterministic; shared-memory atomics drop by the particles-per-cell factor
+// and lanes never collide (a warp's lanes own different cells and add the
+// same stencil offset at the same time).
 template <class R>
 __device__ __forceinline__ long long to_fixed(R v, R sc);
 template <>
@@ -657,20 +529,23 @@ __device__ __forceinline__ long long to_fixed<double>(double v, double sc) {
     return __double2ll_rn(v * sc);
 }
 
+// A node's fixed-point sum is kept as two 32-bit words without carries:
+// lo collects the low 24 bits of each addend (at most 64 addends per node
+// and tile, so lo < 2^30) and hi the arithmetic upper part (the scale keeps
+// every node sum below 2^55, so hi fits 32 bits); the 64-bit value is
+// hi * 2^24 + lo.  Both adds are fire-and-forget reductions.
 template <class R>
 __device__ __forceinline__ void fx_add_r(unsigned *lo, int *hi, int idx, R v, R sc) {
     const long long q = to_fixed<R>(v, sc);
     if (!q) return;
-    const unsigned l = (unsigned)(unsigned long long)q;
-    int h = (int)(q >> 32);
-    const unsigned old = atomicAdd(&lo[idx], l);
-    h += (old + l < old) ? 1 : 0;
+    atomicAdd(&lo[idx], (unsigned)(q & 0xFFFFFFll));
+    const int h = (int)(q >> 24);
     if (h) atomicAdd(&hi[idx], h);
 }
 
 // Per-axis weights of a cell whose stencil nodes are all interior (shape
-// type 3): the polynomial piece of each stencil offset is fixed (cubic) or
-// picked by f < 1/2 (quadratic); same coefficients as the tables.
+// type 3): the polynomial piece of each stencil offset is fixed (linear,
+// cubic; quadratic uses dual_axis_weights); same coefficients as the tables.
 template <class R, int ORD>
 __device__ __forceinline__ void axis_weights_interior(const Params &P, int d, double x, int i,
                                                       AxisW<R, Stc<ORD>::W> &a) {
@@ -681,21 +556,6 @@ __device__ __forceinline__ void axis_weights_interior(const Params &P, int d, do
         a.w[1] = f;
         a.dw[0] = -dxinv;
         a.dw[1] = dxinv;
-    } else if (ORD == 2) {
-        // type-3 quadratic pieces: p0 = .5z^2+1.5z+1.125, p1 = -z^2+.75, p2 = .5z^2-1.5z+1.125
-        R z = f + R(1);
-        const bool lo = f < R(0.5);
-        a.w[0] = lo ? (R(0.5) * z * z + R(-1.5) * z + R(1.125)) : R(0);
-        a.dw[0] = lo ? (z - R(1.5)) * dxinv : R(0);
-        z = f;
-        a.w[1] = lo ? (R(-1) * z * z + R(0) * z + R(0.75)) : (R(0.5) * z * z + R(-1.5) * z + R(1.125));
-        a.dw[1] = (lo ? (R(-2) * z) : (z - R(1.5))) * dxinv;
-        z = f - R(1);
-        a.w[2] = lo ? (R(0.5) * z * z + R(1.5) * z + R(1.125)) : (R(-1) * z * z + R(0) * z + R(0.75));
-        a.dw[2] = (lo ? (z + R(1.5)) : (R(-2) * z)) * dxinv;
-        z = f - R(2);
-        a.w[3] = lo ? R(0) : (R(0.5) * z * z + R(1.5) * z + R(1.125));
-        a.dw[3] = lo ? R(0) : (z + R(1.5)) * dxinv;
     } else {
         // type-3 cubic pieces, interval 3 - s for stencil slot s
         const R o6 = (R)kOneBySix, t3 = (R)kTwoByThree, f3 = (R)kFourByThree;
@@ -726,16 +586,82 @@ __device__ __forceinline__ void cell_axis_weights(const SplineTables &tab, const
         axis_weights<R, Stc<ORD>::W, Stc<ORD>::LO>(tab, P, d, x, i, a);
 }
 
+// Quadratic weights on the 3-node window bin-1..bin+1 of a nearest-node bin
+// (dual_bin).  Interior bins (all three nodes of shape type 3) use the fixed
+// pieces; elsewhere each node's own piece comes from the tables, and nodes
+// outside the domain get 0, which is what compute_bounds leaves out
+// (mpm_particle_grid_ops.cpp:255-299): every in-domain node outside the
+// window is at least 1.5 dx away and has weight 0 for every shape type.
+template <class R>
+__device__ __forceinline__ void dual_axis_weights(const SplineTables &tab, const Params &P, int d, double x, int n0,
+                                                  bool interior, AxisW<R, 3> &a) {
+    const R dxinv = (R)P.dxi[d];
+    if (interior) {
+        const R u = (R)((x - (P.plo[d] + n0 * P.dx[d])) * P.dxi[d]);
+        R z = u + R(1);  // node n0-1, piece [0.5, 1.5]
+        a.w[0] = R(0.5) * z * z + R(-1.5) * z + R(1.125);
+        a.dw[0] = (z - R(1.5)) * dxinv;
+        z = u;  // node n0, piece [-0.5, 0.5]
+        a.w[1] = R(-1) * z * z + R(0) * z + R(0.75);
+        a.dw[1] = (R(-2) * z) * dxinv;
+        z = u - R(1);  // node n0+1, piece [-1.5, -0.5]
+        a.w[2] = R(0.5) * z * z + R(1.5) * z + R(1.125);
+        a.dw[2] = (z + R(1.5)) * dxinv;
+        return;
+    }
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        const int n = n0 - 1 + s;
+        R val = R(0), der = R(0);
+        if (P.periodic[d] || (n >= 0 && n <= P.nc[d])) {
+            const int ty = shape_type(n, P.nc[d], P.periodic[d]);
+            const R r = (R)((x - (P.plo[d] + n * P.dx[d])) * P.dxi[d]);
+            spline_eval<R>(tab, 2, ty, r, val, der);
+            der *= dxinv;
+        }
+        a.w[s] = val;
+        a.dw[s] = der;
+    }
+}
+
+// Stencil width of the per-cell P2G: cells (linear, cubic, mixed orders) or
+// nearest-node bins (uniform quadratic).  The block index of stencil slot s
+// is (local cell or bin) + s in every case.
+template <int ORD>
+struct P2GStc {
+    static constexpr int W = (ORD == 1) ? 2 : (ORD == 2 ? 3 : 4);
+};
+
+template <class R, int ORD>
+__device__ __forceinline__ void p2g_axis_weights(const SplineTables &tab, const Params &P, int d, double x, int i,
+                                                 bool interior, AxisW<R, P2GStc<ORD>::W> &a) {
+    if constexpr (ORD == 2)
+        dual_axis_weights<R>(tab, P, d, x, i, interior, a);
+    else
+        cell_axis_weights<R, ORD>(tab, P, d, x, i, interior, a);
+}
+
 constexpr int kCellThreads = 128;
 
+// Threads per block and register cap of the per-cell P2G: the 3-wide
+// quadratic accumulators fit 128 registers at 256 threads.
 template <class R, int ORD, bool THERM>
-__global__ void __launch_bounds__(kCellThreads) k_p2g_cell(Params P, Parts<R> A, const int *active, const int *start,
-                                                           const int *cell_start, const int32_t *perm,
-                                                           long long *staging, Ctl *ctl, int flags) {
-    constexpr int W = Stc<ORD>::W;
-    constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
+struct P2GCfg {
+    static constexpr int W = P2GStc<ORD>::W;
     // y rows of the stencil slice accumulated per pass (register budget)
-    constexpr int ROWS = (sizeof(R) == 8) ? 1 : ((THERM && W == 4) ? 2 : W);
+    static constexpr int ROWS = (sizeof(R) == 8) ? 1 : (THERM ? (W == 4 ? 2 : 1) : W);
+    static constexpr int THREADS = (ORD == 2) ? 256 : kCellThreads;
+    static constexpr int MINB = (ORD == 2) ? 2 : 1;
+};
+
+template <class R, int ORD, bool THERM>
+__global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD, THERM>::MINB)
+    k_p2g_cell(Params P, Parts<R> A, const int *active, const int *start, const int *cell_start, const int32_t *perm,
+               long long *staging, Ctl *ctl, int flags) {
+    constexpr int W = P2GCfg<R, ORD, THERM>::W;
+    constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
+    constexpr int ROWS = P2GCfg<R, ORD, THERM>::ROWS;
+    __shared__ int s_item;
     extern __shared__ __align__(16) unsigned char smraw[];
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
     const int B = P.B, B3 = B * B * B, T = P.T, T3 = T * T * T;
@@ -751,12 +677,17 @@ __global__ void __launch_bounds__(kCellThreads) k_p2g_cell(Params P, Parts<R> A,
 #pragma unroll
     for (int d = 0; d < 3; ++d) grav[d] = (R)P.gravity[d];
     const int nitems = ctl->n_active_tiles;
-    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    for (;;) {
+        // tiles are taken in turn from a device counter: blocks that drew
+        // light tiles take more of them
+        if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_p2g, 1);
         for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) {
             acc_lo[i] = 0u;
             acc_hi[i] = 0;
         }
         __syncthreads();
+        const int w = s_item;
+        if (w >= nitems) break;
         const int t = active[w];
         int tc[3];
         tile_coords(P, t, tc);
@@ -770,7 +701,8 @@ __global__ void __launch_bounds__(kCellThreads) k_p2g_cell(Params P, Parts<R> A,
             bool inter[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-                inter[d] = (ORD == 1) || P.periodic[d] || (iv[d] >= 3 && iv[d] <= P.nc[d] - 4);
+                inter[d] = (ORD == 1) || P.periodic[d] ||
+                           (ORD == 2 ? (iv[d] >= 3 && iv[d] <= P.nc[d] - 3) : (iv[d] >= 3 && iv[d] <= P.nc[d] - 4));
             for (int sz = 0; sz < W; ++sz) {
 #pragma unroll
                 for (int sy0 = 0; sy0 < W; sy0 += ROWS) {
@@ -787,13 +719,13 @@ __global__ void __launch_bounds__(kCellThreads) k_p2g_cell(Params P, Parts<R> A,
                         if (A.phase[p] != 0) continue;
                         const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
                         AxisW<R, W> az;
-                        cell_axis_weights<R, ORD>(*tab, P, 2, x[2], iv[2], inter[2], az);
+                        p2g_axis_weights<R, ORD>(*tab, P, 2, dual_x(P, 2, x[2]), iv[2], inter[2], az);
                         const R wz = pick<W>(az.w, sz), dzw = pick<W>(az.dw, sz);
                         if (wz == R(0) && dzw == R(0)) continue;
                         any = true;
                         AxisW<R, W> ax, ay;
-                        cell_axis_weights<R, ORD>(*tab, P, 0, x[0], iv[0], inter[0], ax);
-                        cell_axis_weights<R, ORD>(*tab, P, 1, x[1], iv[1], inter[1], ay);
+                        p2g_axis_weights<R, ORD>(*tab, P, 0, dual_x(P, 0, x[0]), iv[0], inter[0], ax);
+                        p2g_axis_weights<R, ORD>(*tab, P, 1, dual_x(P, 1, x[1]), iv[1], inter[1], ay);
                         const R m = A.mass[p], vol = A.vol[p];
                         R mv[3], bf[3], s[6];
                         const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
@@ -863,7 +795,7 @@ __global__ void __launch_bounds__(kCellThreads) k_p2g_cell(Params P, Parts<R> A,
         __syncthreads();
         long long *dst = staging + (long long)w * NCH * B3;
         for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x)
-            dst[i] = (long long)((((unsigned long long)(unsigned)acc_hi[i]) << 32) + (unsigned long long)acc_lo[i]);
+            dst[i] = (long long)acc_hi[i] * (1ll << 24) + (long long)acc_lo[i];
         __syncthreads();
     }
 }
@@ -1007,6 +939,9 @@ __global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeB
 #pragma unroll
     for (int c = 0; c < NCH; ++c) isc[c] = ctl->inv_scale[c];
     const int T = P.T;
+    // the fused G2P that follows takes its tiles from 0 (it starts after
+    // this kernel ends, and the previous one has ended)
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->next_g2p = 0;
     const int nitems = tiles ? ctl->n_touched_tiles : (int)P.ntiles;
     for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
     const int t = tiles ? tiles[w] : w;
@@ -1264,11 +1199,26 @@ template <class R, int ORD, class NodeAcc>
 __device__ __forceinline__ void g2p_particle_generic(const SplineTables &tab, const Params &P, const NodeAcc &na,
                                              const double x[3], const int iv[3], bool upd_vel, bool upd_sr, R v[3],
                                              R vp[3], R E[9], R sr[6], double dt) {
-    constexpr int W = Stc<ORD>::W, LO = Stc<ORD>::LO;
+    // uniform quadratic: the 3-node window of the nearest-node bin (every
+    // node with a non-zero weight), the same bin as the sort key's
+    constexpr int W = (ORD == 2) ? 3 : Stc<ORD>::W, LO = Stc<ORD>::LO;
     AxisW<R, W> ax, ay, az;
-    axis_weights<R, W, LO>(tab, P, 0, x[0], iv[0], ax);
-    axis_weights<R, W, LO>(tab, P, 1, x[1], iv[1], ay);
-    axis_weights<R, W, LO>(tab, P, 2, x[2], iv[2], az);
+    int base[3];
+    if constexpr (ORD == 2) {
+        AxisW<R, W> *a[3] = {&ax, &ay, &az};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int n0 = dual_bin(P, d, x[d]);
+            dual_axis_weights<R>(tab, P, d, dual_x(P, d, x[d]), n0, false, *a[d]);
+            base[d] = n0 - 1;
+        }
+    } else {
+        axis_weights<R, W, LO>(tab, P, 0, x[0], iv[0], ax);
+        axis_weights<R, W, LO>(tab, P, 1, x[1], iv[1], ay);
+        axis_weights<R, W, LO>(tab, P, 2, x[2], iv[2], az);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) base[d] = iv[d] + LO;
+    }
     R vpic[3] = {R(0), R(0), R(0)}, dpic[3] = {R(0), R(0), R(0)};
     R gv[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
     const bool generic = (ORD == 0);
@@ -1283,7 +1233,7 @@ __device__ __forceinline__ void g2p_particle_generic(const SplineTables &tab, co
                 if (wx == R(0) && dx == R(0)) continue;
                 if (wy == R(0) && dy == R(0)) continue;
                 if (wz == R(0) && dz == R(0)) continue;
-                const int ni = iv[0] + LO + sx, nj = iv[1] + LO + sy, nk = iv[2] + LO + sz;
+                const int ni = base[0] + sx, nj = base[1] + sy, nk = base[2] + sz;
                 const R nv[3] = {na.get(0, ni, nj, nk), na.get(1, ni, nj, nk), na.get(2, ni, nj, nk)};
                 if (upd_vel && !generic) {
                     const R N = wx * wy * wz;
@@ -1320,27 +1270,6 @@ __device__ __forceinline__ void g2p_particle_generic(const SplineTables &tab, co
         }
     }
     g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt);
-}
-
-// Quadratic interior weights on the 3-node window that holds the support:
-// offsets -1..1 when f < 1/2, else 0..2 (the fourth offset's weight is 0).
-// Returns the stencil offset of window entry 0.
-template <class R>
-__device__ __forceinline__ int quad_window(const Params &P, int d, double x, int i, R w[3], R dw[3]) {
-    const R f = (R)((x - (P.plo[d] + i * P.dx[d])) * P.dxi[d]);
-    const R dxinv = (R)P.dxi[d];
-    const bool lo = f < R(0.5);
-    const R u = lo ? f : f - R(1);
-    R z = u + R(1);
-    w[0] = R(0.5) * z * z + R(-1.5) * z + R(1.125);
-    dw[0] = (z - R(1.5)) * dxinv;
-    z = u;
-    w[1] = R(-1) * z * z + R(0) * z + R(0.75);
-    dw[1] = (R(-2) * z) * dxinv;
-    z = u - R(1);
-    w[2] = R(0.5) * z * z + R(1.5) * z + R(1.125);
-    dw[2] = (z + R(1.5)) * dxinv;
-    return lo ? -1 : 0;
 }
 
 // Interpolation over a WN^3 window of the shared-memory node block.
@@ -1395,6 +1324,25 @@ template <class R, int ORD>
 __device__ __forceinline__ void g2p_particle_smem(const SplineTables &tab, const Params &P, const SmemNodes<R> &na,
                                                   const double x[3], const int iv[3], bool upd_vel, bool upd_sr,
                                                   R v[3], R vp[3], R E[9], R sr[6], double dt) {
+    R vpic[3] = {R(0), R(0), R(0)}, dpic[3] = {R(0), R(0), R(0)};
+    R gv[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
+    if constexpr (ORD == 2) {
+        // the window of the particle's nearest-node bin (the bin its tile
+        // was sorted by), fixed pieces on interior axes
+        AxisW<R, 3> a[3];
+        int base[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int n0 = dual_bin(P, d, x[d]);
+            const bool in = P.periodic[d] || (n0 >= 3 && n0 <= P.nc[d] - 3);
+            dual_axis_weights<R>(tab, P, d, dual_x(P, d, x[d]), n0, in, a[d]);
+            base[d] = n0 - 1;
+        }
+        g2p_window<R, 3>(na, base, a[0].w, a[0].dw, a[1].w, a[1].dw, a[2].w, a[2].dw, upd_vel, upd_sr, vpic, dpic,
+                         gv);
+        g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt);
+        return;
+    }
     bool inter = (ORD != 0);
 #pragma unroll
     for (int d = 0; d < 3; ++d)
@@ -1403,15 +1351,7 @@ __device__ __forceinline__ void g2p_particle_smem(const SplineTables &tab, const
         g2p_particle_generic<R, ORD>(tab, P, na, x, iv, upd_vel, upd_sr, v, vp, E, sr, dt);
         return;
     }
-    R vpic[3] = {R(0), R(0), R(0)}, dpic[3] = {R(0), R(0), R(0)};
-    R gv[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
-    if (ORD == 2) {
-        R w[3][3], dw[3][3];
-        int base[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) base[d] = iv[d] + quad_window<R>(P, d, x[d], iv[d], w[d], dw[d]);
-        g2p_window<R, 3>(na, base, w[0], dw[0], w[1], dw[1], w[2], dw[2], upd_vel, upd_sr, vpic, dpic, gv);
-    } else if (ORD == 1 || ORD == 3) {
+    if (ORD == 1 || ORD == 3) {
         constexpr int WN = (ORD == 1) ? 2 : 4;
         constexpr int OW = (ORD == 0) ? 3 : ORD;  // keeps the template argument valid when ORD == 0
         AxisW<R, WN> a[3];
@@ -1567,7 +1507,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_g2p_fused(Params P, Parts<R> A,
     double run_dt = 1.7976931348623157e308;
     bool red = false;
     const int nitems = ctl->n_active_tiles;
-    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    __shared__ int s_item;
+    for (;;) {
+    // tiles are taken in turn from a device counter (reset by k_nodes)
+    if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_g2p, 1);
+    __syncthreads();
+    const int w = s_item;
+    if (w >= nitems) break;
     const int t = active[w];
     int tc[3];
     tile_coords(P, t, tc);
@@ -2381,7 +2327,7 @@ void launch_dt_finalize(Ctx &c, bool reset) {
 }
 
 void launch_scales_from(Ctx &c, const unsigned long long *bounds) {
-    const int W = (c.P.uniform_order == 1) ? 2 : 4;
+    const int W = (c.P.uniform_order == 1) ? 2 : (c.P.dual ? 3 : 4);
     k_scales<<<1, 32, 0, c.stream>>>(c.ctl, W * W * W, bounds);
     EXG_CUDA_OK(cudaGetLastError());
 }
@@ -2416,6 +2362,7 @@ static void p2g_cell_t(Ctx &c, int flags) {
     const int B3 = c.P.B * c.P.B * c.P.B;
     size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * NCH * B3;
     auto kern = k_p2g_cell<R, ORD, TH>;
+    constexpr int nthr = P2GCfg<R, ORD, TH>::THREADS;
     EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     static int grid = 0;
     static size_t gsm = 0;
@@ -2423,36 +2370,20 @@ static void p2g_cell_t(Ctx &c, int flags) {
         int dev = 0, nsm = 0, per = 0;
         EXG_CUDA_OK(cudaGetDevice(&dev));
         EXG_CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        EXG_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kCellThreads, sm));
+        EXG_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, nthr, sm));
         grid = nsm * (per < 1 ? 1 : per);
         gsm = sm;
     }
-    kern<<<grid, kCellThreads, sm, c.stream>>>(c.P, c.A<R>(), c.sb.active, c.sb.tile_start, c.sb.cell_start,
-                                               c.sb.perm, c.staging, c.ctl, flags);
+    kern<<<grid, nthr, sm, c.stream>>>(c.P, c.A<R>(), c.sb.active, c.sb.tile_start, c.sb.cell_start, c.sb.perm,
+                                       c.staging, c.ctl, flags);
     EXG_CUDA_OK(cudaGetLastError());
 }
 
 template <class R, int ORD, bool TH>
 static void p2g_t(Ctx &c, int flags) {
-    if (!std::getenv("EXG_P2G_ATOMIC")) {
-        p2g_cell_t<R, ORD, TH>(c, flags);
-        return;
-    }
-    const int NCH = TH ? CH_ALL : CH_MOM_END;
-    const int B3 = c.P.B * c.P.B * c.P.B;
-    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * NCH * B3;
-    auto kern = k_p2g<R, ORD, TH>;
-    EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    static int grid = 0;
-    static size_t gsm = 0;
-    if (!grid || gsm != sm) {
-        grid = persistent_grid(kern, sm);
-        gsm = sm;
-    }
-    kern<<<grid, kThreads, sm, c.stream>>>(c.P, c.A<R>(), c.sb.active, c.sb.tile_start, c.sb.tile_count, c.sb.perm,
-                                           c.staging, c.ctl, flags);
-    EXG_CUDA_OK(cudaGetLastError());
+    p2g_cell_t<R, ORD, TH>(c, flags);
 }
+
 void EXG_SFX(launch_p2g)(Ctx &c, int flags) {
     using R = EXG_R;
     const bool th = (flags & (PF_TEMP | PF_SRC)) != 0;

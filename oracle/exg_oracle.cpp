@@ -1345,8 +1345,12 @@ void orc_diagnostics(orc_ctx *o, exg_diag *out) {
 // tiles per axis, x fastest) times T^3 plus the cell's index inside the tile
 // (x fastest).  Particles outside the domain get 0xFFFFFFFF.
 void orc_sort_keys(orc_ctx *o, int T, uint32_t *keys, int32_t *perm) {
+    // the B200 binning: cells, or with uniform quadratic B-splines the
+    // nearest node floor((x - plo) / dx + 1/2) (wrapped on periodic axes);
+    // particles outside the domain's cells get the sentinel key
+    const bool dual = o->s.order[0] == 2 && o->s.order[1] == 2 && o->s.order[2] == 2;
     int nt[3];
-    for (int d = 0; d < 3; ++d) nt[d] = (o->nc[d] + 1 + T - 1) / T;
+    for (int d = 0; d < 3; ++d) nt[d] = o->s.periodic[d] ? o->nc[d] / T : (o->nc[d] + 1 + T - 1) / T;
     for (int64_t p = 0; p < o->np; ++p) {
         int iv[3];
         o->cell(p, iv);
@@ -1356,6 +1360,11 @@ void orc_sort_keys(orc_ctx *o, int T, uint32_t *keys, int32_t *perm) {
             keys[p] = 0xFFFFFFFFu;
             continue;
         }
+        if (dual)
+            for (int d = 0; d < 3; ++d) {
+                iv[d] = (int)std::floor((o->pos[d][p] - o->plo[d]) * o->dxi[d] + 0.5);
+                if (o->s.periodic[d] && iv[d] >= o->nc[d]) iv[d] -= o->nc[d];
+            }
         uint32_t tile = (uint32_t)((iv[2] / T) * nt[1] + iv[1] / T) * nt[0] + iv[0] / T;
         uint32_t loc = (uint32_t)(((iv[2] % T) * T + iv[1] % T) * T + iv[0] % T);
         keys[p] = tile * (uint32_t)(T * T * T) + loc;
