@@ -365,8 +365,8 @@ __global__ void k_dt_finalize(Params P, Ctl *ctl, int reset) {
 
 // Fixed-point scales: a channel's node sum is bounded by
 // (particles per cell) x (stencil cells) x (largest per-particle term);
-// the scale 2^e keeps twice that bound below 2^55 (see fx_add_r).
-__global__ void k_scales(Ctl *ctl, int stencil_cells, const unsigned long long *bounds) {
+// the scale 2^e keeps twice that bound below 2^bits (see fx_add_r).
+__global__ void k_scales(Ctl *ctl, int stencil_cells, int bits, const unsigned long long *bounds) {
     int c = threadIdx.x;
     if (c == 0) ctl->next_p2g = 0;  // the P2G launch that follows takes tiles from 0
     if (c >= CH_ALL) return;
@@ -377,7 +377,7 @@ __global__ void k_scales(Ctl *ctl, int stencil_cells, const unsigned long long *
         int ex;
         frexp(S, &ex);  // S < 2^ex
         // 2^e stays inside FP32's range; a channel this small contributes 0
-        sc = ldexp(1.0, max(-100, min(100, 55 - ex)));
+        sc = ldexp(1.0, max(-100, min(100, bits - ex)));
     }
     ctl->scale[c] = sc;
     ctl->inv_scale[c] = 1.0 / sc;
@@ -529,18 +529,35 @@ __device__ __forceinline__ long long to_fixed<double>(double v, double sc) {
     return __double2ll_rn(v * sc);
 }
 
-// A node's fixed-point sum is kept as two 32-bit words without carries:
-// lo collects the low 24 bits of each addend (at most 64 addends per node
-// and tile, so lo < 2^30) and hi the arithmetic upper part (the scale keeps
-// every node sum below 2^55, so hi fits 32 bits); the 64-bit value is
-// hi * 2^24 + lo.  Both adds are fire-and-forget reductions.
+// A node's fixed-point sum is kept in two 32-bit shared-memory words.
+// FP32 state (scale bound 2^55, kFxBits32): without carries, lo collects the
+// low 24 bits of each addend (at most 64 addends per node and tile, so
+// lo < 2^30) and hi the arithmetic upper part, which fits 32 bits; the value
+// is hi * 2^24 + lo and both adds are fire-and-forget reductions.  FP64
+// state (bound 2^61, kFxBits64, the full precision the FP64 path needs): the
+// low word's returning add yields the carry into the high word, and the
+// value is hi * 2^32 + lo.
+constexpr int kFxBits32 = 55, kFxBits64 = 61;
 template <class R>
 __device__ __forceinline__ void fx_add_r(unsigned *lo, int *hi, int idx, R v, R sc) {
     const long long q = to_fixed<R>(v, sc);
     if (!q) return;
-    atomicAdd(&lo[idx], (unsigned)(q & 0xFFFFFFll));
-    const int h = (int)(q >> 24);
-    if (h) atomicAdd(&hi[idx], h);
+    if (sizeof(R) == 4) {
+        atomicAdd(&lo[idx], (unsigned)(q & 0xFFFFFFll));
+        const int h = (int)(q >> 24);
+        if (h) atomicAdd(&hi[idx], h);
+    } else {
+        const unsigned l = (unsigned)(unsigned long long)q;
+        int h = (int)(q >> 32);
+        const unsigned old = atomicAdd(&lo[idx], l);
+        h += (old + l < old) ? 1 : 0;
+        if (h) atomicAdd(&hi[idx], h);
+    }
+}
+template <class R>
+__device__ __forceinline__ long long fx_value(unsigned lo, int hi) {
+    if (sizeof(R) == 4) return (long long)hi * (1ll << 24) + (long long)lo;
+    return (long long)((((unsigned long long)(unsigned)hi) << 32) + (unsigned long long)lo);
 }
 
 // Per-axis weights of a cell whose stencil nodes are all interior (shape
@@ -795,7 +812,7 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
         __syncthreads();
         long long *dst = staging + (long long)w * NCH * B3;
         for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x)
-            dst[i] = (long long)acc_hi[i] * (1ll << 24) + (long long)acc_lo[i];
+            dst[i] = fx_value<R>(acc_lo[i], acc_hi[i]);
         __syncthreads();
     }
 }
@@ -2328,7 +2345,7 @@ void launch_dt_finalize(Ctx &c, bool reset) {
 
 void launch_scales_from(Ctx &c, const unsigned long long *bounds) {
     const int W = (c.P.uniform_order == 1) ? 2 : (c.P.dual ? 3 : 4);
-    k_scales<<<1, 32, 0, c.stream>>>(c.ctl, W * W * W, bounds);
+    k_scales<<<1, 32, 0, c.stream>>>(c.ctl, W * W * W, c.precision == EXG_PREC_FP64 ? kFxBits64 : kFxBits32, bounds);
     EXG_CUDA_OK(cudaGetLastError());
 }
 
@@ -2599,7 +2616,7 @@ __global__ void k_na_bounds(Params P, NaArgs a) {
 }
 
 // scale 2^e per channel so that (particles per cell) x (stencil cells) x
-// (largest term) x 2 < 2^61, the bound of the context path's k_scales
+// (largest term) x 2 < 2^61, the bound of the context path's FP64 k_scales
 __global__ void k_na_scale(NaArgs a, int stencil_cells) {
     const int c = threadIdx.x;
     if (c >= kNaCh) return;

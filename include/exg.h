@@ -253,17 +253,29 @@ int exg_update_mp_positions(exg_ctx *ctx, double dt);
 int exg_update_mp_volume(exg_ctx *ctx);
 /* Calculate_MP_Stress_Strain (utilities.cpp:372-400 -> mpm_particle_container.cpp:43-142). */
 int exg_calculate_mp_stress_strain(exg_ctx *ctx, double time, double dt);
-/* Thermal counterparts (main.cpp:99-106, 129-135). */
+/* Thermal counterparts (main.cpp:99-106, 129-136); need specs.use_temp
+ * (EXG_ERR_NOT_READY otherwise). */
+/* P2G_Temperature (utilities.cpp:153-164 -> mpm_particle_grid_ops.cpp:656-884);
+ * reset must be 1 (the only value the reference passes). */
 int exg_p2g_temperature(exg_ctx *ctx, int reset, int update_temp, int update_source);
+/* backup_current_temperature (nodal_data_ops.cpp:95-114). */
 int exg_backup_current_temperature(exg_ctx *ctx);
+/* Nodal_Time_Update_Temperature (nodal_data_ops.cpp:500-527). */
 int exg_nodal_time_update_temperature(exg_ctx *ctx, double dt);
+/* Apply_Nodal_BCs_Temperature (utilities.cpp:221-240): wall BCs, UDF wall
+ * tables at `time`, level-set bodies (isothermal ones only when
+ * dirichlet_only). */
 int exg_apply_nodal_bcs_temperature(exg_ctx *ctx, double dt, double time, int dirichlet_only);
+/* store_delta_temperature (nodal_data_ops.cpp:409-430). */
 int exg_store_delta_temperature(exg_ctx *ctx);
+/* G2P_Temperature (utilities.cpp:288-298 -> mpm_particle_grid_ops.cpp:1129-1270). */
 int exg_g2p_temperature(exg_ctx *ctx, int update_temperature, int update_heatflux);
 
 /* One or more complete explicit steps of main.cpp:83-171 (without output),
- * fused into four kernels per step and replayed from a CUDA graph when the
- * step has no host-side dependency.  dt and time stay on the device. */
+ * USL or MUSL, with temperature when specs.use_temp: a fixed launch sequence
+ * (sort, P2G, nodal update + BCs, fused G2P/advection/stress) replayed from a
+ * CUDA graph when the step has no host-side dependency (UDF wall tables are
+ * re-tabulated on the host each step).  dt and time stay on the device. */
 int exg_step(exg_ctx *ctx, int nsteps);
 int exg_get_time(exg_ctx *ctx, double *time, double *last_dt, int64_t *steps);
 int exg_set_time(exg_ctx *ctx, double time, int64_t steps);

@@ -222,9 +222,15 @@ def test_fused_twisted_column_heat():
     s, p, phi = scenes.twisted_column(n=(16, 16, 48), precision=nt.PREC_FP64, n_obstacles=6, heat=True)
     ctx, o = run_both(s, p, 20, phi)
     g, r = ctx.download(), o.download()
-    check_particles(g, r, fields=[("vel", nt.R_VEL, 3), ("stress", nt.R_STRESS, 6), ("heatflux", nt.R_HEATFLUX, 3)])
-    e = np.abs(g.rdata[nt.R_TEMPERATURE] - r.rdata[nt.R_TEMPERATURE]).max()
-    assert e < TOL64 * 300.0, f"temperature: max abs err {e:.3e}"
+    check_particles(g, r, fields=[("vel", nt.R_VEL, 3), ("stress", nt.R_STRESS, 6)])
+    T = r.rdata[nt.R_TEMPERATURE]
+    e = np.abs(g.rdata[nt.R_TEMPERATURE] - T).max()
+    assert e < TOL64 * np.abs(T).max(), f"temperature: max abs err {e:.3e}"
+    # q = -k sum_I T_I grad N_I cancels temperatures of ~300 K down to
+    # their 1e-2 K spread: the tolerance carries that conditioning factor
+    cond = np.abs(T).max() / (T.max() - T.min())
+    q0, q1 = g.rdata[nt.R_HEATFLUX:nt.R_HEATFLUX + 3], r.rdata[nt.R_HEATFLUX:nt.R_HEATFLUX + 3]
+    assert rel(q0, q1) < TOL64 * cond, f"heatflux: {rel(q0, q1):.3e} (conditioning {cond:.1f})"
 
 
 def test_fused_deterministic():
