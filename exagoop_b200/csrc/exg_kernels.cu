@@ -658,6 +658,88 @@ __device__ __forceinline__ void p2g_axis_weights(const SplineTables &tab, const 
         cell_axis_weights<R, ORD>(tab, P, d, x, i, interior, a);
 }
 
+// Per-particle P2G coefficients: m, m v, the body force m g (+ the external
+// force inside the slab) and -V sigma, so that every node contribution is a
+// chain of fused multiply-adds; thermal: m cp, m cp T, m k, V q, V Q.
+template <class R, bool THERM>
+struct P2GCoef {
+    R m, mv[3], b[3], s[6];
+    R mcp, mcpT, mk, qv[3], VQ;
+};
+
+// Register accumulators of one stencil node.  FP32 keeps channel pairs in
+// float2 and adds them with the packed FP32 FMA of sm_100 (two lanes per
+// instruction): (m, p_x), (p_y, p_z), (f_x, f_y), then f_z alone.
+template <class R, bool THERM>
+struct P2GAcc {
+    R c[THERM ? CH_ALL : CH_MOM_END];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < (THERM ? CH_ALL : CH_MOM_END); ++i) c[i] = R(0);
+    }
+    __device__ __forceinline__ void add(const P2GCoef<R, THERM> &q, R N, R g0, R g1, R g2) {
+        c[CH_M] = fma(q.m, N, c[CH_M]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) c[CH_P + d] = fma(q.mv[d], N, c[CH_P + d]);
+        c[CH_F + 0] = fma(q.s[2], g2, fma(q.s[1], g1, fma(q.s[0], g0, fma(q.b[0], N, c[CH_F + 0]))));
+        c[CH_F + 1] = fma(q.s[4], g2, fma(q.s[3], g1, fma(q.s[1], g0, fma(q.b[1], N, c[CH_F + 1]))));
+        c[CH_F + 2] = fma(q.s[5], g2, fma(q.s[4], g1, fma(q.s[2], g0, fma(q.b[2], N, c[CH_F + 2]))));
+        if (THERM) add_thermal(q, N, g0, g1, g2);
+    }
+    __device__ __forceinline__ void add_thermal(const P2GCoef<R, THERM> &q, R N, R g0, R g1, R g2) {
+        if constexpr (THERM) {
+            c[CH_MC] = fma(q.mcp, N, c[CH_MC]);
+            c[CH_MCT] = fma(q.mcpT, N, c[CH_MCT]);
+            c[CH_MK] = fma(q.mk, N, c[CH_MK]);
+            c[CH_SRC] = fma(q.VQ, N, fma(q.qv[2], g2, fma(q.qv[1], g1, fma(q.qv[0], g0, c[CH_SRC]))));
+        }
+    }
+    __device__ __forceinline__ R get(int ch) const { return c[ch]; }
+};
+
+template <bool THERM>
+struct P2GAcc<float, THERM> {
+    float2 mp0, p12, f01;
+    float f2;
+    float th[4];  // m cp, m cp T, m k, source
+    __device__ __forceinline__ void zero() {
+        mp0 = p12 = f01 = make_float2(0.f, 0.f);
+        f2 = 0.f;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) th[i] = 0.f;
+    }
+    // N, g0, g1, g2 arrive as broadcast pairs (both lanes equal)
+    __device__ __forceinline__ void add2(const float2 cm, const float2 cp, const float2 cb, const float2 cs0,
+                                         const float2 cs1, const float2 cs2, const P2GCoef<float, THERM> &q,
+                                         float2 NN, float2 G0, float2 G1, float2 G2) {
+        mp0 = __ffma2_rn(cm, NN, mp0);
+        p12 = __ffma2_rn(cp, NN, p12);
+        f01 = __ffma2_rn(cb, NN, f01);
+        f01 = __ffma2_rn(cs0, G0, f01);
+        f01 = __ffma2_rn(cs1, G1, f01);
+        f01 = __ffma2_rn(cs2, G2, f01);
+        f2 = fmaf(q.s[5], G2.x, fmaf(q.s[4], G1.x, fmaf(q.s[2], G0.x, fmaf(q.b[2], NN.x, f2))));
+        if constexpr (THERM) {
+            th[0] = fmaf(q.mcp, NN.x, th[0]);
+            th[1] = fmaf(q.mcpT, NN.x, th[1]);
+            th[2] = fmaf(q.mk, NN.x, th[2]);
+            th[3] = fmaf(q.VQ, NN.x, fmaf(q.qv[2], G2.x, fmaf(q.qv[1], G1.x, fmaf(q.qv[0], G0.x, th[3]))));
+        }
+    }
+    __device__ __forceinline__ float get(int ch) const {
+        switch (ch) {
+            case CH_M: return mp0.x;
+            case CH_P: return mp0.y;
+            case CH_P + 1: return p12.x;
+            case CH_P + 2: return p12.y;
+            case CH_F: return f01.x;
+            case CH_F + 1: return f01.y;
+            case CH_F + 2: return f2;
+            default: return th[ch - CH_MC];
+        }
+    }
+};
+
 constexpr int kCellThreads = 128;
 
 // Threads per block and register cap of the per-cell P2G: the 3-wide
@@ -688,8 +770,7 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
     R sc[NCH];
 #pragma unroll
     for (int c = 0; c < NCH; ++c) sc[c] = (R)ctl->scale[c];
-    const bool fm = flags & PF_MASS, fv = flags & PF_VEL, ff = flags & PF_FORCE, fT = flags & PF_TEMP,
-               fS = flags & PF_SRC;
+    (void)flags;
     R grav[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) grav[d] = (R)P.gravity[d];
@@ -723,13 +804,11 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
             for (int sz = 0; sz < W; ++sz) {
 #pragma unroll
                 for (int sy0 = 0; sy0 < W; sy0 += ROWS) {
-                    R acc[ROWS][W][NCH];
+                    P2GAcc<R, THERM> acc[ROWS][W];
 #pragma unroll
                     for (int r = 0; r < ROWS; ++r)
 #pragma unroll
-                        for (int sx = 0; sx < W; ++sx)
-#pragma unroll
-                            for (int ch = 0; ch < NCH; ++ch) acc[r][sx][ch] = R(0);
+                        for (int sx = 0; sx < W; ++sx) acc[r][sx].zero();
                     bool any = false;
                     for (int k = ka; k < kb; ++k) {
                         const int p = perm[s0 + k];
@@ -743,56 +822,58 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
                         AxisW<R, W> ax, ay;
                         p2g_axis_weights<R, ORD>(*tab, P, 0, dual_x(P, 0, x[0]), iv[0], inter[0], ax);
                         p2g_axis_weights<R, ORD>(*tab, P, 1, dual_x(P, 1, x[1]), iv[1], inter[1], ay);
-                        const R m = A.mass[p], vol = A.vol[p];
-                        R mv[3], bf[3], s[6];
+                        // every channel is deposited; the nodal kernel keeps
+                        // the ones the call asked for
+                        P2GCoef<R, THERM> q;
+                        q.m = A.mass[p];
+                        const R vol = A.vol[p];
                         const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
                                           x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] &&
                                           x[2] < P.slab_hi[2];
 #pragma unroll
                         for (int d = 0; d < 3; ++d) {
-                            mv[d] = m * A.v[d][p];
-                            bf[d] = m * grav[d];
+                            q.mv[d] = q.m * A.v[d][p];
+                            q.b[d] = q.m * grav[d] + (slab ? (R)P.extforce[d] : R(0));
                         }
 #pragma unroll
-                        for (int c6 = 0; c6 < 6; ++c6) s[c6] = -vol * A.sig[c6][p];
-                        R ext[3];
+                        for (int c6 = 0; c6 < 6; ++c6) q.s[c6] = -vol * A.sig[c6][p];
+                        if constexpr (THERM) {
+                            q.mcp = q.m * A.cp[p];
+                            q.mcpT = (R)(q.mcp * A.T[p]);
+                            q.mk = q.m * A.kc[p];
 #pragma unroll
-                        for (int d = 0; d < 3; ++d) ext[d] = slab ? (R)P.extforce[d] : R(0);
-                        R mcp = R(0), mcpT = R(0), mk = R(0), qv[3] = {R(0), R(0), R(0)}, VQ = R(0);
-                        if (THERM) {
-                            mcp = m * A.cp[p];
-                            mcpT = (R)(mcp * A.T[p]);
-                            mk = m * A.kc[p];
-#pragma unroll
-                            for (int d = 0; d < 3; ++d) qv[d] = vol * A.q[d][p];
-                            VQ = vol * A.Q[p];
+                            for (int d = 0; d < 3; ++d) q.qv[d] = vol * A.q[d][p];
+                            q.VQ = vol * A.Q[p];
                         }
+                        if constexpr (sizeof(R) == 4) {
+                            const float2 cm = make_float2(q.m, q.mv[0]), cp = make_float2(q.mv[1], q.mv[2]);
+                            const float2 cb = make_float2(q.b[0], q.b[1]);
+                            const float2 cs0 = make_float2(q.s[0], q.s[1]), cs1 = make_float2(q.s[1], q.s[3]),
+                                         cs2 = make_float2(q.s[2], q.s[4]);
+                            const float2 wzz = make_float2(wz, wz), dzz = make_float2(dzw, dzw);
 #pragma unroll
-                        for (int r = 0; r < ROWS; ++r) {
-                            const R wy = ay.w[sy0 + r], dyw = ay.dw[sy0 + r];
-                            const R wyz = wy * wz;
+                            for (int r = 0; r < ROWS; ++r) {
+                                const float2 wyy = make_float2(ay.w[sy0 + r], ay.w[sy0 + r]);
+                                const float2 dyy = make_float2(ay.dw[sy0 + r], ay.dw[sy0 + r]);
+                                const float2 wyz = __fmul2_rn(wyy, wzz), dyz = __fmul2_rn(dyy, wzz),
+                                             wdz = __fmul2_rn(wyy, dzz);
 #pragma unroll
-                            for (int sx = 0; sx < W; ++sx) {
-                                const R N = ax.w[sx] * wyz;
-                                R *a = acc[r][sx];
-                                if (fm) a[CH_M] += m * N;
-                                if (fv) {
-#pragma unroll
-                                    for (int d = 0; d < 3; ++d) a[CH_P + d] += mv[d] * N;
+                                for (int sx = 0; sx < W; ++sx) {
+                                    const float2 wxx = make_float2(ax.w[sx], ax.w[sx]);
+                                    const float2 dxx = make_float2(ax.dw[sx], ax.dw[sx]);
+                                    acc[r][sx].add2(cm, cp, cb, cs0, cs1, cs2, q, __fmul2_rn(wxx, wyz),
+                                                    __fmul2_rn(dxx, wyz), __fmul2_rn(wxx, dyz), __fmul2_rn(wxx, wdz));
                                 }
-                                if (ff || (THERM && fS)) {
-                                    const R g0 = ax.dw[sx] * wyz, g1 = ax.w[sx] * dyw * wz, g2 = ax.w[sx] * wy * dzw;
-                                    if (ff) {
-                                        a[CH_F + 0] += (bf[0] * N + ext[0] * N) + (s[0] * g0 + s[1] * g1 + s[2] * g2);
-                                        a[CH_F + 1] += (bf[1] * N + ext[1] * N) + (s[1] * g0 + s[3] * g1 + s[4] * g2);
-                                        a[CH_F + 2] += (bf[2] * N + ext[2] * N) + (s[2] * g0 + s[4] * g1 + s[5] * g2);
-                                    }
-                                    if (THERM && fS) a[CH_SRC] += (qv[0] * g0 + qv[1] * g1 + qv[2] * g2) + VQ * N;
-                                }
-                                if (THERM && fT) {
-                                    a[CH_MC] += mcp * N;
-                                    a[CH_MCT] += mcpT * N;
-                                    a[CH_MK] += mk * N;
+                            }
+                        } else {
+#pragma unroll
+                            for (int r = 0; r < ROWS; ++r) {
+                                const R wy = ay.w[sy0 + r], dyw = ay.dw[sy0 + r];
+                                const R wyz = wy * wz, dyz = dyw * wz, wdz = wy * dzw;
+#pragma unroll
+                                for (int sx = 0; sx < W; ++sx) {
+                                    const R wx = ax.w[sx];
+                                    acc[r][sx].add(q, wx * wyz, ax.dw[sx] * wyz, wx * dyz, wx * wdz);
                                 }
                             }
                         }
@@ -804,7 +885,8 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
                         for (int sx = 0; sx < W; ++sx) {
                             const int idx = ((lz + sz) * B + (ly + sy0 + r)) * B + (lx + sx);
 #pragma unroll
-                            for (int ch = 0; ch < NCH; ++ch) fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, acc[r][sx][ch], sc[ch]);
+                            for (int ch = 0; ch < NCH; ++ch)
+                                fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, acc[r][sx].get(ch), sc[ch]);
                         }
                 }
             }
@@ -1129,11 +1211,14 @@ __global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeB
 // dense global arrays.
 template <class R>
 struct SmemNodes {
-    const R *nb;  // [6][B3]: v(3), dv(3)
+    // [B3][NS]: per node v(3), dv(3) contiguous (FP32 padded to 8 words), so
+    // one node is two 16-byte loads (FP32) or three (FP64)
+    static constexpr int NS = (sizeof(R) == 4) ? 8 : 6;
+    const R *nb;
     int B, B3;
     int org[3];   // node coordinate of block element 0
     __device__ __forceinline__ R get(int c, int i, int j, int k) const {
-        return nb[c * B3 + ((k - org[2]) * B + (j - org[1])) * B + (i - org[0])];
+        return nb[(((k - org[2]) * B + (j - org[1])) * B + (i - org[0])) * NS + c];
     }
 };
 template <class R>
@@ -1289,44 +1374,100 @@ __device__ __forceinline__ void g2p_particle_generic(const SplineTables &tab, co
     g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt);
 }
 
-// Interpolation over a WN^3 window of the shared-memory node block.
+// Interpolation over a WN^3 window of the shared-memory node block.  FP32
+// accumulates channel pairs with the packed FP32 FMA of sm_100:
+// (vpic_x, vpic_y), (vpic_z, dpic_x), (dpic_y, dpic_z) and the first two
+// rows of grad v per column, (gv[0][c], gv[1][c]).
 template <class R, int WN>
 __device__ __forceinline__ void g2p_window(const SmemNodes<R> &na, const int base[3], const R wx[WN], const R dwx[WN],
                                            const R wy[WN], const R dwy[WN], const R wz[WN], const R dwz[WN],
                                            bool upd_vel, bool upd_sr, R vpic[3], R dpic[3], R gv[3][3]) {
-    const int B = na.B, B3 = na.B3;
+    constexpr int NS = SmemNodes<R>::NS;
+    const int B = na.B;
     const int i0 = ((base[2] - na.org[2]) * B + (base[1] - na.org[1])) * B + (base[0] - na.org[0]);
     const R *nb = na.nb;
+    if constexpr (sizeof(R) == 4) {
+        float2 a01 = make_float2(0.f, 0.f), a2d = a01, d12 = a01;
+        float2 gc[3] = {a01, a01, a01};
+        float g2r[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-    for (int sz = 0; sz < WN; ++sz) {
+        for (int sz = 0; sz < WN; ++sz) {
+            const float2 wzz = make_float2(wz[sz], wz[sz]), dzz = make_float2(dwz[sz], dwz[sz]);
 #pragma unroll
-        for (int sy = 0; sy < WN; ++sy) {
-            const R wyz = wy[sy] * wz[sz], dyz = dwy[sy] * wz[sz], wdz = wy[sy] * dwz[sz];
-            const int row = i0 + (sz * B + sy) * B;
+            for (int sy = 0; sy < WN; ++sy) {
+                const float2 wyy = make_float2(wy[sy], wy[sy]), dyy = make_float2(dwy[sy], dwy[sy]);
+                const float2 wyz = __fmul2_rn(wyy, wzz), dyz = __fmul2_rn(dyy, wzz), wdz = __fmul2_rn(wyy, dzz);
+                const int row = i0 + (sz * B + sy) * B;
 #pragma unroll
-            for (int sx = 0; sx < WN; ++sx) {
-                const int idx = row + sx;
-                const R v0 = nb[idx], v1 = nb[B3 + idx], v2 = nb[2 * B3 + idx];
-                if (upd_vel) {
-                    const R N = wx[sx] * wyz;
-                    vpic[0] += N * v0;
-                    vpic[1] += N * v1;
-                    vpic[2] += N * v2;
-                    dpic[0] += N * nb[3 * B3 + idx];
-                    dpic[1] += N * nb[4 * B3 + idx];
-                    dpic[2] += N * nb[5 * B3 + idx];
+                for (int sx = 0; sx < WN; ++sx) {
+                    const float *q = nb + (row + sx) * NS;
+                    const float4 va = *reinterpret_cast<const float4 *>(q);
+                    const float2 v01 = make_float2(va.x, va.y);
+                    const float2 wxx = make_float2(wx[sx], wx[sx]);
+                    if (upd_vel) {
+                        const float2 vb = *reinterpret_cast<const float2 *>(q + 4);
+                        const float2 NN = __fmul2_rn(wxx, wyz);
+                        a01 = __ffma2_rn(v01, NN, a01);
+                        a2d = __ffma2_rn(make_float2(va.z, va.w), NN, a2d);
+                        d12 = __ffma2_rn(vb, NN, d12);
+                    }
+                    if (upd_sr) {
+                        const float2 dxx = make_float2(dwx[sx], dwx[sx]);
+                        const float2 G0 = __fmul2_rn(dxx, wyz), G1 = __fmul2_rn(wxx, dyz), G2 = __fmul2_rn(wxx, wdz);
+                        gc[0] = __ffma2_rn(v01, G0, gc[0]);
+                        gc[1] = __ffma2_rn(v01, G1, gc[1]);
+                        gc[2] = __ffma2_rn(v01, G2, gc[2]);
+                        g2r[0] = fmaf(va.z, G0.x, g2r[0]);
+                        g2r[1] = fmaf(va.z, G1.x, g2r[1]);
+                        g2r[2] = fmaf(va.z, G2.x, g2r[2]);
+                    }
                 }
-                if (upd_sr) {
-                    const R g0 = dwx[sx] * wyz, g1 = wx[sx] * dyz, g2 = wx[sx] * wdz;
-                    gv[0][0] += v0 * g0;
-                    gv[0][1] += v0 * g1;
-                    gv[0][2] += v0 * g2;
-                    gv[1][0] += v1 * g0;
-                    gv[1][1] += v1 * g1;
-                    gv[1][2] += v1 * g2;
-                    gv[2][0] += v2 * g0;
-                    gv[2][1] += v2 * g1;
-                    gv[2][2] += v2 * g2;
+            }
+        }
+        vpic[0] += a01.x;
+        vpic[1] += a01.y;
+        vpic[2] += a2d.x;
+        dpic[0] += a2d.y;
+        dpic[1] += d12.x;
+        dpic[2] += d12.y;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            gv[0][c] += gc[c].x;
+            gv[1][c] += gc[c].y;
+            gv[2][c] += g2r[c];
+        }
+    } else {
+#pragma unroll
+        for (int sz = 0; sz < WN; ++sz) {
+#pragma unroll
+            for (int sy = 0; sy < WN; ++sy) {
+                const R wyz = wy[sy] * wz[sz], dyz = dwy[sy] * wz[sz], wdz = wy[sy] * dwz[sz];
+                const int row = i0 + (sz * B + sy) * B;
+#pragma unroll
+                for (int sx = 0; sx < WN; ++sx) {
+                    const R *q = nb + (row + sx) * NS;
+                    const R v0 = q[0], v1 = q[1], v2 = q[2];
+                    if (upd_vel) {
+                        const R N = wx[sx] * wyz;
+                        vpic[0] = fma(N, v0, vpic[0]);
+                        vpic[1] = fma(N, v1, vpic[1]);
+                        vpic[2] = fma(N, v2, vpic[2]);
+                        dpic[0] = fma(N, q[3], dpic[0]);
+                        dpic[1] = fma(N, q[4], dpic[1]);
+                        dpic[2] = fma(N, q[5], dpic[2]);
+                    }
+                    if (upd_sr) {
+                        const R g0 = dwx[sx] * wyz, g1 = wx[sx] * dyz, g2 = wx[sx] * wdz;
+                        gv[0][0] = fma(v0, g0, gv[0][0]);
+                        gv[0][1] = fma(v0, g1, gv[0][1]);
+                        gv[0][2] = fma(v0, g2, gv[0][2]);
+                        gv[1][0] = fma(v1, g0, gv[1][0]);
+                        gv[1][1] = fma(v1, g1, gv[1][1]);
+                        gv[1][2] = fma(v1, g2, gv[1][2]);
+                        gv[2][0] = fma(v2, g0, gv[2][0]);
+                        gv[2][1] = fma(v2, g1, gv[2][1]);
+                        gv[2][2] = fma(v2, g2, gv[2][2]);
+                    }
                 }
             }
         }
@@ -1542,9 +1683,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_g2p_fused(Params P, Parts<R> A,
     for (int idx = threadIdx.x; idx < B3; idx += blockDim.x) {
         const int bx = idx % B, by = (idx / B) % B, bz = idx / (B * B);
         const long long ni = node_index(P, na.org[0] + bx, na.org[1] + by, na.org[2] + bz);
+        R *q = nb + idx * SmemNodes<R>::NS;
         for (int c = 0; c < 3; ++c) {
-            nb[c * B3 + idx] = ni >= 0 ? Nd.c[EXG_N_VEL + c][ni] : R(0);
-            nb[(3 + c) * B3 + idx] = ni >= 0 ? Nd.c[EXG_N_DVEL + c][ni] : R(0);
+            q[c] = ni >= 0 ? Nd.c[EXG_N_VEL + c][ni] : R(0);
+            q[3 + c] = ni >= 0 ? Nd.c[EXG_N_DVEL + c][ni] : R(0);
         }
     }
     __syncthreads();
@@ -2432,7 +2574,7 @@ void EXG_SFX(launch_nodes)(Ctx &c, int mode, int flags, bool all_tiles) {
 template <class R, int ORD>
 static void g2p_t(Ctx &c, int mode) {
     const int B3 = c.P.B * c.P.B * c.P.B;
-    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(R) * 6 * B3;
+    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(R) * SmemNodes<R>::NS * B3;
     auto kern = k_g2p_fused<R, ORD>;
     EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     static int grid = 0;
