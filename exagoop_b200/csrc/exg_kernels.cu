@@ -426,7 +426,7 @@ __device__ __forceinline__ void particle_bounds(const Params &P, const Material 
 
 __device__ __forceinline__ void block_reduce_push(unsigned long long *bounds, unsigned long long *dtmin,
                                                   double b[CH_ALL], double dtp, bool valid) {
-    __shared__ unsigned long long red[CH_ALL + 1][kThreads / 32];
+    __shared__ unsigned long long red[CH_ALL + 1][32];  // any block of up to 1024 threads
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int c = 0; c < CH_ALL; ++c) {
         unsigned long long u = valid ? dbits(b[c]) : 0ull;
@@ -741,16 +741,34 @@ struct P2GAcc<float, THERM> {
 };
 
 constexpr int kCellThreads = 128;
+// launch shapes of the quadratic P2G and of the fused G2P (threads per
+// block, minimum resident blocks per SM for the register cap); the fused
+// G2P measured fastest at 2 x 256 (128 registers) against 1 x 256, 4 x 128,
+// 3 x 128, 3 x 256, 2 x 384 and 1 x 512
+#ifndef EXG_P2G2_THREADS
+#define EXG_P2G2_THREADS 512
+#endif
+#ifndef EXG_P2G2_MINB
+#define EXG_P2G2_MINB 1
+#endif
+#ifndef EXG_G2P_THREADS
+#define EXG_G2P_THREADS 256
+#endif
+#ifndef EXG_G2P_MINB
+#define EXG_G2P_MINB 2
+#endif
 
 // Threads per block and register cap of the per-cell P2G: the 3-wide
-// quadratic accumulators fit 128 registers at 256 threads.
+// quadratic accumulators fit 128 registers; one 512-thread block per SM (a
+// thread per bin of an 8^3 tile) measured fastest on the dam break, ahead
+// of 2 x 256, 4 x 128 and 1 x 256 with 255 registers.
 template <class R, int ORD, bool THERM>
 struct P2GCfg {
     static constexpr int W = P2GStc<ORD>::W;
     // y rows of the stencil slice accumulated per pass (register budget)
     static constexpr int ROWS = (sizeof(R) == 8) ? 1 : (THERM ? (W == 4 ? 2 : 1) : W);
-    static constexpr int THREADS = (ORD == 2) ? 256 : kCellThreads;
-    static constexpr int MINB = (ORD == 2) ? 2 : 1;
+    static constexpr int THREADS = (ORD == 2) ? EXG_P2G2_THREADS : kCellThreads;
+    static constexpr int MINB = (ORD == 2) ? EXG_P2G2_MINB : 1;
 };
 
 template <class R, int ORD, bool THERM>
@@ -1645,7 +1663,7 @@ __device__ __forceinline__ bool all_finite(const R *a, int n) {
 // particle arrays are physically re-ordered by cell every step at no extra
 // pass.  GM_VEL updates velocity in place in A instead.
 template <class R, int ORD>
-__global__ void __launch_bounds__(kThreads, 2) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
+__global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
                                                         const Material *mats, const int *active, const int *start,
                                                         const int *count, const int32_t *perm, Ctl *ctl, int mode) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -2429,11 +2447,11 @@ static int nblocks(long long n, int t = kThreads) { return (int)((n + t - 1) / t
 
 // Grid of a persistent kernel: every SM filled to its occupancy limit.
 template <class K>
-static int persistent_grid(K kern, size_t smem) {
+static int persistent_grid(K kern, size_t smem, int threads = kThreads) {
     int dev = 0, nsm = 0, per = 0;
     EXG_CUDA_OK(cudaGetDevice(&dev));
     EXG_CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    EXG_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kThreads, smem));
+    EXG_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem));
     if (per < 1) per = 1;
     return nsm * per;
 }
@@ -2580,10 +2598,10 @@ static void g2p_t(Ctx &c, int mode) {
     static int grid = 0;
     static size_t gsm = 0;
     if (!grid || gsm != sm) {
-        grid = persistent_grid(kern, sm);
+        grid = persistent_grid(kern, sm, EXG_G2P_THREADS);
         gsm = sm;
     }
-    kern<<<grid, kThreads, sm, c.stream>>>(c.P, c.A<R>(), c.Bp<R>(), c.N<R>(), make_bc(c), c.mat_dev, c.sb.active,
+    kern<<<grid, EXG_G2P_THREADS, sm, c.stream>>>(c.P, c.A<R>(), c.Bp<R>(), c.N<R>(), make_bc(c), c.mat_dev, c.sb.active,
                                            c.sb.tile_start, c.sb.tile_count, c.sb.perm, c.ctl, mode);
     EXG_CUDA_OK(cudaGetLastError());
 }
