@@ -237,6 +237,60 @@ def run_ours(args, rank, world):
     return line, p
 
 
+def run_batch(args, rank, world):
+    """The batched uneven scenes: 64 independent dam breaks (grid sides from
+    {32,48,64,96,128}, fill fractions in [0.1,0.4], seeded) advanced by
+    exg_batch_step, one launch per hot kernel over all scenes."""
+    import torch
+    from exagoop_b200 import native as nt, scenes
+
+    torch.cuda.set_device(rank % torch.cuda.device_count())
+    dev = torch.cuda.current_device()
+    prec = nt.PREC_MIXED if args.precision == "mixed" else nt.PREC_FP64
+    seed = 2024 + rank
+    specs = scenes.batched_specs(seed=seed, precision=prec)
+    b = nt.Batch(specs, device=dev)
+    total = 0
+    for sc, (s, p) in zip(b.scenes, scenes.batched_dam_breaks(seed=seed, precision=prec)):
+        sc.upload(p)
+        sc.Initialise_Internal_Forces()
+        total += p.n
+        del p
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        ms = time_steps(b, args.steps, args.warmup)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tot = torch.tensor([float(total)], device="cuda")
+        torch.distributed.all_reduce(tot)
+        total_all = int(tot.item())
+    else:
+        total_all = total
+    ms = float(t.item())
+    value = total_all * args.steps / (ms * 1e-3)
+    sides = [int(s.ncells[0]) for s in specs]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if prec == nt.PREC_MIXED else "f64",
+        "data": "synthetic (seeded lattices, jittered)",
+        "config": {"workload": f"batched_dam_breaks_{len(specs)}_scenes", "particles": total_all,
+                   "particles_per_gpu": total, "grid_sides": sides, "order": 2, "precision": args.precision,
+                   "tile": 8, "l2": "inputs larger than L2",
+                   "parallelism": f"replicas{world}" if world > 1 else "single"},
+        "clocks": clk.summary(),
+        "e2e": None,
+        "gpu_launches": args.steps * (len(specs) * 8 + 4),
+        "roofline": None,
+        "cpu_baseline": None,
+    }
+    b.close()
+    return line
+
+
 def ctx_tile(s):
     return int(s.tile) if s.tile else 8
 
@@ -272,7 +326,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="dam_break", choices=["dam_break", "spheres", "axial_bar"])
+    ap.add_argument("--config", default="dam_break", choices=["dam_break", "spheres", "axial_bar", "batch"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--scale", type=float, default=1.0, help="grid scale factor (1 = the benchmark size)")
@@ -305,6 +359,15 @@ def main():
         import torch
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.config == "batch":
+        line = run_batch(args, rank, world)
+        if rank == 0:
+            print(json.dumps(line))
+        if world > 1:
+            import torch
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
     line, p = run_ours(args, rank, world)
     if rank == 0:
         if not args.no_cpu:

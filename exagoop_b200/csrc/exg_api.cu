@@ -16,6 +16,11 @@ using namespace exg;
 struct exg_ctx {
     Ctx c;
 };
+struct exg_batch {
+    Batch b;
+    std::vector<exg_ctx *> ctxs;
+    std::string err;
+};
 
 namespace {
 
@@ -1173,6 +1178,185 @@ int exg_get_stream(exg_ctx *ctx, void **stream) {
     if (!ctx || !stream) return EXG_ERR_ARG;
     *stream = (void *)ctx->c.stream;
     return EXG_OK;
+}
+
+// ------------------------------------------------------------ batches
+namespace {
+int bfail(exg_batch *B, int code, const std::string &msg) {
+    if (B) B->err = msg;
+    return code;
+}
+std::string batch_compatible(const exg_specs *s, int n) {
+    for (int i = 0; i < n; ++i) {
+        const exg_specs &x = s[i];
+        if (x.use_temp) return "scene " + std::to_string(i) + ": batches run without temperature";
+        if (x.stress_update_scheme != 0) return "scene " + std::to_string(i) + ": batches run the USL scheme";
+        for (int d = 0; d < 3; ++d)
+            if (x.udf_wallvel_lo[d] || x.udf_wallvel_hi[d])
+                return "scene " + std::to_string(i) + ": UDF wall tables are not supported in batches";
+        if (x.precision != s[0].precision) return "scenes must share exg.precision";
+        if ((x.tile > 0 ? x.tile : 8) != (s[0].tile > 0 ? s[0].tile : 8)) return "scenes must share exg.tile";
+        for (int d = 0; d < 3; ++d)
+            if (x.order[d] != s[0].order[d]) return "scenes must share the B-spline order of every axis";
+    }
+    return "";
+}
+void enqueue_batch_step(exg_batch *B) {
+    Batch &b = B->b;
+    for (Ctx *cp : b.scenes) {
+        Ctx &c = *cp;
+        EXG_CUDA_OK(cudaMemcpyAsync(c.bounds_cur, &c.ctl->bound_bits[0], sizeof(unsigned long long) * CH_ALL,
+                                    cudaMemcpyDeviceToDevice, c.stream));
+        launch_dt_finalize(c, true);
+        launch_keys(c);
+        launch_sort_rest(c, true);
+        launch_scales_from(c, c.bounds_cur);
+    }
+    launch_batch_plan(b);
+    if (b.precision == EXG_PREC_FP64)
+        launch_batch_core_fp64(b);
+    else
+        launch_batch_core_fp32(b);
+    for (Ctx *cp : b.scenes) {
+        Ctx &c = *cp;
+        if (c.precision == EXG_PREC_FP64)
+            launch_copy_lost_fp64(c);
+        else
+            launch_copy_lost_fp32(c);
+        launch_time_advance(c);
+    }
+}
+void batch_flip(Batch &b) {
+    for (Ctx *c : b.scenes) swap_parts(*c);
+    b.parity ^= 1;
+}
+void batch_drop_graphs(Batch &b) {
+    for (int k = 0; k < 2; ++k) {
+        if (b.gexec[k]) cudaGraphExecDestroy(b.gexec[k]);
+        b.gexec[k] = nullptr;
+        b.warm[k] = false;
+    }
+}
+}  // namespace
+
+int exg_batch_create(const exg_specs *specs, int nscenes, int device, exg_batch **out) {
+    if (!specs || !out || nscenes < 1 || nscenes > kMaxScenes) return EXG_ERR_ARG;
+    *out = nullptr;
+    const std::string why = batch_compatible(specs, nscenes);
+    if (!why.empty()) {
+        fprintf(stderr, "exg_batch_create: %s\n", why.c_str());
+        return EXG_ERR_UNSUPPORTED;
+    }
+    exg_batch *B = new exg_batch();
+    Batch &b = B->b;
+    b.precision = specs[0].precision;
+    try {
+        EXG_CUDA_OK(cudaSetDevice(device));
+        EXG_CUDA_OK(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
+        for (int i = 0; i < nscenes; ++i) {
+            exg_ctx *ctx = nullptr;
+            const int rc = exg_ctx_create(&specs[i], device, &ctx);
+            if (rc) {
+                exg_batch_destroy(B);
+                return rc;
+            }
+            // every scene enqueues on the batch's stream
+            cudaStreamDestroy(ctx->c.stream);
+            ctx->c.stream = b.stream;
+            B->ctxs.push_back(ctx);
+            b.scenes.push_back(&ctx->c);
+        }
+        EXG_CUDA_OK(cudaMalloc(&b.bctl, sizeof(BatchCtl)));
+        EXG_CUDA_OK(cudaMemset(b.bctl, 0, sizeof(BatchCtl)));
+        EXG_CUDA_OK(cudaMemcpy(&b.bctl->nscenes, &nscenes, sizeof(int), cudaMemcpyHostToDevice));
+        std::vector<Ctl *> ctls(nscenes);
+        for (int i = 0; i < nscenes; ++i) ctls[i] = b.scenes[i]->ctl;
+        EXG_CUDA_OK(cudaMalloc(&b.ctls, sizeof(Ctl *) * nscenes));
+        EXG_CUDA_OK(cudaMemcpy(b.ctls, ctls.data(), sizeof(Ctl *) * nscenes, cudaMemcpyHostToDevice));
+    } catch (const std::exception &e) {
+        fprintf(stderr, "exg_batch_create: %s\n", e.what());
+        exg_batch_destroy(B);
+        return EXG_ERR_CUDA;
+    }
+    *out = B;
+    return EXG_OK;
+}
+
+int exg_batch_destroy(exg_batch *B) {
+    if (!B) return EXG_OK;
+    Batch &b = B->b;
+    if (b.stream) cudaStreamSynchronize(b.stream);
+    batch_drop_graphs(b);
+    for (exg_ctx *ctx : B->ctxs) {
+        ctx->c.stream = nullptr;  // the batch's stream
+        exg_ctx_destroy(ctx);
+    }
+    cudaFree(b.bctl);
+    cudaFree(b.ctls);
+    for (void *d : b.desc) cudaFree(d);
+    if (b.stream) cudaStreamDestroy(b.stream);
+    delete B;
+    return EXG_OK;
+}
+
+exg_ctx *exg_batch_scene(exg_batch *B, int i) {
+    if (!B || i < 0 || i >= (int)B->ctxs.size()) return nullptr;
+    return B->ctxs[i];
+}
+
+int exg_batch_num_scenes(const exg_batch *B) { return B ? (int)B->ctxs.size() : 0; }
+
+const char *exg_batch_last_error(const exg_batch *B) { return B ? B->err.c_str() : "null batch"; }
+
+int exg_batch_step(exg_batch *B, int nsteps) {
+    if (!B || nsteps < 0) return EXG_ERR_ARG;
+    Batch &b = B->b;
+    for (size_t i = 0; i < b.scenes.size(); ++i)
+        if (b.scenes[i]->np == 0) return bfail(B, EXG_ERR_NOT_READY, "scene " + std::to_string(i) + " has no particles");
+    try {
+        for (Ctx *c : b.scenes)
+            if (c->reduce_stale) do_reduce(*c);
+        const bool changed = b.precision == EXG_PREC_FP64 ? batch_descriptors_fp64(b) : batch_descriptors_fp32(b);
+        if (changed) batch_drop_graphs(b);
+        const bool use_graph = std::getenv("EXG_NO_GRAPH") == nullptr;
+        for (int s = 0; s < nsteps; ++s) {
+            cudaGraphExec_t &g = b.gexec[b.parity];
+            if (!use_graph || !b.warm[b.parity]) {
+                // the first step of each parity runs eagerly (kernel
+                // attributes, occupancy queries), later ones replay a graph
+                enqueue_batch_step(B);
+                b.warm[b.parity] = true;
+                batch_flip(b);
+                continue;
+            }
+            if (!g) {
+                cudaGraph_t graph = nullptr;
+                EXG_CUDA_OK(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
+                enqueue_batch_step(B);
+                EXG_CUDA_OK(cudaStreamEndCapture(b.stream, &graph));
+                EXG_CUDA_OK(cudaGraphInstantiate(&g, graph, 0));
+                cudaGraphDestroy(graph);
+            }
+            EXG_CUDA_OK(cudaGraphLaunch(g, b.stream));
+            batch_flip(b);
+        }
+        int rc = EXG_OK;
+        for (size_t i = 0; i < b.scenes.size(); ++i) {
+            Ctx &c = *b.scenes[i];
+            c.parts_sorted = false;
+            const int r = status_from_ctl(c);
+            c.host_time = c.ctl_host->time;
+            c.host_dt = c.ctl_host->dt;
+            c.host_steps = c.ctl_host->steps;
+            if (r && !rc) {
+                rc = r;
+                B->err = "scene " + std::to_string(i) + ": " + c.err;
+            }
+        }
+        return rc;
+    } catch (const std::exception &e) {
+        return bfail(B, EXG_ERR_CUDA, e.what());
+    }
 }
 
 }  // extern "C"

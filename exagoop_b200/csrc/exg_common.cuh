@@ -59,6 +59,18 @@ struct Ctl {
     int next_g2p;                      // dynamic tile counter of the fused G2P (reset by k_nodes)
 };
 
+// Control block of a batch of independent scenes advanced by one launch per
+// kernel: prefix sums of the scenes' tile counts and the batch's dynamic
+// tile counters (k_batch_plan fills them before each step's batched
+// kernels).
+constexpr int kMaxScenes = 1024;
+struct BatchCtl {
+    int nscenes;
+    int next_p2g, next_nodes, next_g2p;
+    int pre_active[kMaxScenes + 1];   // scene s owns items [pre[s], pre[s+1]) of the active-tile list
+    int pre_touched[kMaxScenes + 1];  // the same for the tiles the nodal kernel writes
+};
+
 struct Body {
     int mom_bc;
     double wall_mu;

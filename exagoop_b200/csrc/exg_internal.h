@@ -81,6 +81,30 @@ void launch_node_reset(Ctx &c);
 EXG_DECL_PREC(_fp64)
 EXG_DECL_PREC(_fp32)
 
+// A batch of independent scenes (batch.cu side of exg_batch): scene
+// contexts, a shared stream, the batch control block and the scene
+// descriptors for both particle-buffer parities.
+struct Batch {
+    std::vector<Ctx *> scenes;
+    cudaStream_t stream = nullptr;
+    int precision = 0;
+    BatchCtl *bctl = nullptr;            // device
+    Ctl **ctls = nullptr;                // device: each scene's control block
+    void *desc[2] = {nullptr, nullptr};  // device SceneDesc<R>[n], one array per parity
+    std::vector<unsigned char> desc_host[2];
+    size_t desc_bytes = 0;
+    int parity = 0;                      // flips every step
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    bool warm[2] = {false, false};
+};
+// Uploads the scene descriptors of both parities; true when they changed.
+bool batch_descriptors_fp64(Batch &b);
+bool batch_descriptors_fp32(Batch &b);
+// k_batch_plan + batched P2G, nodal and fused G2P kernels (USL step).
+void launch_batch_plan(Batch &b);
+void launch_batch_core_fp64(Batch &b);
+void launch_batch_core_fp32(Batch &b);
+
 struct Ctx {
     exg_specs specs;
     Params P;

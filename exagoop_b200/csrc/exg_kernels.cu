@@ -9,6 +9,7 @@
 // reductions on the device so that a whole step can be replayed from a CUDA
 // graph without a host round trip.
 #include <algorithm>
+#include <cstring>
 #include <cstdio>
 #include <cstdlib>
 #include <stdexcept>
@@ -771,24 +772,144 @@ struct P2GCfg {
     static constexpr int MINB = (ORD == 2) ? EXG_P2G2_MINB : 1;
 };
 
+// One tile of the per-cell P2G into its fixed-point node block (zeroed by
+// the caller) and from there to the tile's staging slot.
+template <class R, int ORD, bool THERM>
+__device__ __forceinline__ void p2g_tile(const SplineTables *tab, unsigned *acc_lo, int *acc_hi, const Params &P,
+                                         const Parts<R> &A, const int *active, const int *start, const int *cell_start,
+                                         const int32_t *perm, long long *staging, const R *sc, const R *grav, int w) {
+    constexpr int W = P2GCfg<R, ORD, THERM>::W;
+    constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
+    constexpr int ROWS = P2GCfg<R, ORD, THERM>::ROWS;
+    const int B = P.B, B3 = B * B * B, T = P.T, T3 = T * T * T;
+    const int t = active[w];
+    int tc[3];
+    tile_coords(P, t, tc);
+    const int s0 = start[t];
+    const int *cs = cell_start + (long long)w * (T3 + 1);
+    for (int c = threadIdx.x; c < T3; c += blockDim.x) {
+        const int ka = cs[c], kb = cs[c + 1];
+        if (ka == kb) continue;
+        const int lx = c % T, ly = (c / T) % T, lz = c / (T * T);
+        const int iv[3] = {tc[0] * T + lx, tc[1] * T + ly, tc[2] * T + lz};
+        bool inter[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            inter[d] = (ORD == 1) || P.periodic[d] ||
+                       (ORD == 2 ? (iv[d] >= 3 && iv[d] <= P.nc[d] - 3) : (iv[d] >= 3 && iv[d] <= P.nc[d] - 4));
+        for (int sz = 0; sz < W; ++sz) {
+#pragma unroll
+            for (int sy0 = 0; sy0 < W; sy0 += ROWS) {
+                P2GAcc<R, THERM> acc[ROWS][W];
+#pragma unroll
+                for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+                    for (int sx = 0; sx < W; ++sx) acc[r][sx].zero();
+                bool any = false;
+                for (int k = ka; k < kb; ++k) {
+                    const int p = perm[s0 + k];
+                    if (A.phase[p] != 0) continue;
+                    const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+                    AxisW<R, W> az;
+                    p2g_axis_weights<R, ORD>(*tab, P, 2, dual_x(P, 2, x[2]), iv[2], inter[2], az);
+                    const R wz = pick<W>(az.w, sz), dzw = pick<W>(az.dw, sz);
+                    if (wz == R(0) && dzw == R(0)) continue;
+                    any = true;
+                    AxisW<R, W> ax, ay;
+                    p2g_axis_weights<R, ORD>(*tab, P, 0, dual_x(P, 0, x[0]), iv[0], inter[0], ax);
+                    p2g_axis_weights<R, ORD>(*tab, P, 1, dual_x(P, 1, x[1]), iv[1], inter[1], ay);
+                    // every channel is deposited; the nodal kernel keeps
+                    // the ones the call asked for
+                    P2GCoef<R, THERM> q;
+                    q.m = A.mass[p];
+                    const R vol = A.vol[p];
+                    const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
+                                      x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] &&
+                                      x[2] < P.slab_hi[2];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        q.mv[d] = q.m * A.v[d][p];
+                        q.b[d] = q.m * grav[d] + (slab ? (R)P.extforce[d] : R(0));
+                    }
+#pragma unroll
+                    for (int c6 = 0; c6 < 6; ++c6) q.s[c6] = -vol * A.sig[c6][p];
+                    if constexpr (THERM) {
+                        q.mcp = q.m * A.cp[p];
+                        q.mcpT = (R)(q.mcp * A.T[p]);
+                        q.mk = q.m * A.kc[p];
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) q.qv[d] = vol * A.q[d][p];
+                        q.VQ = vol * A.Q[p];
+                    }
+                    if constexpr (sizeof(R) == 4) {
+                        const float2 cm = make_float2(q.m, q.mv[0]), cp = make_float2(q.mv[1], q.mv[2]);
+                        const float2 cb = make_float2(q.b[0], q.b[1]);
+                        const float2 cs0 = make_float2(q.s[0], q.s[1]), cs1 = make_float2(q.s[1], q.s[3]),
+                                     cs2 = make_float2(q.s[2], q.s[4]);
+                        const float2 wzz = make_float2(wz, wz), dzz = make_float2(dzw, dzw);
+#pragma unroll
+                        for (int r = 0; r < ROWS; ++r) {
+                            const float2 wyy = make_float2(ay.w[sy0 + r], ay.w[sy0 + r]);
+                            const float2 dyy = make_float2(ay.dw[sy0 + r], ay.dw[sy0 + r]);
+                            const float2 wyz = __fmul2_rn(wyy, wzz), dyz = __fmul2_rn(dyy, wzz),
+                                         wdz = __fmul2_rn(wyy, dzz);
+#pragma unroll
+                            for (int sx = 0; sx < W; ++sx) {
+                                const float2 wxx = make_float2(ax.w[sx], ax.w[sx]);
+                                const float2 dxx = make_float2(ax.dw[sx], ax.dw[sx]);
+                                acc[r][sx].add2(cm, cp, cb, cs0, cs1, cs2, q, __fmul2_rn(wxx, wyz),
+                                                __fmul2_rn(dxx, wyz), __fmul2_rn(wxx, dyz), __fmul2_rn(wxx, wdz));
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < ROWS; ++r) {
+                            const R wy = ay.w[sy0 + r], dyw = ay.dw[sy0 + r];
+                            const R wyz = wy * wz, dyz = dyw * wz, wdz = wy * dzw;
+#pragma unroll
+                            for (int sx = 0; sx < W; ++sx) {
+                                const R wx = ax.w[sx];
+                                acc[r][sx].add(q, wx * wyz, ax.dw[sx] * wyz, wx * dyz, wx * wdz);
+                            }
+                        }
+                    }
+                }
+                if (!any) continue;
+#pragma unroll
+                for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+                    for (int sx = 0; sx < W; ++sx) {
+                        const int idx = ((lz + sz) * B + (ly + sy0 + r)) * B + (lx + sx);
+#pragma unroll
+                        for (int ch = 0; ch < NCH; ++ch)
+                            fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, acc[r][sx].get(ch), sc[ch]);
+                    }
+            }
+        }
+    }
+    __syncthreads();
+    long long *dst = staging + (long long)w * NCH * B3;
+    for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x)
+        dst[i] = fx_value<R>(acc_lo[i], acc_hi[i]);
+    __syncthreads();
+}
+
 template <class R, int ORD, bool THERM>
 __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD, THERM>::MINB)
     k_p2g_cell(Params P, Parts<R> A, const int *active, const int *start, const int *cell_start, const int32_t *perm,
                long long *staging, Ctl *ctl, int flags) {
-    constexpr int W = P2GCfg<R, ORD, THERM>::W;
     constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
-    constexpr int ROWS = P2GCfg<R, ORD, THERM>::ROWS;
     __shared__ int s_item;
     extern __shared__ __align__(16) unsigned char smraw[];
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
-    const int B = P.B, B3 = B * B * B, T = P.T, T3 = T * T * T;
+    const int B3 = P.B * P.B * P.B;
     unsigned *acc_lo = reinterpret_cast<unsigned *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
     int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3);
     load_tables(tab);
     R sc[NCH];
 #pragma unroll
     for (int c = 0; c < NCH; ++c) sc[c] = (R)ctl->scale[c];
-    (void)flags;
+    (void)flags;  // every channel is deposited; the nodal kernel keeps the requested ones
     R grav[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) grav[d] = (R)P.gravity[d];
@@ -804,116 +925,7 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
         __syncthreads();
         const int w = s_item;
         if (w >= nitems) break;
-        const int t = active[w];
-        int tc[3];
-        tile_coords(P, t, tc);
-        const int s0 = start[t];
-        const int *cs = cell_start + (long long)w * (T3 + 1);
-        for (int c = threadIdx.x; c < T3; c += blockDim.x) {
-            const int ka = cs[c], kb = cs[c + 1];
-            if (ka == kb) continue;
-            const int lx = c % T, ly = (c / T) % T, lz = c / (T * T);
-            const int iv[3] = {tc[0] * T + lx, tc[1] * T + ly, tc[2] * T + lz};
-            bool inter[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d)
-                inter[d] = (ORD == 1) || P.periodic[d] ||
-                           (ORD == 2 ? (iv[d] >= 3 && iv[d] <= P.nc[d] - 3) : (iv[d] >= 3 && iv[d] <= P.nc[d] - 4));
-            for (int sz = 0; sz < W; ++sz) {
-#pragma unroll
-                for (int sy0 = 0; sy0 < W; sy0 += ROWS) {
-                    P2GAcc<R, THERM> acc[ROWS][W];
-#pragma unroll
-                    for (int r = 0; r < ROWS; ++r)
-#pragma unroll
-                        for (int sx = 0; sx < W; ++sx) acc[r][sx].zero();
-                    bool any = false;
-                    for (int k = ka; k < kb; ++k) {
-                        const int p = perm[s0 + k];
-                        if (A.phase[p] != 0) continue;
-                        const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
-                        AxisW<R, W> az;
-                        p2g_axis_weights<R, ORD>(*tab, P, 2, dual_x(P, 2, x[2]), iv[2], inter[2], az);
-                        const R wz = pick<W>(az.w, sz), dzw = pick<W>(az.dw, sz);
-                        if (wz == R(0) && dzw == R(0)) continue;
-                        any = true;
-                        AxisW<R, W> ax, ay;
-                        p2g_axis_weights<R, ORD>(*tab, P, 0, dual_x(P, 0, x[0]), iv[0], inter[0], ax);
-                        p2g_axis_weights<R, ORD>(*tab, P, 1, dual_x(P, 1, x[1]), iv[1], inter[1], ay);
-                        // every channel is deposited; the nodal kernel keeps
-                        // the ones the call asked for
-                        P2GCoef<R, THERM> q;
-                        q.m = A.mass[p];
-                        const R vol = A.vol[p];
-                        const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
-                                          x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] &&
-                                          x[2] < P.slab_hi[2];
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            q.mv[d] = q.m * A.v[d][p];
-                            q.b[d] = q.m * grav[d] + (slab ? (R)P.extforce[d] : R(0));
-                        }
-#pragma unroll
-                        for (int c6 = 0; c6 < 6; ++c6) q.s[c6] = -vol * A.sig[c6][p];
-                        if constexpr (THERM) {
-                            q.mcp = q.m * A.cp[p];
-                            q.mcpT = (R)(q.mcp * A.T[p]);
-                            q.mk = q.m * A.kc[p];
-#pragma unroll
-                            for (int d = 0; d < 3; ++d) q.qv[d] = vol * A.q[d][p];
-                            q.VQ = vol * A.Q[p];
-                        }
-                        if constexpr (sizeof(R) == 4) {
-                            const float2 cm = make_float2(q.m, q.mv[0]), cp = make_float2(q.mv[1], q.mv[2]);
-                            const float2 cb = make_float2(q.b[0], q.b[1]);
-                            const float2 cs0 = make_float2(q.s[0], q.s[1]), cs1 = make_float2(q.s[1], q.s[3]),
-                                         cs2 = make_float2(q.s[2], q.s[4]);
-                            const float2 wzz = make_float2(wz, wz), dzz = make_float2(dzw, dzw);
-#pragma unroll
-                            for (int r = 0; r < ROWS; ++r) {
-                                const float2 wyy = make_float2(ay.w[sy0 + r], ay.w[sy0 + r]);
-                                const float2 dyy = make_float2(ay.dw[sy0 + r], ay.dw[sy0 + r]);
-                                const float2 wyz = __fmul2_rn(wyy, wzz), dyz = __fmul2_rn(dyy, wzz),
-                                             wdz = __fmul2_rn(wyy, dzz);
-#pragma unroll
-                                for (int sx = 0; sx < W; ++sx) {
-                                    const float2 wxx = make_float2(ax.w[sx], ax.w[sx]);
-                                    const float2 dxx = make_float2(ax.dw[sx], ax.dw[sx]);
-                                    acc[r][sx].add2(cm, cp, cb, cs0, cs1, cs2, q, __fmul2_rn(wxx, wyz),
-                                                    __fmul2_rn(dxx, wyz), __fmul2_rn(wxx, dyz), __fmul2_rn(wxx, wdz));
-                                }
-                            }
-                        } else {
-#pragma unroll
-                            for (int r = 0; r < ROWS; ++r) {
-                                const R wy = ay.w[sy0 + r], dyw = ay.dw[sy0 + r];
-                                const R wyz = wy * wz, dyz = dyw * wz, wdz = wy * dzw;
-#pragma unroll
-                                for (int sx = 0; sx < W; ++sx) {
-                                    const R wx = ax.w[sx];
-                                    acc[r][sx].add(q, wx * wyz, ax.dw[sx] * wyz, wx * dyz, wx * wdz);
-                                }
-                            }
-                        }
-                    }
-                    if (!any) continue;
-#pragma unroll
-                    for (int r = 0; r < ROWS; ++r)
-#pragma unroll
-                        for (int sx = 0; sx < W; ++sx) {
-                            const int idx = ((lz + sz) * B + (ly + sy0 + r)) * B + (lx + sx);
-#pragma unroll
-                            for (int ch = 0; ch < NCH; ++ch)
-                                fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, acc[r][sx].get(ch), sc[ch]);
-                        }
-                }
-            }
-        }
-        __syncthreads();
-        long long *dst = staging + (long long)w * NCH * B3;
-        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x)
-            dst[i] = fx_value<R>(acc_lo[i], acc_hi[i]);
-        __syncthreads();
+        p2g_tile<R, ORD, THERM>(tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm, staging, sc, grav, w);
     }
 }
 
@@ -1044,23 +1056,13 @@ __device__ void node_bcs(const Params &P, const NodeBCArgs &bc, int i, int j, in
 // One CTA per tile; each thread owns nodes of the tile, adds the fixed-point
 // partials of the <= 8 node blocks covering the node (exact integer sums),
 // converts to FP64 and applies the nodal operations of the mode.
+// One tile of the nodal kernel: every owned node of tile tiles[w] (or w).
 template <class R, bool THERM>
-__global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeBCArgs bc, const int *tiles,
-                                                    const int *slot, const long long *staging, Ctl *ctl, int mode,
-                                                    int flags) {
+__device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, const NodeBCArgs &bc, const int *tiles,
+                                           const int *slot, const long long *staging, const double *isc, double dt,
+                                           int mode, int flags, int w, unsigned &status) {
     constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
-    const int B = P.B, B3 = B * B * B;
-    const double dt = ctl->dt;
-    unsigned status = 0;
-    double isc[NCH];
-#pragma unroll
-    for (int c = 0; c < NCH; ++c) isc[c] = ctl->inv_scale[c];
-    const int T = P.T;
-    // the fused G2P that follows takes its tiles from 0 (it starts after
-    // this kernel ends, and the previous one has ended)
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->next_g2p = 0;
-    const int nitems = tiles ? ctl->n_touched_tiles : (int)P.ntiles;
-    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    const int B = P.B, B3 = B * B * B, T = P.T;
     const int t = tiles ? tiles[w] : w;
     int tc[3];
     tile_coords(P, t, tc);
@@ -1220,7 +1222,24 @@ __global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeB
             }
         }
     }
-    }
+}
+
+template <class R, bool THERM>
+__global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeBCArgs bc, const int *tiles,
+                                                    const int *slot, const long long *staging, Ctl *ctl, int mode,
+                                                    int flags) {
+    constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
+    const double dt = ctl->dt;
+    unsigned status = 0;
+    double isc[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) isc[c] = ctl->inv_scale[c];
+    // the fused G2P that follows takes its tiles from 0 (it starts after
+    // this kernel ends, and the previous one has ended)
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->next_g2p = 0;
+    const int nitems = tiles ? ctl->n_touched_tiles : (int)P.ntiles;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x)
+        nodes_tile<R, THERM>(P, Nd, bc, tiles, slot, staging, isc, dt, mode, flags, w, status);
     if (status) atomicOr(&ctl->status, status);
 }
 
@@ -1662,34 +1681,15 @@ __device__ __forceinline__ bool all_finite(const R *a, int n) {
 // permutation and written to storage B at its sorted position, so the
 // particle arrays are physically re-ordered by cell every step at no extra
 // pass.  GM_VEL updates velocity in place in A instead.
+// One tile of the fused G2P: stage the tile's node block (v, dv and halo)
+// in shared memory, then update each of the tile's particles.
 template <class R, int ORD>
-__global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
-                                                        const Material *mats, const int *active, const int *start,
-                                                        const int *count, const int32_t *perm, Ctl *ctl, int mode) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
-    R *nb = reinterpret_cast<R *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
+__device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const Params &P, const Parts<R> &A,
+                                         const Parts<R> &Bo, const Nodes<R> &Nd, const NodeBCArgs &bc,
+                                         const Material *mats, const int *active, const int *start, const int *count,
+                                         const int32_t *perm, int mode, int w, double dt, double asr, bool upd_vel,
+                                         float (&run_b)[CH_ALL], double &run_dt, bool &red, unsigned &status) {
     const int B = P.B, B3 = B * B * B;
-    load_tables(tab);
-    const double dt = ctl->dt, time = ctl->time;
-    const double asr = (time < P.applied_sr_time) ? P.applied_sr : 0.0;
-    unsigned status = 0;
-    const bool upd_vel = (mode != GM_STRAIN);
-    // running per-thread maxima of the P2G bounds (float is enough for a
-    // power-of-two scale with a factor-2 margin; rounded up on conversion)
-    float run_b[CH_ALL];
-#pragma unroll
-    for (int c = 0; c < CH_ALL; ++c) run_b[c] = 0.0f;
-    double run_dt = 1.7976931348623157e308;
-    bool red = false;
-    const int nitems = ctl->n_active_tiles;
-    __shared__ int s_item;
-    for (;;) {
-    // tiles are taken in turn from a device counter (reset by k_nodes)
-    if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_g2p, 1);
-    __syncthreads();
-    const int w = s_item;
-    if (w >= nitems) break;
     const int t = active[w];
     int tc[3];
     tile_coords(P, t, tc);
@@ -1835,6 +1835,37 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB) k_g2p_fused(Par
         }
     }
     __syncthreads();
+}
+
+template <class R, int ORD>
+__global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
+                                                        const Material *mats, const int *active, const int *start,
+                                                        const int *count, const int32_t *perm, Ctl *ctl, int mode) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
+    R *nb = reinterpret_cast<R *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
+    load_tables(tab);
+    const double dt = ctl->dt, time = ctl->time;
+    const double asr = (time < P.applied_sr_time) ? P.applied_sr : 0.0;
+    unsigned status = 0;
+    const bool upd_vel = (mode != GM_STRAIN);
+    // running per-thread maxima of the P2G bounds (float is enough for a
+    // power-of-two scale with a factor-2 margin; rounded up on conversion)
+    float run_b[CH_ALL];
+#pragma unroll
+    for (int c = 0; c < CH_ALL; ++c) run_b[c] = 0.0f;
+    double run_dt = 1.7976931348623157e308;
+    bool red = false;
+    const int nitems = ctl->n_active_tiles;
+    __shared__ int s_item;
+    for (;;) {
+        // tiles are taken in turn from a device counter (reset by k_nodes)
+        if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_g2p, 1);
+        __syncthreads();
+        const int w = s_item;
+        if (w >= nitems) break;
+        g2p_tile<R, ORD>(tab, nb, P, A, Bo, Nd, bc, mats, active, start, count, perm, mode, w, dt, asr, upd_vel, run_b,
+                         run_dt, red, status);
     }
     if (mode != GM_VEL) {
         double rb[CH_ALL];
@@ -2440,6 +2471,216 @@ __global__ void k_diag_final(const double *part, int nblk, double *out) {
     out[c] = acc;
 }
 
+// ---------------------------------------------------------------- batched scenes
+// Many independent scenes (each a context with its own grid, particles,
+// control block and buffers) advance with ONE launch of each hot kernel: the
+// items are the concatenation of every scene's tile list, taken dynamically;
+// a block copies the descriptor of an item's scene into shared memory when
+// the scene changes and runs the same tile code as the single-scene kernels.
+template <class R>
+struct SceneDesc {
+    Params P;
+    Parts<R> A, Bo;
+    Nodes<R> N;
+    NodeBCArgs bc;
+    const Material *mats;
+    const int *active, *start, *count, *cell_start, *touched, *slot;
+    const int32_t *perm;
+    long long *staging;
+    Ctl *ctl;
+};
+
+// Largest s with pre[s] <= i (pre[0] = 0, pre ascending).
+__device__ __forceinline__ int scene_of(const int *pre, int ns, int i) {
+    int lo = 0, hi = ns;  // invariant: pre[lo] <= i < pre[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pre[mid] <= i)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+template <class D>
+__device__ __forceinline__ void copy_desc(D *dst, const D *src) {
+    static_assert(sizeof(D) % 8 == 0, "descriptor copied in 8-byte words");
+    const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
+    unsigned long long *d = reinterpret_cast<unsigned long long *>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(D) / 8); i += blockDim.x) d[i] = s[i];
+}
+
+// Prefix sums of the scenes' active and touched tile counts; resets the
+// batch's tile counters.  One block.
+__global__ void k_batch_plan(BatchCtl *b, Ctl *const *ctls) {
+    __shared__ int sh[34];
+    __shared__ int ca, ct;
+    const int ns = b->nscenes;
+    if (threadIdx.x == 0) {
+        ca = ct = 0;
+        b->next_p2g = b->next_nodes = b->next_g2p = 0;
+    }
+    __syncthreads();
+    for (int base = 0; base < ns; base += blockDim.x) {
+        const int s = base + threadIdx.x;
+        const int na = s < ns ? ctls[s]->n_active_tiles : 0;
+        const int nt = s < ns ? ctls[s]->n_touched_tiles : 0;
+        int ta, tt;
+        const int ea = block_exclusive_scan(na, &ta, sh);
+        const int et = block_exclusive_scan(nt, &tt, sh);
+        if (s < ns) {
+            b->pre_active[s] = ca + ea;
+            b->pre_touched[s] = ct + et;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            ca += ta;
+            ct += tt;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        b->pre_active[ns] = ca;
+        b->pre_touched[ns] = ct;
+    }
+}
+
+template <class R, int ORD, bool THERM>
+__global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD, THERM>::MINB)
+    k_p2g_batch(const SceneDesc<R> *descs, BatchCtl *b, int B3) {
+    constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
+    __shared__ SceneDesc<R> sd;
+    __shared__ int s_item, s_scene;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
+    unsigned *acc_lo = reinterpret_cast<unsigned *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
+    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3);
+    load_tables(tab);
+    const int ns = b->nscenes, total = b->pre_active[ns];
+    int cur = -1;
+    R sc[NCH], grav[3];
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int i = atomicAdd(&b->next_p2g, 1);
+            s_item = i;
+            s_scene = i < total ? scene_of(b->pre_active, ns, i) : -1;
+        }
+        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) {
+            acc_lo[i] = 0u;
+            acc_hi[i] = 0;
+        }
+        __syncthreads();
+        const int i = s_item, s = s_scene;
+        if (i >= total) break;
+        if (s != cur) {
+            copy_desc(&sd, &descs[s]);
+            __syncthreads();
+            cur = s;
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) sc[c] = (R)sd.ctl->scale[c];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) grav[d] = (R)sd.P.gravity[d];
+        }
+        p2g_tile<R, ORD, THERM>(tab, acc_lo, acc_hi, sd.P, sd.A, sd.active, sd.start, sd.cell_start, sd.perm,
+                                sd.staging, sc, grav, i - b->pre_active[s]);
+    }
+}
+
+template <class R, bool THERM>
+__global__ void __launch_bounds__(kThreads) k_nodes_batch(const SceneDesc<R> *descs, BatchCtl *b, int mode, int flags) {
+    constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
+    __shared__ SceneDesc<R> sd;
+    __shared__ int s_item, s_scene;
+    const int ns = b->nscenes, total = b->pre_touched[ns];
+    int cur = -1;
+    unsigned status = 0;
+    double isc[NCH], dt = 0.0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int i = atomicAdd(&b->next_nodes, 1);
+            s_item = i;
+            s_scene = i < total ? scene_of(b->pre_touched, ns, i) : -1;
+        }
+        __syncthreads();
+        const int i = s_item, s = s_scene;
+        if (i >= total) break;
+        if (s != cur) {
+            if (cur >= 0 && status) atomicOr(&sd.ctl->status, status);
+            status = 0;
+            __syncthreads();
+            copy_desc(&sd, &descs[s]);
+            __syncthreads();
+            cur = s;
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) isc[c] = sd.ctl->inv_scale[c];
+            dt = sd.ctl->dt;
+        }
+        nodes_tile<R, THERM>(sd.P, sd.N, sd.bc, sd.touched, sd.slot, sd.staging, isc, dt, mode, flags,
+                             i - b->pre_touched[s], status);
+        __syncthreads();
+    }
+    if (cur >= 0 && status) atomicOr(&sd.ctl->status, status);
+}
+
+template <class R, int ORD>
+__global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
+    k_g2p_batch(const SceneDesc<R> *descs, BatchCtl *b, int mode) {
+    __shared__ SceneDesc<R> sd;
+    __shared__ int s_item, s_scene;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
+    R *nb = reinterpret_cast<R *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
+    load_tables(tab);
+    const int ns = b->nscenes, total = b->pre_active[ns];
+    const bool upd_vel = (mode != GM_STRAIN);
+    int cur = -1;
+    unsigned status = 0;
+    double dt = 0.0, asr = 0.0;
+    float run_b[CH_ALL];
+    double run_dt = 1.7976931348623157e308;
+    bool red = false;
+    // the reductions of a scene go to its control block when the block moves
+    // on to another scene, and at the end
+    auto flush = [&]() {
+        if (mode != GM_VEL) {
+            double rb[CH_ALL];
+#pragma unroll
+            for (int c = 0; c < CH_ALL; ++c) rb[c] = (double)run_b[c];
+            block_reduce_push(&sd.ctl->bound_bits[0], &sd.ctl->dtmin_bits, rb, run_dt, red);
+        }
+        if (status) atomicOr(&sd.ctl->status, status);
+        __syncthreads();
+    };
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int i = atomicAdd(&b->next_g2p, 1);
+            s_item = i;
+            s_scene = i < total ? scene_of(b->pre_active, ns, i) : -1;
+        }
+        __syncthreads();
+        const int i = s_item, s = s_scene;
+        if (i >= total) break;
+        if (s != cur) {
+            if (cur >= 0) flush();
+            copy_desc(&sd, &descs[s]);
+            __syncthreads();
+            cur = s;
+            dt = sd.ctl->dt;
+            const double time = sd.ctl->time;
+            asr = (time < sd.P.applied_sr_time) ? sd.P.applied_sr : 0.0;
+#pragma unroll
+            for (int c = 0; c < CH_ALL; ++c) run_b[c] = 0.0f;
+            run_dt = 1.7976931348623157e308;
+            red = false;
+            status = 0;
+        }
+        g2p_tile<R, ORD>(tab, nb, sd.P, sd.A, sd.Bo, sd.N, sd.bc, sd.mats, sd.active, sd.start, sd.count, sd.perm, mode,
+                         i - b->pre_active[s], dt, asr, upd_vel, run_b, run_dt, red, status);
+    }
+    if (cur >= 0) flush();
+}
+
 }  // namespace
 
 // ====================================================================== launchers
@@ -2711,6 +2952,107 @@ void EXG_SFX(launch_diag)(Ctx &c, double *out_dev) {
     k_diag_final<<<1, 32, 0, c.stream>>>(part, nb, out_dev);
     EXG_CUDA_OK(cudaGetLastError());
 }
+
+// ---- batched scenes
+template <class R>
+static bool batch_descriptors_t(Batch &b) {
+    const size_t n = b.scenes.size();
+    bool changed = false;
+    for (int par = 0; par < 2; ++par) {
+        std::vector<SceneDesc<R>> d(n);
+        for (size_t s = 0; s < n; ++s) {
+            Ctx &c = *b.scenes[s];
+            SceneDesc<R> &x = d[s];
+            std::memset(&x, 0, sizeof(x));
+            x.P = c.P;
+            // at the batch's current parity the scene reads its current
+            // storage and writes the other one; the next parity swaps them
+            const bool now = (par == b.parity);
+            x.A = now ? c.A<R>() : c.Bp<R>();
+            x.Bo = now ? c.Bp<R>() : c.A<R>();
+            x.N = c.N<R>();
+            x.bc = make_bc(c);
+            x.mats = c.mat_dev;
+            x.active = c.sb.active;
+            x.start = c.sb.tile_start;
+            x.count = c.sb.tile_count;
+            x.cell_start = c.sb.cell_start;
+            x.touched = c.sb.touched;
+            x.slot = c.sb.slot;
+            x.perm = c.sb.perm;
+            x.staging = c.staging;
+            x.ctl = c.ctl;
+        }
+        const unsigned char *raw = reinterpret_cast<const unsigned char *>(d.data());
+        std::vector<unsigned char> h(raw, raw + n * sizeof(SceneDesc<R>));
+        if (h != b.desc_host[par]) {
+            changed = true;
+            if (!b.desc[par]) EXG_CUDA_OK(cudaMalloc(&b.desc[par], h.size()));
+            EXG_CUDA_OK(cudaMemcpy(b.desc[par], h.data(), h.size(), cudaMemcpyHostToDevice));
+            b.desc_host[par] = std::move(h);
+        }
+    }
+    b.desc_bytes = sizeof(SceneDesc<R>);
+    return changed;
+}
+bool EXG_SFX(batch_descriptors)(Batch &b) { return batch_descriptors_t<EXG_R>(b); }
+
+template <class R, int ORD>
+static void batch_core_t(Batch &b) {
+    Ctx &c0 = *b.scenes[0];
+    const SceneDesc<R> *d = reinterpret_cast<const SceneDesc<R> *>(b.desc[b.parity]);
+    const int B3 = c0.P.B * c0.P.B * c0.P.B;
+    const int flags = PF_MASS | PF_VEL | PF_FORCE;
+    {
+        constexpr int NCH = CH_MOM_END;
+        const size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * NCH * B3;
+        auto kern = k_p2g_batch<R, ORD, false>;
+        constexpr int nthr = P2GCfg<R, ORD, false>::THREADS;
+        EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        static int grid = 0;
+        static size_t gsm = 0;
+        if (!grid || gsm != sm) {
+            grid = persistent_grid(kern, sm, nthr);
+            gsm = sm;
+        }
+        kern<<<grid, nthr, sm, b.stream>>>(d, b.bctl, B3);
+        EXG_CUDA_OK(cudaGetLastError());
+    }
+    {
+        static int grid = 0;
+        if (!grid) grid = persistent_grid(k_nodes_batch<R, false>, 0);
+        k_nodes_batch<R, false><<<grid, kThreads, 0, b.stream>>>(d, b.bctl, NM_FUSED, flags);
+        EXG_CUDA_OK(cudaGetLastError());
+    }
+    {
+        const size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(R) * SmemNodes<R>::NS * B3;
+        auto kern = k_g2p_batch<R, ORD>;
+        EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        static int grid = 0;
+        static size_t gsm = 0;
+        if (!grid || gsm != sm) {
+            grid = persistent_grid(kern, sm, EXG_G2P_THREADS);
+            gsm = sm;
+        }
+        kern<<<grid, EXG_G2P_THREADS, sm, b.stream>>>(d, b.bctl, GM_FULL);
+        EXG_CUDA_OK(cudaGetLastError());
+    }
+}
+void EXG_SFX(launch_batch_core)(Batch &b) {
+    using R = EXG_R;
+    switch (b.scenes[0]->P.uniform_order) {
+        case 1: batch_core_t<R, 1>(b); break;
+        case 2: batch_core_t<R, 2>(b); break;
+        case 3: batch_core_t<R, 3>(b); break;
+        default: batch_core_t<R, 0>(b); break;
+    }
+}
+#if defined(EXG_R_FP64)
+void launch_batch_plan(Batch &b) {
+    k_batch_plan<<<1, kThreads, 0, b.stream>>>(b.bctl, b.ctls);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+#endif
 
 
 #if defined(EXG_R_FP64)

@@ -119,7 +119,8 @@ EXPORTED = [
     "exg_backup_current_temperature", "exg_nodal_time_update_temperature", "exg_apply_nodal_bcs_temperature",
     "exg_store_delta_temperature", "exg_g2p_temperature", "exg_step", "exg_get_time", "exg_set_time",
     "exg_diagnostics", "exg_sort_keys", "exg_tile_size", "exg_set_stage_timing", "exg_last_step_timing",
-    "exg_get_stream", "exg_p2g_momentum_noalloc",
+    "exg_get_stream", "exg_p2g_momentum_noalloc", "exg_batch_create", "exg_batch_destroy", "exg_batch_scene",
+    "exg_batch_num_scenes", "exg_batch_step", "exg_batch_last_error",
 ]
 
 _lib = None
@@ -184,6 +185,12 @@ def lib() -> C.CDLL:
         "exg_last_step_timing": (i, [vp, pd]),
         "exg_get_stream": (i, [vp, C.POINTER(vp)]),
         "exg_p2g_momentum_noalloc": (i, [C.POINTER(Specs), C.POINTER(ParticleSoA), pd, pd, pd, vp]),
+        "exg_batch_create": (i, [C.POINTER(Specs), i, i, C.POINTER(vp)]),
+        "exg_batch_destroy": (i, [vp]),
+        "exg_batch_scene": (vp, [vp, i]),
+        "exg_batch_num_scenes": (i, [vp]),
+        "exg_batch_step": (i, [vp, i]),
+        "exg_batch_last_error": (C.c_char_p, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -439,3 +446,56 @@ class Context:
 
     def synchronize(self):
         self._ck(self.L.exg_synchronize(self.h), "exg_synchronize")
+
+
+class _SceneContext(Context):
+    """Context of one scene of a Batch (owned by the batch)."""
+
+    def __init__(self, batch: "Batch", handle: int, specs: Specs):
+        self.L = lib()
+        self.specs = specs.copy()
+        self.h = C.c_void_p(handle)
+        self.n = 0
+        self._batch = batch
+
+    def close(self):
+        self.h = C.c_void_p()  # the batch destroys it
+
+
+class Batch:
+    """Independent scenes advanced together, one launch per hot kernel
+    (exg_batch in include/exg.h)."""
+
+    def __init__(self, specs: list, device: int = 0):
+        self.L = lib()
+        arr = (Specs * len(specs))(*[s.copy() for s in specs])
+        self.h = C.c_void_p()
+        rc = self.L.exg_batch_create(arr, len(specs), device, C.byref(self.h))
+        if rc:
+            raise ExgError(rc, "exg_batch_create")
+        self.scenes = [_SceneContext(self, self.L.exg_batch_scene(self.h, i), specs[i]) for i in range(len(specs))]
+
+    def stream(self) -> int:
+        """The CUDA stream every scene of the batch enqueues on."""
+        return self.scenes[0].stream()
+
+    def synchronize(self):
+        self.scenes[0].synchronize()
+
+    def step(self, nsteps: int = 1):
+        rc = self.L.exg_batch_step(self.h, nsteps)
+        if rc:
+            raise ExgError(rc, "exg_batch_step", self.L.exg_batch_last_error(self.h).decode(errors="replace"))
+
+    def close(self):
+        if self.h:
+            for sc in self.scenes:
+                sc.h = C.c_void_p()
+            self.L.exg_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

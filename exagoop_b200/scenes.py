@@ -93,6 +93,15 @@ def axial_bar(nx=64, steps=1000, precision=nt.PREC_FP64):
     return s, p
 
 
+def dam_break_specs(n, size, precision=nt.PREC_FP64, order=2):
+    """Specs of dam_break: gravity -9.81 in z, CFL 0.1, FLIP 0.99, slip walls."""
+    s = base_specs((0, 0, 0), size, n, order, precision)
+    s.gravity[2] = -9.81
+    s.cfl = 0.1
+    s.alpha_pic_flip = 0.99
+    return s
+
+
 def dam_break(n=(256, 128, 128), size=(1.0, 0.5, 0.5), block=(0.4, 0.5, 0.3), seed=1234,
               precision=nt.PREC_FP64, order=2):
     """3-D dam break of a weakly compressible fluid: Tait EOS K = 2e6 Pa,
@@ -100,10 +109,7 @@ def dam_break(n=(256, 128, 128), size=(1.0, 0.5, 0.5), block=(0.4, 0.5, 0.3), se
     the low corner at 2x2x2 particles per cell, jittered uniformly within
     +-0.25 dx from a seed; quadratic B-splines, slip walls, CFL dt."""
     dx = tuple(size[d] / n[d] for d in range(3))
-    s = base_specs((0, 0, 0), size, n, order, precision)
-    s.gravity[2] = -9.81
-    s.cfl = 0.1
-    s.alpha_pic_flip = 0.99
+    s = dam_break_specs(n, size, precision, order)
     pos = lattice((0, 0, 0), block, dx, (2, 2, 2))
     rng = np.random.default_rng(seed)
     pos = pos + rng.uniform(-0.25, 0.25, size=pos.shape) * np.array(dx)[:, None]
@@ -238,3 +244,28 @@ def heated_block(n=(24, 16, 20), size=(1.2, 0.8, 1.0), fill=0.7, order=2, seed=7
         c = (size[0] / 2, size[1] / 2, fill * size[2] / 2)
         phi = sphere_union_levelset(s, [c], [0.25])
     return s, p, phi
+
+
+def batched_dam_breaks(n_scenes=64, sides=(32, 48, 64, 96, 128), fill=(0.1, 0.4), seed=2024, precision=nt.PREC_MIXED):
+    """Generator of the batched uneven scenes: n_scenes independent dam
+    breaks (the dam_break fluid and walls) in unit cubes with a cubic grid
+    side drawn from `sides` and a water fill fraction f drawn uniformly from
+    `fill`; the block spans x in [0, 2f], all of y and z in [0, 0.5] (volume
+    fraction f) at 2x2x2 particles per cell, jittered.  Yields (specs,
+    particles) one scene at a time, so the host holds one scene's arrays."""
+    draws = batched_scene_sizes(n_scenes, sides, fill, seed)
+    for i, (n, f) in enumerate(draws):
+        yield dam_break(n=(n, n, n), size=(1.0, 1.0, 1.0), block=(2.0 * f, 1.0, 0.5), seed=seed + 1 + i,
+                        precision=precision)
+
+
+def batched_specs(n_scenes=64, sides=(32, 48, 64, 96, 128), fill=(0.1, 0.4), seed=2024, precision=nt.PREC_MIXED):
+    """Specs of the scenes batched_dam_breaks yields, without particles."""
+    return [dam_break_specs((n, n, n), (1.0, 1.0, 1.0), precision)
+            for n, _ in batched_scene_sizes(n_scenes, sides, fill, seed)]
+
+
+def batched_scene_sizes(n_scenes=64, sides=(32, 48, 64, 96, 128), fill=(0.1, 0.4), seed=2024):
+    """(side, fill) of every scene batched_dam_breaks generates."""
+    rng = np.random.default_rng(seed)
+    return [(int(rng.choice(sides)), float(rng.uniform(*fill))) for _ in range(n_scenes)]

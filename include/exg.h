@@ -280,6 +280,27 @@ int exg_step(exg_ctx *ctx, int nsteps);
 int exg_get_time(exg_ctx *ctx, double *time, double *last_dt, int64_t *steps);
 int exg_set_time(exg_ctx *ctx, double time, int64_t steps);
 
+/* ------------------------------------------------ batches of scenes
+ * Many independent scenes, each with its own grid, particles and
+ * parameters, advanced together: every hot kernel of a step (P2G, nodal
+ * update, fused G2P) is ONE launch over the tiles of all scenes, taken from
+ * a device counter; the per-scene sort and bookkeeping kernels run in the
+ * same CUDA graph.  No counterpart in the reference, which runs one scene
+ * per process.  All scenes share exg.precision, the B-spline order of every
+ * axis and exg.tile, run the USL scheme, and use neither temperature nor
+ * UDF wall tables (EXG_ERR_UNSUPPORTED otherwise). */
+typedef struct exg_batch exg_batch;
+int exg_batch_create(const exg_specs *specs, int nscenes, int device, exg_batch **out);
+int exg_batch_destroy(exg_batch *batch);
+/* Context of scene i, owned by the batch (never pass it to exg_ctx_destroy):
+ * upload, download, exg_init_internal_forces, exg_diagnostics and
+ * exg_get_time work on it as on any context. */
+exg_ctx *exg_batch_scene(exg_batch *batch, int i);
+int exg_batch_num_scenes(const exg_batch *batch);
+/* nsteps explicit steps of every scene; each scene keeps its own dt and time. */
+int exg_batch_step(exg_batch *batch, int nsteps);
+const char *exg_batch_last_error(const exg_batch *batch);
+
 /* Deterministic device reductions of Do_All_Diagnostics (utilities.cpp:551-615). */
 int exg_diagnostics(exg_ctx *ctx, exg_diag *out);
 
