@@ -140,6 +140,20 @@ def workload(args, precision):
     return s, p, name
 
 
+def job_reduce(ms, units, world, device="cuda"):
+    """Whole-job figures over the ranks: the slowest rank's device time
+    (max) and the units all ranks processed (sum).  Every rank calls it
+    once, in the same order (NCCL on the GPUs, gloo in the CPU tests)."""
+    if world == 1:
+        return float(ms), int(units)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    u = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    torch.distributed.all_reduce(u)
+    return float(t.item()), int(u.item())
+
+
 def time_steps(ctx, K, W):
     import torch
     stream = torch.cuda.ExternalStream(ctx.stream())
@@ -171,11 +185,7 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     with ClockSampler(dev) as clk:
         ms = time_steps(ctx, args.steps, args.warmup)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms = float(t.item())
-    n_total = p.n * world
+    ms, n_total = job_reduce(ms, p.n, world)
     value = n_total * args.steps / (ms * 1e-3)
     # per-stage device times (eager, CUDA events between the stages)
     ctx.stage_timing(True)
@@ -261,15 +271,7 @@ def run_batch(args, rank, world):
     torch.cuda.synchronize()
     with ClockSampler(dev) as clk:
         ms = time_steps(b, args.steps, args.warmup)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        tot = torch.tensor([float(total)], device="cuda")
-        torch.distributed.all_reduce(tot)
-        total_all = int(tot.item())
-    else:
-        total_all = total
-    ms = float(t.item())
+    ms, total_all = job_reduce(ms, total, world)
     value = total_all * args.steps / (ms * 1e-3)
     sides = [int(s.ncells[0]) for s in specs]
     line = {
