@@ -285,7 +285,10 @@ def run_batch(args, rank, world):
                    "parallelism": f"replicas{world}" if world > 1 else "single"},
         "clocks": clk.summary(),
         "e2e": None,
-        "gpu_launches": args.steps * (len(specs) * 8 + 4),
+        # per scene: dt_finalize, keys, tile_scan, touched, scatter,
+        # tile_sort, scales, copy_lost, time_advance; per batch: plan and the
+        # batched P2G, nodal and G2P kernels
+        "gpu_launches": args.steps * (len(specs) * 9 + 4),
         "roofline": None,
         "cpu_baseline": None,
     }
