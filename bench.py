@@ -258,10 +258,10 @@ def run_batch(args, rank, world):
     dev = torch.cuda.current_device()
     prec = nt.PREC_MIXED if args.precision == "mixed" else nt.PREC_FP64
     seed = 2024 + rank
-    specs = scenes.batched_specs(seed=seed, precision=prec)
+    specs = scenes.batched_specs(n_scenes=args.scenes, seed=seed, precision=prec)
     b = nt.Batch(specs, device=dev)
     total = 0
-    for sc, (s, p) in zip(b.scenes, scenes.batched_dam_breaks(seed=seed, precision=prec)):
+    for sc, (s, p) in zip(b.scenes, scenes.batched_dam_breaks(n_scenes=args.scenes, seed=seed, precision=prec)):
         sc.upload(p)
         sc.Initialise_Internal_Forces()
         total += p.n
@@ -336,6 +336,7 @@ def main():
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--scale", type=float, default=1.0, help="grid scale factor (1 = the benchmark size)")
     ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--scenes", type=int, default=64, help="scenes of --config batch")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     args = ap.parse_args()

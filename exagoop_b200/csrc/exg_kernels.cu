@@ -2475,8 +2475,9 @@ __global__ void k_diag_final(const double *part, int nblk, double *out) {
 // Many independent scenes (each a context with its own grid, particles,
 // control block and buffers) advance with ONE launch of each hot kernel: the
 // items are the concatenation of every scene's tile list, taken dynamically;
-// a block copies the descriptor of an item's scene into shared memory when
-// the scene changes and runs the same tile code as the single-scene kernels.
+// a block reads the item's scene descriptor in place (read-only global
+// memory, so its fields stay in registers and the L1 across the tile) and
+// runs the same tile code as the single-scene kernels.
 template <class R>
 struct SceneDesc {
     Params P;
@@ -2501,14 +2502,6 @@ __device__ __forceinline__ int scene_of(const int *pre, int ns, int i) {
             hi = mid;
     }
     return lo;
-}
-
-template <class D>
-__device__ __forceinline__ void copy_desc(D *dst, const D *src) {
-    static_assert(sizeof(D) % 8 == 0, "descriptor copied in 8-byte words");
-    const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
-    unsigned long long *d = reinterpret_cast<unsigned long long *>(dst);
-    for (int i = threadIdx.x; i < (int)(sizeof(D) / 8); i += blockDim.x) d[i] = s[i];
 }
 
 // Prefix sums of the scenes' active and touched tile counts; resets the
@@ -2548,9 +2541,8 @@ __global__ void k_batch_plan(BatchCtl *b, Ctl *const *ctls) {
 
 template <class R, int ORD, bool THERM>
 __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD, THERM>::MINB)
-    k_p2g_batch(const SceneDesc<R> *descs, BatchCtl *b, int B3) {
+    k_p2g_batch(const SceneDesc<R> *__restrict__ descs, BatchCtl *b, int B3) {
     constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
-    __shared__ SceneDesc<R> sd;
     __shared__ int s_item, s_scene;
     extern __shared__ __align__(16) unsigned char smraw[];
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
@@ -2573,9 +2565,8 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
         __syncthreads();
         const int i = s_item, s = s_scene;
         if (i >= total) break;
+        const SceneDesc<R> &sd = descs[s];
         if (s != cur) {
-            copy_desc(&sd, &descs[s]);
-            __syncthreads();
             cur = s;
 #pragma unroll
             for (int c = 0; c < NCH; ++c) sc[c] = (R)sd.ctl->scale[c];
@@ -2588,9 +2579,9 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
 }
 
 template <class R, bool THERM>
-__global__ void __launch_bounds__(kThreads) k_nodes_batch(const SceneDesc<R> *descs, BatchCtl *b, int mode, int flags) {
+__global__ void __launch_bounds__(kThreads) k_nodes_batch(const SceneDesc<R> *__restrict__ descs, BatchCtl *b, int mode,
+                                                          int flags) {
     constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
-    __shared__ SceneDesc<R> sd;
     __shared__ int s_item, s_scene;
     const int ns = b->nscenes, total = b->pre_touched[ns];
     int cur = -1;
@@ -2605,12 +2596,10 @@ __global__ void __launch_bounds__(kThreads) k_nodes_batch(const SceneDesc<R> *de
         __syncthreads();
         const int i = s_item, s = s_scene;
         if (i >= total) break;
+        const SceneDesc<R> &sd = descs[s];
         if (s != cur) {
-            if (cur >= 0 && status) atomicOr(&sd.ctl->status, status);
+            if (cur >= 0 && status) atomicOr(&descs[cur].ctl->status, status);
             status = 0;
-            __syncthreads();
-            copy_desc(&sd, &descs[s]);
-            __syncthreads();
             cur = s;
 #pragma unroll
             for (int c = 0; c < NCH; ++c) isc[c] = sd.ctl->inv_scale[c];
@@ -2620,13 +2609,12 @@ __global__ void __launch_bounds__(kThreads) k_nodes_batch(const SceneDesc<R> *de
                              i - b->pre_touched[s], status);
         __syncthreads();
     }
-    if (cur >= 0 && status) atomicOr(&sd.ctl->status, status);
+    if (cur >= 0 && status) atomicOr(&descs[cur].ctl->status, status);
 }
 
 template <class R, int ORD>
 __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
-    k_g2p_batch(const SceneDesc<R> *descs, BatchCtl *b, int mode) {
-    __shared__ SceneDesc<R> sd;
+    k_g2p_batch(const SceneDesc<R> *__restrict__ descs, BatchCtl *b, int mode) {
     __shared__ int s_item, s_scene;
     extern __shared__ __align__(16) unsigned char smraw[];
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
@@ -2642,14 +2630,14 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
     bool red = false;
     // the reductions of a scene go to its control block when the block moves
     // on to another scene, and at the end
-    auto flush = [&]() {
+    auto flush = [&](Ctl *ctl) {
         if (mode != GM_VEL) {
             double rb[CH_ALL];
 #pragma unroll
             for (int c = 0; c < CH_ALL; ++c) rb[c] = (double)run_b[c];
-            block_reduce_push(&sd.ctl->bound_bits[0], &sd.ctl->dtmin_bits, rb, run_dt, red);
+            block_reduce_push(&ctl->bound_bits[0], &ctl->dtmin_bits, rb, run_dt, red);
         }
-        if (status) atomicOr(&sd.ctl->status, status);
+        if (status) atomicOr(&ctl->status, status);
         __syncthreads();
     };
     for (;;) {
@@ -2661,10 +2649,9 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
         __syncthreads();
         const int i = s_item, s = s_scene;
         if (i >= total) break;
+        const SceneDesc<R> &sd = descs[s];
         if (s != cur) {
-            if (cur >= 0) flush();
-            copy_desc(&sd, &descs[s]);
-            __syncthreads();
+            if (cur >= 0) flush(descs[cur].ctl);
             cur = s;
             dt = sd.ctl->dt;
             const double time = sd.ctl->time;
@@ -2678,7 +2665,7 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
         g2p_tile<R, ORD>(tab, nb, sd.P, sd.A, sd.Bo, sd.N, sd.bc, sd.mats, sd.active, sd.start, sd.count, sd.perm, mode,
                          i - b->pre_active[s], dt, asr, upd_vel, run_b, run_dt, red, status);
     }
-    if (cur >= 0) flush();
+    if (cur >= 0) flush(descs[cur].ctl);
 }
 
 }  // namespace
@@ -2730,7 +2717,9 @@ void launch_sort_rest(Ctx &c, bool touched_list) {
     EXG_CUDA_OK(cudaFuncSetAttribute(k_tile_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     static int sgrid = 0;
     if (!sgrid) sgrid = persistent_grid(k_tile_sort, sm);
-    k_tile_sort<<<sgrid, kThreads, sm, c.stream>>>(c.sb.active, c.sb.tile_start, c.sb.tile_count, c.sb.key,
+    // no more blocks than the scene has tiles (small scenes of a batch)
+    const int tgrid = (int)std::min<long long>(sgrid, c.P.ntiles);
+    k_tile_sort<<<tgrid, kThreads, sm, c.stream>>>(c.sb.active, c.sb.tile_start, c.sb.tile_count, c.sb.key,
                                                     c.sb.bucket, c.sb.bucket + c.cap, c.sb.perm, c.sb.cell_start, ncell,
                                                     c.ctl);
     if (touched_list)

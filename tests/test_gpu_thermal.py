@@ -231,3 +231,28 @@ def test_mixed_precision_thermal():
     g, r = ctx.download(), o.download()
     eT = np.linalg.norm(g.rdata[nt.R_TEMPERATURE] - r.rdata[nt.R_TEMPERATURE]) / np.linalg.norm(r.rdata[nt.R_TEMPERATURE])
     assert eT < 1e-6, eT
+
+
+def test_fused_thermal_periodic_conserves_heat():
+    # fully periodic, no sources: the GPU step matches the oracle and keeps
+    # sum m cp T to round-off (no BC touches a node)
+    s, p, _ = scenes.heated_block(n=(24, 24, 24), size=(0.6, 0.6, 0.6), fill=1.0, seed=7)
+    for d in range(3):
+        s.periodic[d] = 1
+        s.bclo[d] = s.bchi[d] = nt.BC_PERIODIC
+        s.bclo_temp[d] = s.bchi_temp[d] = nt.BCT_PERIODIC
+        s.gravity[d] = 0.0
+    p.rdata[nt.R_HEATSRC] = 0.0
+    ctx, o = pair(s, p)
+    ctx.Initialise_Internal_Forces()
+    o.init_internal_forces()
+
+    def heat(q):
+        return float(np.sum(q.rdata[nt.R_MASS] * q.rdata[nt.R_SPHEAT] * q.rdata[nt.R_TEMPERATURE]))
+
+    h0 = heat(ctx.download())
+    ctx.step(10)
+    assert o.step(10) == 0
+    g, r = ctx.download(), o.download()
+    check_parts(g, r, FUSED_FIELDS)
+    assert abs(heat(g) - h0) / h0 < 1e-12
