@@ -210,18 +210,22 @@ void free_list(std::vector<void *> &al) {
     al.clear();
 }
 
+// Host transfers of the particle state: every real field crosses PCIe as the
+// caller's FP64 array (pinned when it comes from exg_particles_alloc_pinned)
+// and is converted on the device; downloads return to upload order on the
+// device (pid), so the host side is contiguous copies only.
 template <class R>
 void upload_parts(Ctx &c, const exg_particle_soa *h, const std::vector<int32_t> &mat) {
     Parts<R> &P = c.A<R>();
     const long long n = h->np;
-    std::vector<R> buf(n);
+    const bool f64 = sizeof(R) == 8;
     auto put_r = [&](R *dst, int field, double sub = 0.0) {
         const double *src = h->rdata + (size_t)field * n;
-        for (long long i = 0; i < n; ++i) buf[i] = (R)(src[i] - sub);
-        EXG_CUDA_OK(cudaMemcpy(dst, buf.data(), sizeof(R) * n, cudaMemcpyHostToDevice));
+        f64 ? h2d_field_fp64(c, dst, src, n, sub) : h2d_field_fp32(c, dst, src, n, sub);
     };
     for (int d = 0; d < 3; ++d) {
-        EXG_CUDA_OK(cudaMemcpy(P.x[d], h->pos + (size_t)d * n, sizeof(double) * n, cudaMemcpyHostToDevice));
+        EXG_CUDA_OK(cudaMemcpyAsync(P.x[d], h->pos + (size_t)d * n, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                    c.stream));
         put_r(P.v[d], EXG_R_VEL + d);
         put_r(P.vp[d], EXG_R_VEL_PRIME + d);
     }
@@ -240,42 +244,39 @@ void upload_parts(Ctx &c, const exg_particle_soa *h, const std::vector<int32_t> 
     put_r(P.radius, EXG_R_RADIUS);
     put_r(P.yacc, EXG_R_YACC);
     if (c.specs.use_temp) {
-        EXG_CUDA_OK(cudaMemcpy(P.T, h->rdata + (size_t)EXG_R_TEMPERATURE * n, sizeof(double) * n,
-                               cudaMemcpyHostToDevice));
+        EXG_CUDA_OK(cudaMemcpyAsync(P.T, h->rdata + (size_t)EXG_R_TEMPERATURE * n, sizeof(double) * n,
+                                    cudaMemcpyHostToDevice, c.stream));
         put_r(P.cp, EXG_R_SPHEAT);
         put_r(P.kc, EXG_R_THERMCOND);
         for (int d = 0; d < 3; ++d) put_r(P.q[d], EXG_R_HEATFLUX + d);
         put_r(P.Q, EXG_R_HEATSRC);
     }
-    EXG_CUDA_OK(cudaMemcpy(P.mat, mat.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    EXG_CUDA_OK(cudaMemcpyAsync(P.mat, mat.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, c.stream));
     std::vector<uint8_t> ph(n);
-    std::vector<int32_t> rid(n), pid(n);
+    std::vector<int32_t> pid(n);
     for (long long i = 0; i < n; ++i) {
         ph[i] = (uint8_t)h->idata[(size_t)EXG_I_PHASE * n + i];
-        rid[i] = h->idata[(size_t)EXG_I_RIGID_ID * n + i];
         pid[i] = (int32_t)i;
     }
-    EXG_CUDA_OK(cudaMemcpy(P.phase, ph.data(), n, cudaMemcpyHostToDevice));
-    EXG_CUDA_OK(cudaMemcpy(P.rigid, rid.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
-    EXG_CUDA_OK(cudaMemcpy(P.pid, pid.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    EXG_CUDA_OK(cudaMemcpyAsync(P.phase, ph.data(), n, cudaMemcpyHostToDevice, c.stream));
+    EXG_CUDA_OK(cudaMemcpyAsync(P.rigid, h->idata + (size_t)EXG_I_RIGID_ID * n, sizeof(int32_t) * n,
+                                cudaMemcpyHostToDevice, c.stream));
+    EXG_CUDA_OK(cudaMemcpyAsync(P.pid, pid.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, c.stream));
+    EXG_CUDA_OK(cudaStreamSynchronize(c.stream));  // the host vectors above go out of scope
 }
 
 template <class R>
 void download_parts(Ctx &c, exg_particle_soa *h) {
     Parts<R> &P = c.A<R>();
     const long long n = c.np;
-    std::vector<int32_t> pid(n);
-    EXG_CUDA_OK(cudaMemcpy(pid.data(), P.pid, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
-    std::vector<R> buf(n);
+    if (n == 0) return;
+    const bool f64 = sizeof(R) == 8;
     auto get_r = [&](const R *src, int field, double add = 0.0) {
-        EXG_CUDA_OK(cudaMemcpy(buf.data(), src, sizeof(R) * n, cudaMemcpyDeviceToHost));
         double *dst = h->rdata + (size_t)field * n;
-        for (long long i = 0; i < n; ++i) dst[pid[i]] = (double)buf[i] + add;
+        f64 ? d2h_field_fp64(c, src, P.pid, dst, n, add) : d2h_field_fp32(c, src, P.pid, dst, n, add);
     };
-    std::vector<double> xb(n);
+    d2h_positions(c, P.x, P.pid, h->pos, n);
     for (int d = 0; d < 3; ++d) {
-        EXG_CUDA_OK(cudaMemcpy(xb.data(), P.x[d], sizeof(double) * n, cudaMemcpyDeviceToHost));
-        for (long long i = 0; i < n; ++i) h->pos[(size_t)d * n + pid[i]] = xb[i];
         get_r(P.v[d], EXG_R_VEL + d);
         get_r(P.vp[d], EXG_R_VEL_PRIME + d);
     }
@@ -294,8 +295,7 @@ void download_parts(Ctx &c, exg_particle_soa *h) {
     get_r(P.radius, EXG_R_RADIUS);
     get_r(P.yacc, EXG_R_YACC);
     if (c.specs.use_temp) {
-        EXG_CUDA_OK(cudaMemcpy(xb.data(), P.T, sizeof(double) * n, cudaMemcpyDeviceToHost));
-        for (long long i = 0; i < n; ++i) h->rdata[(size_t)EXG_R_TEMPERATURE * n + pid[i]] = xb[i];
+        d2h_field_fp64(c, P.T, P.pid, h->rdata + (size_t)EXG_R_TEMPERATURE * n, n, 0.0);
         get_r(P.cp, EXG_R_SPHEAT);
         get_r(P.kc, EXG_R_THERMCOND);
         for (int d = 0; d < 3; ++d) get_r(P.q[d], EXG_R_HEATFLUX + d);
@@ -306,21 +306,19 @@ void download_parts(Ctx &c, exg_particle_soa *h) {
         for (int f : tf)
             std::fill(h->rdata + (size_t)f * n, h->rdata + (size_t)(f + 1) * n, 0.0);
     }
-    std::vector<int32_t> mat(n), rid(n);
-    std::vector<uint8_t> ph(n);
-    EXG_CUDA_OK(cudaMemcpy(mat.data(), P.mat, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
-    EXG_CUDA_OK(cudaMemcpy(rid.data(), P.rigid, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
-    EXG_CUDA_OK(cudaMemcpy(ph.data(), P.phase, n, cudaMemcpyDeviceToHost));
-    for (long long i = 0; i < n; ++i) {
-        const Material &m = c.mats[mat[i]];
-        const long long j = pid[i];
+    d2h_int(c, P.phase, 1, P.pid, h->idata + (size_t)EXG_I_PHASE * n, n);
+    d2h_int(c, P.rigid, 4, P.pid, h->idata + (size_t)EXG_I_RIGID_ID * n, n);
+    // material index in upload order, expanded to the per-particle fields
+    std::vector<int32_t> mat(n);
+    d2h_int(c, P.mat, 4, P.pid, mat.data(), n);
+    EXG_CUDA_OK(cudaStreamSynchronize(c.stream));
+    for (long long j = 0; j < n; ++j) {
+        const Material &m = c.mats[mat[j]];
         h->rdata[(size_t)EXG_R_E * n + j] = m.E;
         h->rdata[(size_t)EXG_R_NU * n + j] = m.nu;
         h->rdata[(size_t)EXG_R_BULK * n + j] = m.K;
         h->rdata[(size_t)EXG_R_GAMMA * n + j] = m.gamma;
         h->rdata[(size_t)EXG_R_VISC * n + j] = m.mu;
-        h->idata[(size_t)EXG_I_PHASE * n + j] = ph[i];
-        h->idata[(size_t)EXG_I_RIGID_ID * n + j] = rid[i];
         h->idata[(size_t)EXG_I_MODEL * n + j] = m.model;
     }
 }
@@ -613,7 +611,7 @@ int exg_ctx_destroy(exg_ctx *ctx) {
     cudaFree(c.ttmp);
     void *bufs[] = {c.sb.key, c.sb.perm, c.sb.bucket, c.sb.tile_count, c.sb.tile_fill, c.sb.tile_start,
                     c.sb.active, c.sb.slot, c.sb.touched, c.sb.touched_step, c.sb.cell_start, c.staging, c.ctl,
-                    c.bounds_cur, c.bounds2, c.dtmin2, c.mat_dev, c.diag_dev};
+                    c.bounds_cur, c.bounds2, c.dtmin2, c.mat_dev, c.diag_dev, c.stage};
     for (void *p : bufs) cudaFree(p);
     if (c.ctl_host) cudaFreeHost(c.ctl_host);
     for (auto &e : c.ev)
@@ -657,25 +655,34 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
         std::map<std::tuple<double, double, double, double, double, int>, int> idx;
         std::vector<int32_t> mat(n);
         c.mats.clear();
+        auto key_of = [&](long long i) {
+            return std::make_tuple(p->rdata[(size_t)EXG_R_E * n + i], p->rdata[(size_t)EXG_R_NU * n + i],
+                                   p->rdata[(size_t)EXG_R_BULK * n + i], p->rdata[(size_t)EXG_R_GAMMA * n + i],
+                                   p->rdata[(size_t)EXG_R_VISC * n + i], (int)p->idata[(size_t)EXG_I_MODEL * n + i]);
+        };
+        std::tuple<double, double, double, double, double, int> last;
+        int last_id = -1;
         for (long long i = 0; i < n; ++i) {
-            Material m;
-            m.E = p->rdata[(size_t)EXG_R_E * n + i];
-            m.nu = p->rdata[(size_t)EXG_R_NU * n + i];
-            m.K = p->rdata[(size_t)EXG_R_BULK * n + i];
-            m.gamma = p->rdata[(size_t)EXG_R_GAMMA * n + i];
-            m.mu = p->rdata[(size_t)EXG_R_VISC * n + i];
-            m.model = p->idata[(size_t)EXG_I_MODEL * n + i];
-            m.pad = 0;
-            if (m.model != 0 && m.model != 1)
-                return fail(ctx, EXG_ERR_UNSUPPORTED, "constitutive model " + std::to_string(m.model) +
+            const auto key = key_of(i);
+            if (last_id >= 0 && key == last) {  // runs of one material: no map lookup
+                mat[i] = last_id;
+                continue;
+            }
+            const int model = std::get<5>(key);
+            if (model != 0 && model != 1)
+                return fail(ctx, EXG_ERR_UNSUPPORTED, "constitutive model " + std::to_string(model) +
                                                           " (neo-Hookean) is outside this library's scope");
-            auto key = std::make_tuple(m.E, m.nu, m.K, m.gamma, m.mu, m.model);
             auto it = idx.find(key);
             if (it == idx.end()) {
+                Material m;
+                std::tie(m.E, m.nu, m.K, m.gamma, m.mu, m.model) = key;
+                m.pad = 0;
                 it = idx.emplace(key, (int)c.mats.size()).first;
                 c.mats.push_back(m);
             }
             mat[i] = it->second;
+            last = key;
+            last_id = it->second;
         }
         if (c.mats.empty()) c.mats.push_back(Material{});
         if (c.mat_dev) cudaFree(c.mat_dev);
@@ -688,6 +695,11 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
         if (c.orient) std::swap(c.pa, c.pb);
         c.orient = 0;
         const bool temp = c.specs.use_temp != 0;
+        if (c.stage_cap < n) {  // one FP64 field for the host transfers
+            cudaFree(c.stage);
+            c.stage = dalloc<double>(n > 0 ? n : 1);
+            c.stage_cap = n;
+        }
         if (fp64(c)) {
             delete reinterpret_cast<Parts<double> *>(c.pa);
             delete reinterpret_cast<Parts<double> *>(c.pb);
@@ -735,6 +747,34 @@ int exg_particles_download(exg_ctx *ctx, exg_particle_soa *p) {
             download_parts<float>(c, p);
     });
     return EXG_OK;
+}
+
+int exg_particles_alloc_pinned(int64_t np, exg_particle_soa *p) {
+    if (!p || np < 0) return EXG_ERR_ARG;
+    p->np = np;
+    p->pos = p->rdata = nullptr;
+    p->idata = nullptr;
+    const size_t n = (size_t)(np > 0 ? np : 1);
+    if (cudaMallocHost(&p->pos, 3 * n * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&p->rdata, (size_t)EXG_NREAL * n * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&p->idata, (size_t)EXG_NINT * n * sizeof(int32_t)) != cudaSuccess) {
+        exg_particles_free_pinned(p);
+        return EXG_ERR_ALLOC;
+    }
+    std::memset(p->pos, 0, 3 * n * sizeof(double));
+    std::memset(p->rdata, 0, (size_t)EXG_NREAL * n * sizeof(double));
+    std::memset(p->idata, 0, (size_t)EXG_NINT * n * sizeof(int32_t));
+    return EXG_OK;
+}
+
+void exg_particles_free_pinned(exg_particle_soa *p) {
+    if (!p) return;
+    if (p->pos) cudaFreeHost(p->pos);
+    if (p->rdata) cudaFreeHost(p->rdata);
+    if (p->idata) cudaFreeHost(p->idata);
+    p->pos = p->rdata = nullptr;
+    p->idata = nullptr;
+    p->np = 0;
 }
 
 int exg_num_particles(exg_ctx *ctx, int64_t *np) {

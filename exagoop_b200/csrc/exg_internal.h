@@ -49,6 +49,9 @@ struct SortBufs {
 };
 
 struct Ctx;
+// positions and integer fields back to upload order (exg_kernels.cu)
+void d2h_positions(Ctx &c, double *const x[3], const int32_t *pid, double *host, long long n);
+void d2h_int(Ctx &c, const void *src, int bytes, const int32_t *pid, int32_t *host, long long n);
 
 // launchers (exg_kernels.cu; _fp64/_fp32 variants come from the two
 // precision builds of that file)
@@ -77,7 +80,9 @@ void launch_node_reset(Ctx &c);
     void launch_diag##sfx(Ctx &c, double *out_dev);                              \
     void launch_temp_node_op##sfx(Ctx &c, int op, double dt);                     \
     void launch_temp_bcs##sfx(Ctx &c, int walls_mask, int udf, int ls, int dirichlet_only); \
-    void launch_g2p_temp##sfx(Ctx &c, int upd_T, int upd_q);
+    void launch_g2p_temp##sfx(Ctx &c, int upd_T, int upd_q);                     \
+    void h2d_field##sfx(Ctx &c, void *dst, const double *host, long long n, double sub); \
+    void d2h_field##sfx(Ctx &c, const void *src, const int32_t *pid, double *host, long long n, double add);
 EXG_DECL_PREC(_fp64)
 EXG_DECL_PREC(_fp32)
 
@@ -135,6 +140,8 @@ struct Ctx {
     // sort
     SortBufs sb;
     long long *staging = nullptr;      // P2G partial node blocks (fixed point)
+    double *stage = nullptr;           // one FP64 particle field: host transfers
+    long long stage_cap = 0;
     size_t staging_cap = 0;            // in tiles
     int nch = 7;
     // control block

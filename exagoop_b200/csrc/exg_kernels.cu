@@ -2668,6 +2668,25 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
     if (cur >= 0) flush(descs[cur].ctl);
 }
 
+// ---------------------------------------------------------------- host transfers
+// Particle fields cross PCIe as the caller's FP64 arrays; the precision
+// conversion and the return to upload order run here.
+template <class R>
+__global__ void k_from_f64(const double *src, R *dst, long long n, double sub) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = (R)(src[i] - sub);
+}
+template <class R>
+__global__ void k_to_f64_unperm(const R *src, const int32_t *pid, double *dst, long long n, double add) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[pid[i]] = (double)src[i] + add;
+}
+template <class T>
+__global__ void k_unperm_i32(const T *src, const int32_t *pid, int32_t *dst, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[pid[i]] = (int32_t)src[i];
+}
+
 }  // namespace
 
 // ====================================================================== launchers
@@ -2941,6 +2960,45 @@ void EXG_SFX(launch_diag)(Ctx &c, double *out_dev) {
     k_diag_final<<<1, 32, 0, c.stream>>>(part, nb, out_dev);
     EXG_CUDA_OK(cudaGetLastError());
 }
+
+// ---- host transfers of particle fields (through the device staging buffer)
+void EXG_SFX(h2d_field)(Ctx &c, void *dst, const double *host, long long n, double sub) {
+    using R = EXG_R;
+    if (n == 0) return;
+    if (sizeof(R) == 8 && sub == 0.0) {
+        EXG_CUDA_OK(cudaMemcpyAsync(dst, host, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+        return;
+    }
+    EXG_CUDA_OK(cudaMemcpyAsync(c.stage, host, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+    k_from_f64<R><<<nblocks(n), kThreads, 0, c.stream>>>(c.stage, reinterpret_cast<R *>(dst), n, sub);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+void EXG_SFX(d2h_field)(Ctx &c, const void *src, const int32_t *pid, double *host, long long n, double add) {
+    using R = EXG_R;
+    if (n == 0) return;
+    k_to_f64_unperm<R><<<nblocks(n), kThreads, 0, c.stream>>>(reinterpret_cast<const R *>(src), pid, c.stage, n, add);
+    EXG_CUDA_OK(cudaGetLastError());
+    EXG_CUDA_OK(cudaMemcpyAsync(host, c.stage, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+}
+#if defined(EXG_R_FP64)
+void d2h_positions(Ctx &c, double *const x[3], const int32_t *pid, double *host, long long n) {
+    for (int d = 0; d < 3; ++d) {
+        k_to_f64_unperm<double><<<nblocks(n), kThreads, 0, c.stream>>>(x[d], pid, c.stage, n, 0.0);
+        EXG_CUDA_OK(cudaGetLastError());
+        EXG_CUDA_OK(cudaMemcpyAsync(host + (size_t)d * n, c.stage, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                    c.stream));
+    }
+}
+void d2h_int(Ctx &c, const void *src, int bytes, const int32_t *pid, int32_t *host, long long n) {
+    int32_t *st = reinterpret_cast<int32_t *>(c.stage);
+    if (bytes == 1)
+        k_unperm_i32<uint8_t><<<nblocks(n), kThreads, 0, c.stream>>>(reinterpret_cast<const uint8_t *>(src), pid, st, n);
+    else
+        k_unperm_i32<int32_t><<<nblocks(n), kThreads, 0, c.stream>>>(reinterpret_cast<const int32_t *>(src), pid, st, n);
+    EXG_CUDA_OK(cudaGetLastError());
+    EXG_CUDA_OK(cudaMemcpyAsync(host, st, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c.stream));
+}
+#endif
 
 // ---- batched scenes
 template <class R>

@@ -120,7 +120,8 @@ EXPORTED = [
     "exg_store_delta_temperature", "exg_g2p_temperature", "exg_step", "exg_get_time", "exg_set_time",
     "exg_diagnostics", "exg_sort_keys", "exg_tile_size", "exg_set_stage_timing", "exg_last_step_timing",
     "exg_get_stream", "exg_p2g_momentum_noalloc", "exg_batch_create", "exg_batch_destroy", "exg_batch_scene",
-    "exg_batch_num_scenes", "exg_batch_step", "exg_batch_last_error",
+    "exg_batch_num_scenes", "exg_batch_step", "exg_batch_last_error", "exg_particles_alloc_pinned",
+    "exg_particles_free_pinned",
 ]
 
 _lib = None
@@ -147,6 +148,8 @@ def lib() -> C.CDLL:
         "exg_particles_read_ascii": (i, [C.c_char_p, i, C.POINTER(ParticleSoA)]),
         "exg_particles_alloc": (i, [i64, C.POINTER(ParticleSoA)]),
         "exg_particles_free": (None, [C.POINTER(ParticleSoA)]),
+        "exg_particles_alloc_pinned": (i, [i64, C.POINTER(ParticleSoA)]),
+        "exg_particles_free_pinned": (None, [C.POINTER(ParticleSoA)]),
         "exg_ctx_create": (i, [C.POINTER(Specs), i, C.POINTER(vp)]),
         "exg_ctx_destroy": (i, [vp]),
         "exg_last_error": (C.c_char_p, [vp]),
@@ -205,12 +208,42 @@ def dptr(a: np.ndarray):
 
 
 class Particles:
-    """Host particle set in the reference's field layout (FP64 SoA)."""
+    """Host particle set in the reference's field layout (FP64 SoA).  With
+    pinned=True the arrays live in page-locked memory from
+    exg_particles_alloc_pinned (full-speed host transfers; needs a GPU)."""
 
-    def __init__(self, np_: int):
+    def __init__(self, np_: int, pinned: bool = False):
+        self._soa = None
+        if pinned:
+            s = ParticleSoA()
+            rc = lib().exg_particles_alloc_pinned(np_, C.byref(s))
+            if rc:
+                raise ExgError(rc, "exg_particles_alloc_pinned")
+            self._soa = s
+            self.pos = np.ctypeslib.as_array(s.pos, shape=(3 * max(np_, 1),))[:3 * np_].reshape(3, np_)
+            self.rdata = np.ctypeslib.as_array(s.rdata, shape=(EXG_NREAL * max(np_, 1),))[:EXG_NREAL * np_].reshape(
+                EXG_NREAL, np_)
+            self.idata = np.ctypeslib.as_array(s.idata, shape=(EXG_NINT * max(np_, 1),))[:EXG_NINT * np_].reshape(
+                EXG_NINT, np_)
+            return
         self.pos = np.zeros((3, np_), dtype=np.float64)
         self.rdata = np.zeros((EXG_NREAL, np_), dtype=np.float64)
         self.idata = np.zeros((EXG_NINT, np_), dtype=np.int32)
+
+    def __del__(self):
+        if getattr(self, "_soa", None) is not None:
+            try:
+                lib().exg_particles_free_pinned(C.byref(self._soa))
+            except Exception:
+                pass
+            self._soa = None
+
+    def pinned_copy(self) -> "Particles":
+        p = Particles(self.n, pinned=True)
+        p.pos[:] = self.pos
+        p.rdata[:] = self.rdata
+        p.idata[:] = self.idata
+        return p
 
     @property
     def n(self) -> int:
@@ -332,9 +365,13 @@ class Context:
 
     def download(self) -> Particles:
         p = Particles(self.n)
+        self.download_into(p)
+        return p
+
+    def download_into(self, p: Particles):
+        """Download into an existing set of this context's size (pinned or not)."""
         s = p.soa()
         self._ck(self.L.exg_particles_download(self.h, C.byref(s)), "exg_particles_download")
-        return p
 
     def nodes(self, comp: int) -> np.ndarray:
         nn = [self.specs.ncells[d] + 1 for d in range(3)]

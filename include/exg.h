@@ -201,6 +201,11 @@ int exg_levelset_build(const exg_inputs *in, const exg_specs *specs, int body, d
 int exg_particles_read_ascii(const char *path, int use_temp, exg_particle_soa *out);
 int exg_particles_alloc(int64_t np, exg_particle_soa *out);
 void exg_particles_free(exg_particle_soa *p);
+/* The same arrays in page-locked host memory (cudaMallocHost): uploads and
+ * downloads from them run at full PCIe speed.  Release with
+ * exg_particles_free_pinned. */
+int exg_particles_alloc_pinned(int64_t np, exg_particle_soa *out);
+void exg_particles_free_pinned(exg_particle_soa *p);
 
 /* ------------------------------------------------------------- context */
 typedef struct exg_ctx exg_ctx;
