@@ -685,16 +685,31 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
             last_id = it->second;
         }
         if (c.mats.empty()) c.mats.push_back(Material{});
-        if (c.mat_dev) cudaFree(c.mat_dev);
-        c.mat_dev = dalloc<Material>(c.mats.size());
+        if (!c.mat_dev || c.mat_cap < c.mats.size()) {
+            if (c.mat_dev) cudaFree(c.mat_dev);
+            c.mat_dev = dalloc<Material>(c.mats.size());
+            c.mat_cap = c.mats.size();
+            drop_graphs(c);  // the step graphs hold the table's address
+        }
         EXG_CUDA_OK(cudaMemcpy(c.mat_dev, c.mats.data(), sizeof(Material) * c.mats.size(), cudaMemcpyHostToDevice));
-        // particle storage (re-allocated on every upload)
+        const bool temp = c.specs.use_temp != 0;
+        if (c.pa && n == c.np && n == c.cap) {
+            // same particle count: the storage, sort buffers and step graphs stay
+            if (fp64(c))
+                upload_parts<double>(c, p, mat);
+            else
+                upload_parts<float>(c, p, mat);
+            c.parts_sorted = false;
+            c.reduce_stale = true;
+            sync(c);
+            return EXG_OK;
+        }
+        // particle storage (re-allocated when the count changes)
         free_list(c.allocs_a);
         free_list(c.allocs_b);
         drop_graphs(c);
         if (c.orient) std::swap(c.pa, c.pb);
         c.orient = 0;
-        const bool temp = c.specs.use_temp != 0;
         if (c.stage_cap < n) {  // one FP64 field for the host transfers
             cudaFree(c.stage);
             c.stage = dalloc<double>(n > 0 ? n : 1);

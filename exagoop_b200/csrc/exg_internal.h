@@ -123,6 +123,7 @@ struct Ctx {
     std::vector<void *> allocs_a, allocs_b;
     // material table
     Material *mat_dev = nullptr;
+    size_t mat_cap = 0;
     std::vector<Material> mats;
     // nodes
     void *nodes = nullptr;             // Nodes<R> host copy (device pointers)

@@ -283,3 +283,34 @@ def test_mixed_precision_error_fluid():
     e = mixed_vs_oracle(s, p, 100)
     assert e["vel"] < 1e-3 and e["stress"] < 1e-3, e
     assert e["jacobian"] < 1e-6, e
+
+
+def test_reupload_same_size_reuses_storage():
+    # a second upload of the same particle count keeps storage and step
+    # graphs; the steps that follow match a fresh context bit for bit
+    s, p = small_dam(seed=21)
+    a = nt.Context(s)
+    a.upload(p)
+    a.Initialise_Internal_Forces()
+    a.step(7)
+    a.upload(p)
+    a.Initialise_Internal_Forces()
+    a.step(5)
+    b = nt.Context(s)
+    b.upload(p)
+    b.Initialise_Internal_Forces()
+    b.step(5)
+    pa, pb = a.download(), b.download()
+    assert np.array_equal(pa.rdata, pb.rdata) and np.array_equal(pa.pos, pb.pos)
+
+
+def test_pinned_particle_sets_round_trip():
+    s, p = small_dam(seed=22)
+    hp = p.pinned_copy()
+    ctx = nt.Context(s)
+    ctx.upload(hp)
+    q = nt.Particles(p.n, pinned=True)
+    ctx.download_into(q)
+    assert np.array_equal(q.pos, p.pos)
+    for f in (nt.R_VEL, nt.R_MASS, nt.R_DENSITY):
+        assert np.allclose(q.rdata[f], p.rdata[f], rtol=0, atol=0)
