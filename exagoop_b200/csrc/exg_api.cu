@@ -113,6 +113,7 @@ void build_params_for(const exg_specs &s, Params &P) {
         o.T_inf = e.T_inf;
     }
     P.use_temp = s.use_temp;
+    P.delta_strain = s.calculate_strain_based_on_delta == 1;
     for (int d = 0; d < 3; ++d) {
         P.bclo_temp[d] = s.bclo_temp[d];
         P.bchi_temp[d] = s.bchi_temp[d];
@@ -159,7 +160,6 @@ std::string validate(const exg_specs &s) {
     for (int d = 0; d < 3; ++d)
         if (s.periodic[d] && (s.ncells[d] % T != 0 || s.ncells[d] < 3 * T))
             return "periodic axes need ncells to be a multiple of the tile edge and at least three tiles";
-    if (s.calculate_strain_based_on_delta) return "calculate_strain_based_on_delta = 1 is outside this library's scope";
     if (s.num_bodies < 0 || s.num_bodies > EXG_MAX_BODIES) return "too many level-set bodies";
     return "";
 }
@@ -669,9 +669,13 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
                 continue;
             }
             const int model = std::get<5>(key);
-            if (model != 0 && model != 1)
-                return fail(ctx, EXG_ERR_UNSUPPORTED, "constitutive model " + std::to_string(model) +
-                                                          " (neo-Hookean) is outside this library's scope");
+            if (model < 0 || model > 2)
+                return fail(ctx, EXG_ERR_UNSUPPORTED, "unknown constitutive model " + std::to_string(model));
+            if (model != 0 && c.specs.calculate_strain_based_on_delta == 1)
+                // apply_constitutive_model_delta aborts on these models
+                // (mpm_particle_container.cpp:251-262)
+                return fail(ctx, EXG_ERR_UNSUPPORTED, "calculate_strain_based_on_delta = 1 supports the "
+                                                      "linear-elastic model only");
             auto it = idx.find(key);
             if (it == idx.end()) {
                 Material m;
@@ -962,7 +966,7 @@ int exg_init_internal_forces(exg_ctx *ctx) {
     // apply_constitutive_model(dt = 0, applied_strainrate) (mpm_init.cpp:398)
     EXG_TRY(ctx, {
         if (c.np)
-            fp64(c) ? launch_stress_fp64(c, -INFINITY, 0.0) : launch_stress_fp32(c, -INFINITY, 0.0);
+            fp64(c) ? launch_stress_fp64(c, -INFINITY, 0.0, true) : launch_stress_fp32(c, -INFINITY, 0.0, true);
         c.reduce_stale = true;
         sync(c);
     });

@@ -76,7 +76,7 @@ void launch_node_reset(Ctx &c);
     void launch_node_bcs##sfx(Ctx &c);                                           \
     void launch_move##sfx(Ctx &c, double dt);                                    \
     void launch_volume##sfx(Ctx &c);                                             \
-    void launch_stress##sfx(Ctx &c, double time, double dt);                     \
+    void launch_stress##sfx(Ctx &c, double time, double dt, bool total = false);  \
     void launch_diag##sfx(Ctx &c, double *out_dev);                              \
     void launch_temp_node_op##sfx(Ctx &c, int op, double dt);                     \
     void launch_temp_bcs##sfx(Ctx &c, int walls_mask, int udf, int ls, int dirichlet_only); \

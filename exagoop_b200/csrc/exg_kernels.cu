@@ -1657,13 +1657,44 @@ __device__ __forceinline__ void volume_stress(const Params &P, const Material &m
         eps[0] += (R)(dt * asr);
         eps[3] += (R)(dt * asr);
         eps[5] += (R)(dt * asr);
-        if (mt.model == 0) {
+        if (P.delta_strain) {
+            // apply_constitutive_model_delta (mpm_particle_container.cpp:178-272):
+            // sigma += C : (dt D + applied strain-rate increment), linear elastic
+            if (mt.model == 0) {
+                R de[6], ds[6];
+#pragma unroll
+                for (int d = 0; d < 6; ++d) de[d] = (R)dt * sr[d];
+                de[0] += (R)(dt * asr);
+                de[3] += (R)(dt * asr);
+                de[5] += (R)(dt * asr);
+                linear_elastic<R>(de, ds, (R)mt.E, (R)mt.nu);
+#pragma unroll
+                for (int d = 0; d < 6; ++d) sig[d] += ds[d];
+            }
+        } else if (mt.model == 0) {
             linear_elastic<R>(eps, sig, (R)mt.E, (R)mt.nu);
         } else if (mt.model == 1) {
             // Tait EOS p = K ((1/J)^gamma - 1) (mpm_particle_container.cpp:113-120), FP64
             const double pj = mt.K * (pow(1.0 / det, mt.gamma) - 1.0);
             pres = (R)pj;
             newtonian<R>(sr, sig, (R)mt.mu, (R)pj);
+        } else {
+            // neo-Hookean (constitutive_models.H:161-250), FP64 from E = F - I:
+            // b - I = E + E^T + E E^T, J = max(det F, 1e-12)
+            const double mu = mt.E / (2.0 * (1.0 + mt.nu));
+            const double lambda = mt.E * mt.nu / ((1.0 + mt.nu) * (1.0 - 2.0 * mt.nu));
+            const double Jc = fmax(det, 1.e-12);
+            const double vol = lambda * log(Jc) / Jc, muJ = mu / Jc;
+            auto bm = [&](int i, int j) {
+                return e[3 * i + j] + e[3 * j + i] +
+                       (e[3 * i] * e[3 * j] + e[3 * i + 1] * e[3 * j + 1] + e[3 * i + 2] * e[3 * j + 2]);
+            };
+            sig[0] = (R)(muJ * bm(0, 0) + vol);
+            sig[1] = (R)(muJ * bm(0, 1));
+            sig[2] = (R)(muJ * bm(0, 2));
+            sig[3] = (R)(muJ * bm(1, 1) + vol);
+            sig[4] = (R)(muJ * bm(1, 2));
+            sig[5] = (R)(muJ * bm(2, 2) + vol);
         }
     }
 }
@@ -1750,6 +1781,10 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
             vol = A.vol[p];
             rho = A.rho[p];
             J = A.J[p];
+        } else if (P.delta_strain) {
+            // the incremental formulation adds to the stored stress
+#pragma unroll
+            for (int c = 0; c < 6; ++c) sig[c] = A.sig[c][p];
         }
         const R mass = A.mass[p], vol0 = A.vol0[p];
         const int mi = A.mat[p];
@@ -2029,7 +2064,7 @@ __global__ void k_vol_stress(Params P, Parts<R> A, const Material *mats, long lo
     }
     R vol = A.vol[p], rho = A.rho[p], J = A.J[p], pres = A.pres[p];
     const Material mt = mats[A.mat[p]];
-    if (do_stress && mt.model != 0 && mt.model != 1) return;
+    if (do_stress && (mt.model < 0 || mt.model > 2)) return;
     volume_stress<R>(P, mt, E, A.vol0[p], A.mass[p], sr, eps, sig, vol, rho, J, pres, dt, asr, do_volume != 0,
                      do_stress != 0);
     if (do_volume) {
@@ -2947,10 +2982,12 @@ void EXG_SFX(launch_volume)(Ctx &c) {
     k_vol_stress<EXG_R><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<EXG_R>(), c.mat_dev, c.np, 0.0, 0.0, 1, 0);
     EXG_CUDA_OK(cudaGetLastError());
 }
-void EXG_SFX(launch_stress)(Ctx &c, double time, double dt) {
+void EXG_SFX(launch_stress)(Ctx &c, double time, double dt, bool total) {
     if (c.np == 0) return;
     double asr = (time < c.P.applied_sr_time) ? c.P.applied_sr : 0.0;
-    k_vol_stress<EXG_R><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<EXG_R>(), c.mat_dev, c.np, dt, asr, 0, 1);
+    Params P = c.P;
+    if (total) P.delta_strain = 0;  // Initialise_Internal_Forces: total formulation
+    k_vol_stress<EXG_R><<<nblocks(c.np), kThreads, 0, c.stream>>>(P, c.A<EXG_R>(), c.mat_dev, c.np, dt, asr, 0, 1);
     EXG_CUDA_OK(cudaGetLastError());
 }
 void EXG_SFX(launch_diag)(Ctx &c, double *out_dev) {

@@ -47,7 +47,7 @@ def make_particles(pos: np.ndarray, dx, ppc, density, model: int, E=0.0, nu=0.0,
         p.rdata[nt.R_DEFGRAD + 4 * d] = 1.0
     p.idata[nt.I_MODEL] = model
     p.idata[nt.I_RIGID_ID] = -1
-    if model == 0:
+    if model in (0, 2):  # linear elastic, neo-Hookean
         p.rdata[nt.R_E] = E
         p.rdata[nt.R_NU] = nu
     else:
@@ -119,7 +119,7 @@ def dam_break(n=(256, 128, 128), size=(1.0, 0.5, 0.5), block=(0.4, 0.5, 0.3), se
     return s, p
 
 
-def sphere_collision(n=256, radius=0.2, precision=nt.PREC_FP64, order=3, speed=0.1):
+def sphere_collision(n=256, radius=0.2, precision=nt.PREC_FP64, order=3, speed=0.1, model=0):
     """Two linear-elastic spheres (E = 1e3, nu = 0.3, rho = 1000) of radius
     0.2 centred at (0.3,0.5,0.5) and (0.7,0.5,0.5) moving at +-0.1 m/s in x,
     in a unit cube on an n^3 grid, 2x2x2 lattice; cubic B-splines."""
@@ -133,7 +133,7 @@ def sphere_collision(n=256, radius=0.2, precision=nt.PREC_FP64, order=3, speed=0
     in2 = ((pos - c2) ** 2).sum(0) < radius ** 2
     sel = in1 | in2
     pos = np.ascontiguousarray(pos[:, sel])
-    p = make_particles(pos, (dx, dx, dx), (2, 2, 2), 1000.0, 0, E=1e3, nu=0.3)
+    p = make_particles(pos, (dx, dx, dx), (2, 2, 2), 1000.0, model, E=1e3, nu=0.3)
     p.rdata[nt.R_VEL] = np.where(in1[sel], speed, -speed)
     return s, p
 

@@ -395,6 +395,27 @@ void linear_elastic(const double eps[6], double sig[6], double E, double v) {  /
     sig[XZ] = const2 * eps[XZ];
     sig[YZ] = const2 * eps[YZ];
 }
+// Compressible neo-Hookean solid, constitutive_models.H:161-250 (3-D):
+// b = F F^T, J = max(det F, 1e-12), sigma = (mu/J)(b - I) + (lambda ln J / J) I
+// with the Lame constants of E and nu.
+void neo_hookean(const double F[9], double sig[6], double E, double v) {
+    const double mu = E / (2.0 * (1.0 + v));
+    const double lambda = E * v / ((1.0 + v) * (1.0 - 2.0 * v));
+    auto row = [&](int i, int j) { return F[3 * i] * F[3 * j] + F[3 * i + 1] * F[3 * j + 1] + F[3 * i + 2] * F[3 * j + 2]; };
+    const double bxx = row(0, 0), byy = row(1, 1), bxy = row(0, 1), bzz = row(2, 2), bxz = row(0, 2), byz = row(1, 2);
+    double detF = F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) +
+                  F[2] * (F[3] * F[7] - F[4] * F[6]);
+    detF = std::max(detF, 1.e-12);
+    const double vol = lambda * std::log(detF) / detF;
+    const double muJ = mu / detF;
+    sig[XX] = muJ * (bxx - 1.0) + vol;
+    sig[YY] = muJ * (byy - 1.0) + vol;
+    sig[ZZ] = muJ * (bzz - 1.0) + vol;
+    sig[XY] = muJ * bxy;
+    sig[XZ] = muJ * bxz;
+    sig[YZ] = muJ * byz;
+}
+
 void newtonian_fluid(const double ed[6], double sig[6], double mu, double p) {  // constitutive_models.H:118-159
     double tr = ed[XX] + ed[YY] + ed[ZZ];
     double o3 = 1.0 / 3.0;
@@ -899,10 +920,13 @@ void orc_update_mp_volume(orc_ctx *o) {
 }
 
 // Calculate_MP_Stress_Strain (utilities.cpp:372-400) ->
-// apply_constitutive_model (mpm_particle_container.cpp:43-142).  The delta
-// formulation and the neo-Hookean model are outside this library's scope.
-void orc_calculate_mp_stress_strain(orc_ctx *o, double time, double dt) {
+// apply_constitutive_model (mpm_particle_container.cpp:43-142), or with
+// calculate_strain_based_on_delta = 1 apply_constitutive_model_delta
+// (:178-272): sigma += C : (dt D + applied), linear elastic only (the
+// reference aborts on the other models there).
+static void stress_strain(orc_ctx *o, double time, double dt, bool total) {
     double asr = (time < o->s.applied_strainrate_time) ? o->s.applied_strainrate : 0.0;
+    const bool delta = !total && o->s.calculate_strain_based_on_delta == 1;
     for_particles(o, [&](int64_t p) {
         if (!o->alive(p) || o->idat[EXG_I_PHASE][p] != 0) return;
         for (int d = 0; d < 6; ++d) o->R(EXG_R_STRAIN + d, p) += dt * o->R(EXG_R_STRAINRATE + d, p);
@@ -915,6 +939,17 @@ void orc_calculate_mp_stress_strain(orc_ctx *o, double time, double dt) {
             eps[d] = o->R(EXG_R_STRAIN + d, p);
         }
         int model = o->idat[EXG_I_MODEL][p];
+        if (delta) {
+            if (model != 0) return;
+            double deps[6], dsig[6];
+            for (int d = 0; d < 6; ++d) deps[d] = dt * sr[d];
+            deps[XX] += dt * asr;
+            deps[YY] += dt * asr;
+            deps[ZZ] += dt * asr;
+            linear_elastic(deps, dsig, o->R(EXG_R_E, p), o->R(EXG_R_NU, p));  // linear_elastic_delta: same operator
+            for (int d = 0; d < 6; ++d) o->R(EXG_R_STRESS + d, p) += dsig[d];
+            return;
+        }
         if (model == 0) {
             linear_elastic(eps, sig, o->R(EXG_R_E, p), o->R(EXG_R_NU, p));
         } else if (model == 1) {
@@ -922,12 +957,17 @@ void orc_calculate_mp_stress_strain(orc_ctx *o, double time, double dt) {
             o->R(EXG_R_PRESSURE, p) =
                 o->R(EXG_R_BULK, p) * (std::pow(1.0 / o->R(EXG_R_JACOBIAN, p), o->R(EXG_R_GAMMA, p)) - 1.0) + p_inf;
             newtonian_fluid(sr, sig, o->R(EXG_R_VISC, p), o->R(EXG_R_PRESSURE, p));
+        } else if (model == 2) {
+            double F[9];
+            for (int q = 0; q < 9; ++q) F[q] = o->R(EXG_R_DEFGRAD + q, p);
+            neo_hookean(F, sig, o->R(EXG_R_E, p), o->R(EXG_R_NU, p));
         } else {
             return;
         }
         for (int d = 0; d < 6; ++d) o->R(EXG_R_STRESS + d, p) = sig[d];
     });
 }
+void orc_calculate_mp_stress_strain(orc_ctx *o, double time, double dt) { stress_strain(o, time, dt, false); }
 
 // Calculate_time_step, mpm_particle_timestep.cpp:38-111.
 double orc_calculate_time_step(orc_ctx *o) {
@@ -1232,8 +1272,9 @@ void orc_init_internal_forces(orc_ctx *o) {
     orc_p2g_momentum(o, 1, 1, 1);
     orc_backup_current_velocity(o);
     orc_g2p_momentum(o, 0, 1, 0.0);
-    // apply_constitutive_model(dt = 0, applied_strainrate) (:398)
-    orc_calculate_mp_stress_strain(o, -std::numeric_limits<double>::infinity(), 0.0);
+    // apply_constitutive_model(dt = 0, applied_strainrate) (:398): always
+    // the total formulation
+    stress_strain(o, -std::numeric_limits<double>::infinity(), 0.0, true);
     if (o->s.use_temp) {
         orc_p2g_temperature(o, 1, 1, 0);
         orc_backup_current_temperature(o);
@@ -1401,6 +1442,7 @@ int orc_fn_applybc(const double *in, double *out, double mu, const double *n, in
 }
 void orc_fn_linear_elastic(const double *eps, double *sig, double E, double nu) { linear_elastic(eps, sig, E, nu); }
 void orc_fn_newtonian(const double *ed, double *sig, double mu, double p) { newtonian_fluid(ed, sig, mu, p); }
+void orc_fn_neo_hookean(const double *F, double *sig, double E, double nu) { neo_hookean(F, sig, E, nu); }
 void orc_fn_defgrad(double *F, const double *g, double dt) {
     double gv[3][3];
     for (int a = 0; a < 3; ++a)

@@ -61,6 +61,7 @@ def lib():
         "orc_fn_applybc": (i, [pd, pd, d, pd, i]),
         "orc_fn_linear_elastic": (None, [pd, pd, d, d]),
         "orc_fn_newtonian": (None, [pd, pd, d, d]),
+        "orc_fn_neo_hookean": (None, [pd, pd, d, d]),
         "orc_fn_defgrad": (None, [pd, pd, d]),
         "orc_fn_levelset": (d, [vp, i, pd, pd]),
         "orc_fn_compute_bounds": (None, [i, i, i, i, i, pi, pi]),

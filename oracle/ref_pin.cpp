@@ -77,6 +77,16 @@ void ref_linear_elastic(const double *eps, double *sig, double E, double nu) {
     for (int i = 0; i < 6; ++i) e[i] = eps[i];
     linear_elastic(e, sig, E, nu);
 }
+void ref_neo_hookean(const double *F, double *sig, double E, double nu) {
+    double f[9];
+    for (int i = 0; i < 9; ++i) f[i] = F[i];
+    neo_hookean(sig, f, E, nu);
+}
+void ref_linear_elastic_delta(const double *deps, double *dsig, double E, double nu) {
+    double e[6];
+    for (int i = 0; i < 6; ++i) e[i] = deps[i];
+    linear_elastic_delta(e, dsig, E, nu);
+}
 void ref_newtonian(const double *ed, double *sig, double mu, double p) {
     double e[6];
     for (int i = 0; i < 6; ++i) e[i] = ed[i];

@@ -44,6 +44,8 @@ def load():
     L.ref_applybc.argtypes = [pd, pd, C.c_double, pd, C.c_int]
     L.ref_linear_elastic.argtypes = [pd, pd, C.c_double, C.c_double]
     L.ref_newtonian.argtypes = [pd, pd, C.c_double, C.c_double]
+    L.ref_neo_hookean.argtypes = [pd, pd, C.c_double, C.c_double]
+    L.ref_linear_elastic_delta.argtypes = [pd, pd, C.c_double, C.c_double]
     L.ref_defgrad_update.argtypes = [pd, pd, C.c_double]
     L.ref_levelset.restype = C.c_double
     L.ref_levelset.argtypes = [pd, pi, pi, pd, pd, pd, pd]
@@ -169,6 +171,22 @@ def main():
         L.ref_defgrad_update(P(F2), P(g), dt)
         rows.append(np.concatenate([eps, [E, nu], s1, [mu, p], s2, F, g, [dt], F2]))
     np.savez_compressed(OUT / "constitutive.npz", rows=np.array(rows))
+
+    # neo-Hookean stress (constitutive_models.H:161-250) from F, and the
+    # incremental linear-elastic operator (:69-104)
+    rng2 = np.random.default_rng(20261204)
+    rows = []
+    for i in range(400):
+        scale = 1e-2 if i < 300 else 0.3  # small and large deformations
+        F = np.eye(3).ravel() + rng2.normal(0, scale, 9)
+        E, nu = rng2.uniform(1e2, 1e9), rng2.uniform(0, 0.49)
+        s = np.zeros(6)
+        L.ref_neo_hookean(P(F), P(s), E, nu)
+        deps = rng2.normal(0, 1e-4, 6)
+        ds = np.zeros(6)
+        L.ref_linear_elastic_delta(P(deps), P(ds), E, nu)
+        rows.append(np.concatenate([F, [E, nu], s, deps, ds]))
+    np.savez_compressed(OUT / "neo_hookean.npz", rows=np.array(rows))
 
     # level-set sampling (mpm_eb.H:176-288) on a node array with one ghost layer
     nc = np.array([10, 8, 9], dtype=np.int32)

@@ -314,3 +314,55 @@ def test_pinned_particle_sets_round_trip():
     assert np.array_equal(q.pos, p.pos)
     for f in (nt.R_VEL, nt.R_MASS, nt.R_DENSITY):
         assert np.allclose(q.rdata[f], p.rdata[f], rtol=0, atol=0)
+
+
+def test_fused_neo_hookean_spheres():
+    # constitutive model 2 (constitutive_models.H:161-250) at 4x the speed
+    # of the elastic spheres, so the collision strains are not small
+    s, p = scenes.sphere_collision(n=32, model=2, speed=0.4)
+    ctx, o = run_both(s, p, 30)
+    check_particles(ctx.download(), o.download())
+
+
+def test_neo_hookean_step_functions():
+    s, p = random_scene(61, order=2)
+    p.idata[nt.I_MODEL] = 2
+    p.rdata[nt.R_E], p.rdata[nt.R_NU] = 2e3, 0.25
+    rng = np.random.default_rng(3)
+    p.rdata[nt.R_DEFGRAD:nt.R_DEFGRAD + 9] += rng.normal(0, 0.05, (9, p.n))
+    ctx, o = pair(s, p)
+    dt = 2e-4
+    ctx.P2G_Momentum(1, 1, 1)
+    ctx.backup_current_velocity()
+    ctx.Nodal_Time_Update_Momentum(dt)
+    ctx.Apply_Nodal_BCs(dt, 0.0)
+    ctx.G2P_Momentum(1, 1, dt)
+    ctx.Update_MP_Volume()
+    ctx.Calculate_MP_Stress_Strain(0.0, dt)
+    o.p2g_momentum(1, 1, 1)
+    o.backup_current_velocity()
+    o.nodal_time_update_momentum(dt)
+    o.apply_nodal_bcs(dt, 0.0)
+    o.g2p_momentum(1, 1, dt)
+    o.update_mp_volume()
+    o.calculate_mp_stress_strain(0.0, dt)
+    check_particles(ctx.download(), o.download())
+
+
+def test_fused_incremental_strain():
+    # calculate_strain_based_on_delta = 1: sigma += C : (dt D), the
+    # initial internal forces still from the total formulation
+    s, p = scenes.sphere_collision(n=32)
+    s.calculate_strain_based_on_delta = 1
+    s.applied_strainrate = 0.01
+    s.applied_strainrate_time = 0.05
+    ctx, o = run_both(s, p, 25)
+    check_particles(ctx.download(), o.download())
+
+
+def test_incremental_strain_rejects_fluid():
+    s, p = small_dam()
+    s.calculate_strain_based_on_delta = 1
+    ctx = nt.Context(s)
+    with pytest.raises(nt.ExgError):
+        ctx.upload(p)

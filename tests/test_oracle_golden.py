@@ -119,6 +119,21 @@ def test_constitutive_and_defgrad_bit_exact():
         assert np.array_equal(f, F2)
 
 
+def test_neo_hookean_and_delta_bit_exact():
+    # neo_hookean (constitutive_models.H:161-250) and linear_elastic_delta
+    # (:69-104) against the reference's own header, small and large strains
+    rows = np.load(G / "neo_hookean.npz")["rows"]
+    L = orc.lib()
+    for r in rows:
+        F, E, nu, s_ref, deps, ds_ref = r[0:9], r[9], r[10], r[11:17], r[17:23], r[23:29]
+        a = np.zeros(6)
+        L.orc_fn_neo_hookean(P(F.copy()), P(a), E, nu)
+        assert np.array_equal(a, s_ref)
+        b = np.zeros(6)
+        L.orc_fn_linear_elastic(P(deps.copy()), P(b), E, nu)  # the delta operator is Hooke's
+        assert np.array_equal(b, ds_ref)
+
+
 def test_levelset_sampling():
     f = np.load(G / "levelset.npz")
     nc, plo, dx, phi, rows = f["nc"], f["plo"], f["dx"], f["phi"], f["rows"]
