@@ -238,7 +238,8 @@ void upload_parts(Ctx &c, const exg_particle_soa *h, const std::vector<int32_t> 
     put_r(P.vol, EXG_R_VOLUME);
     put_r(P.mass, EXG_R_MASS);
     put_r(P.rho, EXG_R_DENSITY);
-    put_r(P.J, EXG_R_JACOBIAN);
+    EXG_CUDA_OK(cudaMemcpyAsync(P.J, h->rdata + (size_t)EXG_R_JACOBIAN * n, sizeof(double) * n,
+                                cudaMemcpyHostToDevice, c.stream));
     put_r(P.pres, EXG_R_PRESSURE);
     put_r(P.vol0, EXG_R_VOL_INIT);
     put_r(P.radius, EXG_R_RADIUS);
@@ -289,7 +290,7 @@ void download_parts(Ctx &c, exg_particle_soa *h) {
     get_r(P.vol, EXG_R_VOLUME);
     get_r(P.mass, EXG_R_MASS);
     get_r(P.rho, EXG_R_DENSITY);
-    get_r(P.J, EXG_R_JACOBIAN);
+    d2h_field_fp64(c, P.J, P.pid, h->rdata + (size_t)EXG_R_JACOBIAN * n, n, 0.0);
     get_r(P.pres, EXG_R_PRESSURE);
     get_r(P.vol0, EXG_R_VOL_INIT);
     get_r(P.radius, EXG_R_RADIUS);

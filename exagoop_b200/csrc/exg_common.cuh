@@ -124,7 +124,8 @@ struct Parts {
     R *v[3], *vp[3];
     R *sr[6], *eps[6], *sig[6];
     R *E[9];
-    R *vol, *mass, *rho, *J, *pres, *vol0, *radius, *yacc;
+    R *vol, *mass, *rho, *pres, *vol0, *radius, *yacc;
+    double *J;        // det F: FP64 in both precisions
     double *T;        // temperature: FP64 in both precisions (per-step increments
                       // are far below FP32 resolution at a few hundred kelvin)
     R *cp, *kc, *q[3], *Q;

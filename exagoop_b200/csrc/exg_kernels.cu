@@ -1302,7 +1302,8 @@ __device__ __forceinline__ void interp_axis(const SplineTables &t, const Params 
 template <class R>
 __device__ __forceinline__ void g2p_finish(const Params &P, bool upd_vel, bool upd_sr, const R vpic[3],
                                            const R dpic[3], const R gv[3][3], R v[3], R vp[3], R E[9], R sr[6],
-                                           double dt) {
+                                           double dt, double &jfac) {
+    jfac = 1.0;
     if (upd_vel) {
         const R a = (R)P.alpha;
         for (int d = 0; d < 3; ++d) {
@@ -1327,6 +1328,13 @@ __device__ __forceinline__ void g2p_finish(const Params &P, bool upd_vel, bool u
                     En[a * 3 + b] = acc;
                 }
             for (int q = 0; q < 9; ++q) E[q] = En[q];
+            // det(I + L dt) in FP64: J = det F follows F' = (I + L dt) F
+            // multiplicatively (kept in FP64 by the mixed-precision path)
+            double a[3][3];
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) a[r][c] = (r == c ? 1.0 : 0.0) + (double)gv[r][c] * dt;
+            jfac = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) - a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                   a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
         }
         int ind = 0;
         for (int d1 = 0; d1 < 3; ++d1)
@@ -1337,7 +1345,7 @@ __device__ __forceinline__ void g2p_finish(const Params &P, bool upd_vel, bool u
 template <class R, int ORD, class NodeAcc>
 __device__ __forceinline__ void g2p_particle_generic(const SplineTables &tab, const Params &P, const NodeAcc &na,
                                              const double x[3], const int iv[3], bool upd_vel, bool upd_sr, R v[3],
-                                             R vp[3], R E[9], R sr[6], double dt) {
+                                             R vp[3], R E[9], R sr[6], double dt, double &jfac) {
     // uniform quadratic: the 3-node window of the nearest-node bin (every
     // node with a non-zero weight), the same bin as the sort key's
     constexpr int W = (ORD == 2) ? 3 : Stc<ORD>::W, LO = Stc<ORD>::LO;
@@ -1408,7 +1416,7 @@ __device__ __forceinline__ void g2p_particle_generic(const SplineTables &tab, co
                     }
         }
     }
-    g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt);
+    g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt, jfac);
 }
 
 // Interpolation over a WN^3 window of the shared-memory node block.  FP32
@@ -1518,7 +1526,7 @@ __device__ __forceinline__ void g2p_window(const SmemNodes<R> &na, const int bas
 template <class R, int ORD>
 __device__ __forceinline__ void g2p_particle_smem(const SplineTables &tab, const Params &P, const SmemNodes<R> &na,
                                                   const double x[3], const int iv[3], bool upd_vel, bool upd_sr,
-                                                  R v[3], R vp[3], R E[9], R sr[6], double dt) {
+                                                  R v[3], R vp[3], R E[9], R sr[6], double dt, double &jfac) {
     R vpic[3] = {R(0), R(0), R(0)}, dpic[3] = {R(0), R(0), R(0)};
     R gv[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
     if constexpr (ORD == 2) {
@@ -1535,7 +1543,7 @@ __device__ __forceinline__ void g2p_particle_smem(const SplineTables &tab, const
         }
         g2p_window<R, 3>(na, base, a[0].w, a[0].dw, a[1].w, a[1].dw, a[2].w, a[2].dw, upd_vel, upd_sr, vpic, dpic,
                          gv);
-        g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt);
+        g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt, jfac);
         return;
     }
     bool inter = (ORD != 0);
@@ -1543,7 +1551,7 @@ __device__ __forceinline__ void g2p_particle_smem(const SplineTables &tab, const
     for (int d = 0; d < 3; ++d)
         inter = inter && ((ORD == 1) || P.periodic[d] || (iv[d] >= 3 && iv[d] <= P.nc[d] - 4));
     if (!inter) {
-        g2p_particle_generic<R, ORD>(tab, P, na, x, iv, upd_vel, upd_sr, v, vp, E, sr, dt);
+        g2p_particle_generic<R, ORD>(tab, P, na, x, iv, upd_vel, upd_sr, v, vp, E, sr, dt, jfac);
         return;
     }
     if (ORD == 1 || ORD == 3) {
@@ -1559,15 +1567,15 @@ __device__ __forceinline__ void g2p_particle_smem(const SplineTables &tab, const
         g2p_window<R, WN>(na, base, a[0].w, a[0].dw, a[1].w, a[1].dw, a[2].w, a[2].dw, upd_vel, upd_sr, vpic, dpic,
                           gv);
     }
-    g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt);
+    g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt, jfac);
 }
 
 // G2P of one particle through any node accessor (the unfused L5 path).
 template <class R, int ORD, class NodeAcc>
 __device__ __forceinline__ void g2p_particle(const SplineTables &tab, const Params &P, const NodeAcc &na,
                                              const double x[3], const int iv[3], bool upd_vel, bool upd_sr, R v[3],
-                                             R vp[3], R E[9], R sr[6], double dt) {
-    g2p_particle_generic<R, ORD>(tab, P, na, x, iv, upd_vel, upd_sr, v, vp, E, sr, dt);
+                                             R vp[3], R E[9], R sr[6], double dt, double &jfac) {
+    g2p_particle_generic<R, ORD>(tab, P, na, x, iv, upd_vel, upd_sr, v, vp, E, sr, dt, jfac);
 }
 
 
@@ -1638,16 +1646,18 @@ __device__ __forceinline__ void move_particle(const Params &P, const NodeBCArgs 
 // J, the Tait pressure and the density division are FP64.
 template <class R>
 __device__ __forceinline__ void volume_stress(const Params &P, const Material &mt, const R E[9], R vol0, R mass,
-                                              const R sr[6], R eps[6], R sig[6], R &vol, R &rho, R &J, R &pres,
+                                              const R sr[6], R eps[6], R sig[6], R &vol, R &rho, double &J, R &pres,
                                               double dt, double asr, bool do_volume, bool do_stress) {
     double e[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) e[q] = (double)E[q];
-    // J = det F in FP64 from F = I + E; the stored J is its rounding
-    const double det = det_IpE(e);
+    // J = det F in FP64: from F = I + E with FP64 state; with FP32 state the
+    // caller's J, which follows F multiplicatively in FP64 (det(I + L dt)
+    // per F update), since det of the FP32 F would carry its rounding
+    const double det = (sizeof(R) == 8) ? det_IpE(e) : J;
     if (do_volume) {
         const double V = (double)vol0 * det;
-        J = (R)det;
+        J = det;
         vol = (R)V;
         rho = (R)((double)mass / V);
     }
@@ -1712,6 +1722,38 @@ __device__ __forceinline__ bool all_finite(const R *a, int n) {
 // permutation and written to storage B at its sorted position, so the
 // particle arrays are physically re-ordered by cell every step at no extra
 // pass.  GM_VEL updates velocity in place in A instead.
+// L2 prefetch of the fields the fused G2P reads for storage index i.  The
+// storage is in the previous step's sorted order, and particles rarely change
+// bins in one step, so storage index k holds (nearly always) the particle of
+// sorted position k: prefetching index k + blockDim.x overlaps the next
+// iteration's loads with this one's arithmetic.
+#ifndef EXG_G2P_PREFETCH
+#define EXG_G2P_PREFETCH 1
+#endif
+template <class R>
+__device__ __forceinline__ void prefetch_particle(const Parts<R> &A, long long i) {
+    auto pf = [](const void *q) { asm volatile("prefetch.global.L2 [%0];" ::"l"(q)); };
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        pf(A.x[d] + i);
+        pf(A.v[d] + i);
+        pf(A.vp[d] + i);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) pf(A.E[q] + i);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) pf(A.eps[c] + i);
+    pf(A.pres + i);
+    pf(A.mass + i);
+    pf(A.vol0 + i);
+    pf(A.mat + i);
+    pf(A.phase + i);
+    pf(A.radius + i);
+    pf(A.yacc + i);
+    pf(A.rigid + i);
+    pf(A.pid + i);
+}
+
 // One tile of the fused G2P: stage the tile's node block (v, dv and halo)
 // in shared memory, then update each of the tile's particles.
 template <class R, int ORD>
@@ -1741,6 +1783,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
     __syncthreads();
     const int s0 = start[t], n = count[t];
     for (int k = s0 + threadIdx.x; k < s0 + n; k += blockDim.x) {
+        if (EXG_G2P_PREFETCH && k + (int)blockDim.x < s0 + n) prefetch_particle<R>(A, k + blockDim.x);
         const int p = perm[k];
         const int phase = A.phase[p];
         double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
@@ -1755,7 +1798,8 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
                 int iv[3];
                 cell_of(P, x, iv);
                 R E[9], sr[6];
-                g2p_particle_smem<R, ORD>(*tab, P, na, x, iv, true, false, v, vp, E, sr, dt);
+                double jf;
+                g2p_particle_smem<R, ORD>(*tab, P, na, x, iv, true, false, v, vp, E, sr, dt, jf);
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     A.v[d][p] = v[d];
@@ -1765,7 +1809,8 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
             continue;
         }
         R E[9], sr[6], eps[6], sig[6];
-        R vol, rho, J, pres;
+        R vol, rho, pres;
+        double J = A.J[p], jf = 1.0;
 #pragma unroll
         for (int q = 0; q < 9; ++q) E[q] = A.E[q][p];
 #pragma unroll
@@ -1780,7 +1825,6 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
             }
             vol = A.vol[p];
             rho = A.rho[p];
-            J = A.J[p];
         } else if (P.delta_strain) {
             // the incremental formulation adds to the stored stress
 #pragma unroll
@@ -1791,7 +1835,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
         if (phase == 0) {
             int iv[3];
             cell_of(P, x, iv);
-            g2p_particle_smem<R, ORD>(*tab, P, na, x, iv, upd_vel, true, v, vp, E, sr, dt);
+            g2p_particle_smem<R, ORD>(*tab, P, na, x, iv, upd_vel, true, v, vp, E, sr, dt, jf);
         }
         move_particle<R>(P, bc, phase, x, v, vp, dt, status);
         // Redistribute's periodic wrap
@@ -1806,6 +1850,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
             }
         const Material mt = mats[mi];
         if (phase == 0) {
+            J *= jf;  // FP32 state: J follows F multiplicatively in FP64
             volume_stress<R>(P, mt, E, vol0, mass, sr, eps, sig, vol, rho, J, pres, dt, asr, true, true);
             if (!all_finite(v, 3) || !all_finite(sig, 6) || !isfinite((double)J)) status |= ST_NAN;
             // reductions for the next step (running per thread)
@@ -2019,7 +2064,9 @@ __global__ void __launch_bounds__(kThreads) k_g2p_simple(Params P, Parts<R> A, N
     }
     for (int q = 0; q < 9; ++q) E[q] = A.E[q][p];
     for (int c = 0; c < 6; ++c) sr[c] = A.sr[c][p];
-    g2p_particle<R, ORD>(tab, P, na, x, iv, upd_vel != 0, upd_sr != 0, v, vp, E, sr, dt);
+    double jf = 1.0;
+    g2p_particle<R, ORD>(tab, P, na, x, iv, upd_vel != 0, upd_sr != 0, v, vp, E, sr, dt, jf);
+    if (sizeof(R) == 4 && upd_sr) A.J[p] *= jf;  // FP32 state: J kept in FP64 alongside F
     if (upd_vel)
         for (int d = 0; d < 3; ++d) {
             A.v[d][p] = v[d];
@@ -2062,7 +2109,8 @@ __global__ void k_vol_stress(Params P, Parts<R> A, const Material *mats, long lo
         eps[c] = A.eps[c][p];
         sig[c] = A.sig[c][p];
     }
-    R vol = A.vol[p], rho = A.rho[p], J = A.J[p], pres = A.pres[p];
+    R vol = A.vol[p], rho = A.rho[p], pres = A.pres[p];
+    double J = A.J[p];
     const Material mt = mats[A.mat[p]];
     if (do_stress && (mt.model < 0 || mt.model > 2)) return;
     volume_stress<R>(P, mt, E, A.vol0[p], A.mass[p], sr, eps, sig, vol, rho, J, pres, dt, asr, do_volume != 0,
