@@ -266,6 +266,23 @@ void upload_parts(Ctx &c, const exg_particle_soa *h, const std::vector<int32_t> 
     EXG_CUDA_OK(cudaStreamSynchronize(c.stream));  // the host vectors above go out of scope
 }
 
+void drop_graphs(Ctx &c);
+
+// FP32 state keeps nodal temperatures relative to the mean particle
+// temperature, so that differences of a few millikelvin on a few hundred
+// kelvin stay resolved; a new reference re-bases the stored nodal values.
+void set_tref(Ctx &c, const exg_particle_soa *h) {
+    if (!c.specs.use_temp || fp64(c)) return;
+    const long long n = h->np;
+    double sum = 0.0;
+    for (long long i = 0; i < n; ++i) sum += h->rdata[(size_t)EXG_R_TEMPERATURE * n + i];
+    const double tref = n ? (double)(float)(sum / n) : 0.0;
+    if (tref == c.P.Tref) return;
+    c.P.Tref = tref;
+    drop_graphs(c);  // the step graphs hold the parameters
+    launch_fill_node_fp32(c, EXG_N_TEMPERATURE, -tref);  // untouched nodes: 0 K
+}
+
 template <class R>
 void download_parts(Ctx &c, exg_particle_soa *h) {
     Parts<R> &P = c.A<R>();
@@ -704,6 +721,7 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
                 upload_parts<double>(c, p, mat);
             else
                 upload_parts<float>(c, p, mat);
+            set_tref(c, p);
             c.parts_sorted = false;
             c.reduce_stale = true;
             sync(c);
@@ -741,6 +759,7 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
             c.np = n;
             upload_parts<float>(c, p, mat);
         }
+        set_tref(c, p);
         c.cap = n;
         cudaFree(c.sb.key);
         cudaFree(c.sb.perm);
@@ -815,6 +834,17 @@ int exg_nodes_download(exg_ctx *ctx, int comp, double *out) {
             std::vector<float> b(n);
             EXG_CUDA_OK(cudaMemcpy(b.data(), c.N<float>().c[comp], sizeof(float) * n, cudaMemcpyDeviceToHost));
             for (long long i = 0; i < n; ++i) out[i] = b[i];
+        }
+        // nodal temperatures are stored relative to Tref (FP32 state)
+        if (c.P.Tref != 0.0 && (comp == EXG_N_TEMPERATURE || comp == EXG_N_MASS_SPHEAT_TEMP)) {
+            std::vector<double> mc;
+            if (comp == EXG_N_MASS_SPHEAT_TEMP) {
+                std::vector<float> b(n);
+                EXG_CUDA_OK(cudaMemcpy(b.data(), c.N<float>().c[EXG_N_MASS_SPHEAT], sizeof(float) * n,
+                                       cudaMemcpyDeviceToHost));
+                mc.assign(b.begin(), b.end());
+            }
+            for (long long i = 0; i < n; ++i) out[i] += c.P.Tref * (comp == EXG_N_TEMPERATURE ? 1.0 : mc[i]);
         }
         // periodic axes: node ncells is node 0
         const int *nn = c.P.nn;

@@ -109,6 +109,9 @@ struct Params {
     Body body[kMaxBodies];
     int use_temp;
     int delta_strain;  // calculate_strain_based_on_delta: incremental linear-elastic stress
+    // nodal temperatures are stored as T - Tref (FP32 state: a reference near
+    // the particles' temperatures keeps their differences resolved; 0 in FP64)
+    double Tref;
     // domain-wall thermal BCs (mpm_specs.H bc_temp_* arrays)
     int bclo_temp[3], bchi_temp[3];
     double Twall_lo[3], Twall_hi[3], qflux_lo[3], qflux_hi[3], hc_lo[3], hc_hi[3], Tinf_lo[3], Tinf_hi[3];

@@ -81,6 +81,7 @@ void launch_node_reset(Ctx &c);
     void launch_temp_node_op##sfx(Ctx &c, int op, double dt);                     \
     void launch_temp_bcs##sfx(Ctx &c, int walls_mask, int udf, int ls, int dirichlet_only); \
     void launch_g2p_temp##sfx(Ctx &c, int upd_T, int upd_q);                     \
+    void launch_fill_node##sfx(Ctx &c, int comp, double value);                   \
     void h2d_field##sfx(Ctx &c, void *dst, const double *host, long long n, double sub); \
     void d2h_field##sfx(Ctx &c, const void *src, const int32_t *pid, double *host, long long n, double add);
 EXG_DECL_PREC(_fp64)

@@ -835,7 +835,7 @@ __device__ __forceinline__ void p2g_tile(const SplineTables *tab, unsigned *acc_
                     for (int c6 = 0; c6 < 6; ++c6) q.s[c6] = -vol * A.sig[c6][p];
                     if constexpr (THERM) {
                         q.mcp = q.m * A.cp[p];
-                        q.mcpT = (R)(q.mcp * A.T[p]);
+                        q.mcpT = (R)(q.mcp * (A.T[p] - P.Tref));
                         q.mk = q.m * A.kc[p];
 #pragma unroll
                         for (int d = 0; d < 3; ++d) q.qv[d] = vol * A.q[d][p];
@@ -1156,7 +1156,7 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
                 Nd.c[EXG_N_SOURCE_TEMP][ni] = (R)((flags & PF_SRC) ? (double)accv[CH_SRC] * isc[CH_SRC] : 0.0);
                 if (fT) {
                     Nd.c[EXG_N_MASS_COND][ni] = (R)((double)accv[CH_MK] * isc[CH_MK]);
-                    if (mc > 0.0) Nd.c[EXG_N_TEMPERATURE][ni] = (R)((mc >= P.mass_tol) ? mct / mc : 0.0);
+                    if (mc > 0.0) Nd.c[EXG_N_TEMPERATURE][ni] = (R)((mc >= P.mass_tol) ? mct / mc : -P.Tref);
                 }
             }
         } else if (mode == NM_FUSED) {
@@ -1189,13 +1189,15 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
                 // that Reset_Nodaldata_to_Zero left at 0
                 const double mc = (double)accv[CH_MC] * isc[CH_MC], mct = (double)accv[CH_MCT] * isc[CH_MCT];
                 const double src = (double)accv[CH_SRC] * isc[CH_SRC];
-                double Tn = 0.0;
-                if (mc > 0.0) Tn = (mc >= P.mass_tol) ? mct / mc : 0.0;
+                // temperatures relative to Tref (0 K is -Tref); DELTA holds 0
+                // where m cp = 0, as the reset leaves it
+                double Tn = -P.Tref;
+                if (mc > 0.0) Tn = (mc >= P.mass_tol) ? mct / mc : -P.Tref;
                 const double Told = (mc > 0.0) ? Tn : 0.0;
                 if (mc >= P.mass_tol)
                     Tn += src / mc * dt;
                 else
-                    Tn = 0.0;
+                    Tn = -P.Tref;
                 Nd.c[EXG_N_MASS_SPHEAT][ni] = (R)mc;
                 Nd.c[EXG_N_MASS_SPHEAT_TEMP][ni] = (R)mct;
                 Nd.c[EXG_N_MASS_COND][ni] = (R)((double)accv[CH_MK] * isc[CH_MK]);
@@ -2145,7 +2147,7 @@ __global__ void k_temp_node_op(Params P, Nodes<R> Nd, int op, double dt) {
             Nd.c[EXG_N_TEMPERATURE][n] =
                 (R)((double)Nd.c[EXG_N_TEMPERATURE][n] + (double)Nd.c[EXG_N_SOURCE_TEMP][n] / mc * dt);
         else
-            Nd.c[EXG_N_TEMPERATURE][n] = R(0);
+            Nd.c[EXG_N_TEMPERATURE][n] = (R)(-P.Tref);
     } else {
         if (mc > 0.0)
             Nd.c[EXG_N_DELTA_TEMPERATURE][n] =
@@ -2170,10 +2172,10 @@ struct TLink {
 template <class R>
 struct TempView {
     const R *T, *mc, *mk, *m;
-    bool mask;  // fused step: nodes below the mass tolerance hold 0 before the pass
-    double mass_tol;
+    bool mask;  // fused step: nodes below the mass tolerance hold 0 K before the pass
+    double mass_tol, Tref;
     __device__ __forceinline__ double pre(long long n) const {
-        if (mask && !((double)mc[n] >= mass_tol)) return 0.0;
+        if (mask && !((double)mc[n] >= mass_tol)) return -Tref;
         return (double)T[n];
     }
     // specific conductance k = (m k) / m, 1 on massless nodes
@@ -2201,12 +2203,12 @@ __device__ __forceinline__ bool temp_wall_link(const Params &P, const int id[3],
         L.kind = (signed char)bc;
         L.a = L.b = 0.0;
         if (bc == EXG_BCT_ISOTHERMAL) {
-            L.a = lo ? P.Twall_lo[d] : P.Twall_hi[d];
+            L.a = (lo ? P.Twall_lo[d] : P.Twall_hi[d]) - P.Tref;
         } else if (bc == EXG_BCT_USERFLUX) {
             L.a = lo ? P.qflux_lo[d] : P.qflux_hi[d];
         } else if (bc == EXG_BCT_CONVECTION) {
             L.a = lo ? P.hc_lo[d] : P.hc_hi[d];
-            L.b = lo ? P.Tinf_lo[d] : P.Tinf_hi[d];
+            L.b = (lo ? P.Tinf_lo[d] : P.Tinf_hi[d]) - P.Tref;
         }
     }
     return any;
@@ -2234,8 +2236,9 @@ __device__ __forceinline__ bool temp_udf_link(const Params &P, const NodeBCArgs 
         L.dir = (signed char)dir;
         L.side = (signed char)side;
         L.kind = (signed char)code;
-        L.a = tab[f];
-        L.b = tab[f + 1];
+        // temperatures (isothermal value, convective T_inf) relative to Tref
+        L.a = tab[f] - (code == EXG_BCT_ISOTHERMAL ? P.Tref : 0.0);
+        L.b = tab[f + 1] - (code == EXG_BCT_CONVECTION ? P.Tref : 0.0);
     }
     return any;
 }
@@ -2365,7 +2368,7 @@ __global__ void k_temp_faces(Params P, Nodes<R> Nd, NodeBCArgs bc, double *out, 
     int id[3];
     if (!face_entry(P, e, id)) return;
     TempView<R> tv{Nd.c[EXG_N_TEMPERATURE], Nd.c[EXG_N_MASS_SPHEAT], Nd.c[EXG_N_MASS_COND], Nd.c[EXG_N_MASS],
-                   mask != 0, P.mass_tol};
+                   mask != 0, P.mass_tol, P.Tref};
     unsigned status = 0;
     out[e] = temp_face_value<R>(P, bc, tv, id, walls != 0, udf != 0, status);
     if (status) atomicOr(&ctl->status, status);
@@ -2402,7 +2405,7 @@ __global__ void k_temp_levelset(Params P, Nodes<R> Nd, const double *phi, int b,
             for (int d = 0; d < 3; ++d) nd[d] /= gm;
             const Body &bd = P.body[b];
             if (bd.temp_bc == 1) {
-                out = (R)bd.T_wall;
+                out = (R)(bd.T_wall - P.Tref);
             } else if (bd.temp_bc == 3 || bd.temp_bc == 4) {
                 int dd = 0;
                 for (int d = 1; d < 3; ++d)
@@ -2412,12 +2415,12 @@ __global__ void k_temp_levelset(Params P, Nodes<R> Nd, const double *phi, int b,
                 const double mm = (double)Nd.c[EXG_N_MASS][n];
                 const double kn = (mm > 0.0) ? (double)Nd.c[EXG_N_MASS_COND][n] / mm : 1.0;
                 const long long q = node_index(P, nb[0], nb[1], nb[2]);
-                const double Tnb = q < 0 ? 0.0 : (double)src[q];  // ghost nodes hold 0
+                const double Tnb = q < 0 ? -P.Tref : (double)src[q];  // ghost nodes hold 0 K
                 if (bd.temp_bc == 3) {
                     out = (R)(Tnb + bd.heat_flux * P.dx[dd] / kn);
                 } else {
                     const double Bi = bd.h_conv * P.dx[dd] / kn;
-                    out = (R)((Tnb + Bi * bd.T_inf) / (1.0 + Bi));
+                    out = (R)((Tnb + Bi * (bd.T_inf - P.Tref)) / (1.0 + Bi));
                 }
             }
         }
@@ -2751,6 +2754,12 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
     if (cur >= 0) flush(descs[cur].ctl);
 }
 
+template <class R>
+__global__ void k_fill(R *a, long long n, double value) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) a[i] = (R)value;
+}
+
 // ---------------------------------------------------------------- host transfers
 // Particle fields cross PCIe as the caller's FP64 arrays; the precision
 // conversion and the return to upload order run here.
@@ -2963,6 +2972,11 @@ void EXG_SFX(launch_g2p_simple)(Ctx &c, int uv, int us, double dt) {
         case 3: k_g2p_simple<R, 3><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, uv, us, dt); break;
         default: k_g2p_simple<R, 0><<<nblocks(c.np), kThreads, 0, c.stream>>>(c.P, c.A<R>(), c.N<R>(), c.np, uv, us, dt); break;
     }
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void EXG_SFX(launch_fill_node)(Ctx &c, int comp, double value) {
+    k_fill<EXG_R><<<nblocks(c.P.nnodes), kThreads, 0, c.stream>>>(c.N<EXG_R>().c[comp], c.P.nnodes, value);
     EXG_CUDA_OK(cudaGetLastError());
 }
 
