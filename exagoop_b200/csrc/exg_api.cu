@@ -7,9 +7,11 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <tuple>
 #include "exg_internal.h"
+#include "exg_levelset.h"
 
 using namespace exg;
 
@@ -650,6 +652,99 @@ int exg_synchronize(exg_ctx *ctx) {
 int exg_check_status(exg_ctx *ctx) {
     if (!ctx) return EXG_ERR_ARG;
     EXG_TRY(ctx, return status_from_ctl(ctx->c));
+}
+
+}  // extern "C"
+
+namespace {
+
+// Level set of one body as the union of analytic shapes, one thread per node
+// (node coordinates plo + i dx as the host builder forms them).
+__global__ void k_levelset_shapes(const exg_ls_shape *shapes, int nshapes, int nx, int ny, int nz, double plo0,
+                                  double plo1, double plo2, double dx0, double dx1, double dx2, double *phi) {
+    const long long nn = (long long)nx * ny * nz;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn;
+         n += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(n % nx), j = (int)((n / nx) % ny), k = (int)(n / ((long long)nx * ny));
+        phi[n] = exg_ls_union_eval(shapes, nshapes, exg_ls_node_x(plo0, i, dx0), exg_ls_node_x(plo1, j, dx1),
+                                   exg_ls_node_x(plo2, k, dx2));
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int exg_levelset_build_device(exg_ctx *ctx, int body, const exg_ls_shape *shapes, int nshapes) {
+    if (!ctx || body < 0 || body >= EXG_MAX_BODIES || !shapes || nshapes < 1) return EXG_ERR_ARG;
+    for (int i = 0; i < nshapes; ++i) {
+        const exg_ls_shape &sh = shapes[i];
+        if (sh.kind < EXG_LS_SPHERE || sh.kind > EXG_LS_BOX) return fail(ctx, EXG_ERR_ARG, "unknown level-set shape");
+        if (sh.kind == EXG_LS_CYLINDER && (sh.dir < 0 || sh.dir > 2))
+            return fail(ctx, EXG_ERR_ARG, "cylinder_direction must be 0, 1 or 2");
+        if (sh.kind == EXG_LS_PLANE && sh.normal[0] == 0.0 && sh.normal[1] == 0.0 && sh.normal[2] == 0.0)
+            return fail(ctx, EXG_ERR_ARG, "plane_normal must not be zero");
+    }
+    Ctx &c = ctx->c;
+    EXG_TRY(ctx, {
+        if (!c.ls[body]) c.ls[body] = dalloc<double>(c.P.nnodes);
+        struct DevFree {
+            void operator()(void *q) const { cudaFree(q); }
+        };
+        std::unique_ptr<exg_ls_shape, DevFree> dsh(dalloc<exg_ls_shape>(nshapes));
+        EXG_CUDA_OK(cudaMemcpyAsync(dsh.get(), shapes, sizeof(exg_ls_shape) * nshapes, cudaMemcpyHostToDevice,
+                                    c.stream));
+        int nn[3];
+        double dx[3];
+        for (int d = 0; d < 3; ++d) {
+            nn[d] = c.specs.ncells[d] + 1;
+            dx[d] = (c.specs.phi[d] - c.specs.plo[d]) / c.specs.ncells[d];
+        }
+        const long long total = (long long)nn[0] * nn[1] * nn[2];
+        const int grid = (int)std::min<long long>((total + 255) / 256, 148LL * 8);
+        k_levelset_shapes<<<grid, 256, 0, c.stream>>>(dsh.get(), nshapes, nn[0], nn[1], nn[2], c.specs.plo[0],
+                                                       c.specs.plo[1], c.specs.plo[2], dx[0], dx[1], dx[2],
+                                                       c.ls[body]);
+        EXG_CUDA_OK(cudaGetLastError());
+        EXG_CUDA_OK(cudaStreamSynchronize(c.stream));
+        drop_graphs(c);
+    });
+    return EXG_OK;
+}
+
+int exg_init_levelsets(exg_ctx *ctx, const exg_inputs *in) {
+    if (!ctx || !in) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    std::vector<double> host;
+    for (int b = 0; b < c.specs.num_bodies; ++b) {
+        exg_ls_shape sh;
+        const int rc = exg_levelset_shape(in, b, &sh);
+        if (rc == EXG_OK) {
+            const int r2 = exg_levelset_build_device(ctx, b, &sh, 1);
+            if (r2 != EXG_OK) return r2;
+        } else if (rc == EXG_ERR_UNSUPPORTED) {
+            // udf_cpp: the user's levelset_phi runs on the host
+            if (host.empty()) host.resize(c.P.nnodes);
+            const int r2 = exg_levelset_build(in, &c.specs, b, host.data());
+            if (r2 != EXG_OK) return fail(ctx, r2, "level set of body " + std::to_string(b) + " cannot be built");
+            const int r3 = exg_set_levelset(ctx, b, host.data());
+            if (r3 != EXG_OK) return r3;
+        } else {
+            return fail(ctx, rc, "level set of body " + std::to_string(b) + " has a bad geometry");
+        }
+    }
+    return EXG_OK;
+}
+
+int exg_get_levelset(exg_ctx *ctx, int body, double *phi) {
+    if (!ctx || body < 0 || body >= EXG_MAX_BODIES || !phi) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (!c.ls[body]) return fail(ctx, EXG_ERR_NOT_READY, "body " + std::to_string(body) + " has no level set");
+    EXG_TRY(ctx, {
+        EXG_CUDA_OK(cudaStreamSynchronize(c.stream));
+        EXG_CUDA_OK(cudaMemcpy(phi, c.ls[body], sizeof(double) * c.P.nnodes, cudaMemcpyDeviceToHost));
+    });
+    return EXG_OK;
 }
 
 int exg_set_levelset(exg_ctx *ctx, int body, const double *phi) {

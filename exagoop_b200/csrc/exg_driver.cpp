@@ -102,12 +102,8 @@ int main(int argc, char **argv) {
     }
     exg_ctx *ctx = nullptr;
     check(exg_ctx_create(&s, 0, &ctx), nullptr, "exg_ctx_create");
-    const size_t nn = (size_t)(s.ncells[0] + 1) * (s.ncells[1] + 1) * (s.ncells[2] + 1);
-    std::vector<double> phi(nn);
-    for (int b = 0; b < s.num_bodies; ++b) {
-        check(exg_levelset_build(in, &s, b, phi.data()), ctx, "exg_levelset_build");
-        check(exg_set_levelset(ctx, b, phi.data()), ctx, "exg_set_levelset");
-    }
+    // level-set bodies (init_eb): analytic shapes on the GPU, UDFs on the host
+    check(exg_init_levelsets(ctx, in), ctx, "exg_init_levelsets");
     check(exg_particles_upload(ctx, &parts), ctx, "exg_particles_upload");
     check(exg_init_internal_forces(ctx), ctx, "exg_init_internal_forces");
 

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/exg.h"
+#include "exg_levelset.h"
 
 struct exg_inputs {
     // key -> list of definitions (each a token list); the last one wins, as
@@ -461,6 +462,53 @@ int exg_specs_from_inputs(const exg_inputs *cin, exg_specs *s, char *errbuf, siz
     return EXG_OK;
 }
 
+// Analytic shape of body b from its <geom>_* keys (build_analytic_levelset,
+// mpm_eb.cpp:150-388); udf_cpp and stl bodies have none.
+int exg_levelset_shape(const exg_inputs *cin, int body, exg_ls_shape *sh) {
+    exg_inputs *in = const_cast<exg_inputs *>(cin);
+    if (!in || !sh || body < 0) return EXG_ERR_ARG;
+    bool legacy = false;
+    std::vector<std::string> bodies = body_prefixes(in, legacy);
+    if (body >= (int)bodies.size()) return EXG_ERR_ARG;
+    Reader r{in, ""};
+    const std::string pre = bodies[body] + ".";
+    std::string g;
+    if (!r.str(pre + "geom_type", g)) return EXG_ERR_CONFIG;
+    *sh = exg_ls_shape{};
+    sh->center[0] = sh->center[1] = sh->center[2] = 0.5;
+    sh->normal[1] = 1.0;
+    sh->radius = 1.0;
+    sh->height = 1.0;
+    sh->dir = 2;
+    if (g == "sphere") {
+        sh->kind = EXG_LS_SPHERE;
+        if (!r.real(pre + "sphere_radius", sh->radius) || !r.reals(pre + "sphere_center", sh->center, 3))
+            return EXG_ERR_CONFIG;
+        r.boolean(pre + "sphere_has_fluid_inside", sh->inside);
+    } else if (g == "plane") {
+        sh->kind = EXG_LS_PLANE;
+        if (!r.reals(pre + "plane_point", sh->center, 3) || !r.reals(pre + "plane_normal", sh->normal, 3))
+            return EXG_ERR_CONFIG;
+        r.boolean(pre + "plane_has_fluid_inside", sh->inside);
+    } else if (g == "cylinder") {
+        sh->kind = EXG_LS_CYLINDER;
+        if (!r.real(pre + "cylinder_radius", sh->radius) || !r.reals(pre + "cylinder_center", sh->center, 3))
+            return EXG_ERR_CONFIG;
+        r.real(pre + "cylinder_height", sh->height);
+        r.integer(pre + "cylinder_direction", sh->dir);
+        if (sh->dir < 0 || sh->dir > 2) return EXG_ERR_CONFIG;
+        r.boolean(pre + "cylinder_has_fluid_inside", sh->inside);
+    } else if (g == "box") {
+        sh->kind = EXG_LS_BOX;
+        if (!r.reals(pre + "box_lo", sh->lo, 3) || !r.reals(pre + "box_hi", sh->hi, 3)) return EXG_ERR_CONFIG;
+        r.boolean(pre + "box_has_fluid_inside", sh->inside);
+    } else {
+        return EXG_ERR_UNSUPPORTED;  // udf_cpp (no analytic form), stl and wedge_hopper (AMReX EB2 only)
+    }
+    if (!r.err.empty()) return EXG_ERR_CONFIG;
+    return EXG_OK;
+}
+
 // Nodal level set of body b: phi < 0 inside the solid.  Analytic shapes are
 // exact signed distances (the reference builds them with AMReX EB2 and
 // FillSignedDistance, whose discrete distance this does not reproduce);
@@ -476,72 +524,30 @@ int exg_levelset_build(const exg_inputs *cin, const exg_specs *s, int body, doub
     const std::string pre = bodies[body] + ".";
     std::string g;
     if (!r.str(pre + "geom_type", g)) return EXG_ERR_CONFIG;
-    int nn[3];
-    double dx[3];
-    for (int d = 0; d < 3; ++d) {
-        nn[d] = s->ncells[d] + 1;
-        dx[d] = (s->phi[d] - s->plo[d]) / s->ncells[d];
-    }
     exg_levelset_udf udf = nullptr;
-    double c[3] = {0.5, 0.5, 0.5}, rad = 1.0, n[3] = {0, 1, 0}, lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, height = 1.0;
-    int dir = 2, inside = 0;
-    if (g == "sphere") {
-        if (!r.real(pre + "sphere_radius", rad) || !r.reals(pre + "sphere_center", c, 3)) return EXG_ERR_CONFIG;
-        r.boolean(pre + "sphere_has_fluid_inside", inside);
-    } else if (g == "plane") {
-        if (!r.reals(pre + "plane_point", c, 3) || !r.reals(pre + "plane_normal", n, 3)) return EXG_ERR_CONFIG;
-        r.boolean(pre + "plane_has_fluid_inside", inside);
-    } else if (g == "cylinder") {
-        if (!r.real(pre + "cylinder_radius", rad) || !r.reals(pre + "cylinder_center", c, 3)) return EXG_ERR_CONFIG;
-        r.real(pre + "cylinder_height", height);
-        r.integer(pre + "cylinder_direction", dir);
-        r.boolean(pre + "cylinder_has_fluid_inside", inside);
-    } else if (g == "box") {
-        if (!r.reals(pre + "box_lo", lo, 3) || !r.reals(pre + "box_hi", hi, 3)) return EXG_ERR_CONFIG;
-        r.boolean(pre + "box_has_fluid_inside", inside);
-    } else if (g == "udf_cpp") {
+    exg_ls_shape sh{};
+    if (g == "udf_cpp") {
         std::string so, e;
         if (!r.str(pre + "udf_so_file", so)) return EXG_ERR_CONFIG;
         void *sym = load_symbol(in, so, "levelset_phi", e);
         if (!sym) return EXG_ERR_IO;
         udf = reinterpret_cast<exg_levelset_udf>(sym);
     } else {
-        return EXG_ERR_UNSUPPORTED;  // stl, wedge_hopper: AMReX EB2 only
+        const int rc = exg_levelset_shape(in, body, &sh);
+        if (rc != EXG_OK) return rc;
     }
-    double nl = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    int nn[3];
+    double dx[3];
+    for (int d = 0; d < 3; ++d) {
+        nn[d] = s->ncells[d] + 1;
+        dx[d] = (s->phi[d] - s->plo[d]) / s->ncells[d];
+    }
     for (int k = 0; k < nn[2]; ++k)
         for (int j = 0; j < nn[1]; ++j)
             for (int i = 0; i < nn[0]; ++i) {
-                double x[3] = {s->plo[0] + i * dx[0], s->plo[1] + j * dx[1], s->plo[2] + k * dx[2]};
-                double v;
-                if (udf) {
-                    v = udf(x[0], x[1], x[2]);
-                } else if (g == "sphere") {
-                    v = std::sqrt((x[0] - c[0]) * (x[0] - c[0]) + (x[1] - c[1]) * (x[1] - c[1]) +
-                                  (x[2] - c[2]) * (x[2] - c[2])) -
-                        rad;
-                } else if (g == "plane") {
-                    // normal points into the fluid: negative on the solid side
-                    v = ((x[0] - c[0]) * n[0] + (x[1] - c[1]) * n[1] + (x[2] - c[2]) * n[2]) / nl;
-                } else if (g == "cylinder") {
-                    double rr = 0.0;
-                    for (int d = 0; d < 3; ++d)
-                        if (d != dir) rr += (x[d] - c[d]) * (x[d] - c[d]);
-                    double q0 = std::sqrt(rr) - rad, q1 = std::fabs(x[dir] - c[dir]) - 0.5 * height;
-                    double o0 = std::max(q0, 0.0), o1 = std::max(q1, 0.0);
-                    v = std::sqrt(o0 * o0 + o1 * o1) + std::min(std::max(q0, q1), 0.0);
-                } else {  // box
-                    double q[3], o = 0.0, mx = -1e300;
-                    for (int d = 0; d < 3; ++d) {
-                        double cc = 0.5 * (lo[d] + hi[d]), hh = 0.5 * (hi[d] - lo[d]);
-                        q[d] = std::fabs(x[d] - cc) - hh;
-                        o += std::max(q[d], 0.0) * std::max(q[d], 0.0);
-                        mx = std::max(mx, q[d]);
-                    }
-                    v = std::sqrt(o) + std::min(mx, 0.0);
-                }
-                if (inside && !udf) v = -v;
-                phi[((long long)k * nn[1] + j) * nn[0] + i] = v;
+                const double x0 = exg_ls_node_x(s->plo[0], i, dx[0]), x1 = exg_ls_node_x(s->plo[1], j, dx[1]),
+                             x2 = exg_ls_node_x(s->plo[2], k, dx[2]);
+                phi[((long long)k * nn[1] + j) * nn[0] + i] = udf ? udf(x0, x1, x2) : exg_ls_shape_eval(sh, x0, x1, x2);
             }
     return EXG_OK;
 }

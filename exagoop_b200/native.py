@@ -106,6 +106,33 @@ class Diag(C.Structure):
                 "minpos": list(self.minpos), "maxpos": list(self.maxpos), "np": int(self.np)}
 
 
+LS_SPHERE, LS_PLANE, LS_CYLINDER, LS_BOX = 1, 2, 3, 4
+
+
+class LsShape(C.Structure):
+    """exg_ls_shape: one analytic level-set shape (sphere, plane, cylinder,
+    box), negative inside the solid."""
+    _fields_ = [("kind", C.c_int), ("inside", C.c_int), ("dir", C.c_int), ("center", D3), ("normal", D3),
+                ("radius", C.c_double), ("height", C.c_double), ("lo", D3), ("hi", D3)]
+
+    @classmethod
+    def sphere(cls, center, radius, inside=False):
+        return cls(kind=LS_SPHERE, inside=int(inside), center=D3(*center), radius=radius)
+
+    @classmethod
+    def plane(cls, point, normal, inside=False):
+        return cls(kind=LS_PLANE, inside=int(inside), center=D3(*point), normal=D3(*normal))
+
+    @classmethod
+    def cylinder(cls, center, radius, height, direction=2, inside=False):
+        return cls(kind=LS_CYLINDER, inside=int(inside), center=D3(*center), radius=radius, height=height,
+                   dir=direction)
+
+    @classmethod
+    def box(cls, lo, hi, inside=False):
+        return cls(kind=LS_BOX, inside=int(inside), lo=D3(*lo), hi=D3(*hi))
+
+
 # every symbol include/exg.h declares
 EXPORTED = [
     "exg_inputs_parse", "exg_inputs_parse_text", "exg_inputs_free", "exg_inputs_get", "exg_specs_from_inputs",
@@ -121,7 +148,8 @@ EXPORTED = [
     "exg_diagnostics", "exg_sort_keys", "exg_tile_size", "exg_set_stage_timing", "exg_last_step_timing",
     "exg_get_stream", "exg_p2g_momentum_noalloc", "exg_batch_create", "exg_batch_destroy", "exg_batch_scene",
     "exg_batch_num_scenes", "exg_batch_step", "exg_batch_last_error", "exg_particles_alloc_pinned",
-    "exg_particles_free_pinned",
+    "exg_particles_free_pinned", "exg_levelset_shape", "exg_levelset_build_device", "exg_init_levelsets",
+    "exg_get_levelset",
 ]
 
 _lib = None
@@ -145,6 +173,10 @@ def lib() -> C.CDLL:
         "exg_specs_from_inputs": (i, [vp, C.POINTER(Specs), C.c_char_p, C.c_size_t]),
         "exg_specs_default": (None, [C.POINTER(Specs)]),
         "exg_levelset_build": (i, [vp, C.POINTER(Specs), i, pd]),
+        "exg_levelset_shape": (i, [vp, i, C.POINTER(LsShape)]),
+        "exg_levelset_build_device": (i, [vp, i, C.POINTER(LsShape), i]),
+        "exg_init_levelsets": (i, [vp, vp]),
+        "exg_get_levelset": (i, [vp, i, pd]),
         "exg_particles_read_ascii": (i, [C.c_char_p, i, C.POINTER(ParticleSoA)]),
         "exg_particles_alloc": (i, [i64, C.POINTER(ParticleSoA)]),
         "exg_particles_free": (None, [C.POINTER(ParticleSoA)]),
@@ -328,6 +360,14 @@ class Inputs:
             raise ExgError(rc, "exg_levelset_build")
         return phi
 
+    def levelset_shape(self, body: int) -> LsShape:
+        """Analytic shape of body b (ExgError EXG_ERR_UNSUPPORTED for udf_cpp)."""
+        sh = LsShape()
+        rc = lib().exg_levelset_shape(self.h, body, C.byref(sh))
+        if rc:
+            raise ExgError(rc, "exg_levelset_shape")
+        return sh
+
 
 class Context:
     """One simulation on one GPU (exg_ctx).  Method names follow the
@@ -382,6 +422,22 @@ class Context:
     def set_levelset(self, body: int, phi: np.ndarray):
         phi = np.ascontiguousarray(phi, dtype=np.float64)
         self._ck(self.L.exg_set_levelset(self.h, body, dptr(phi)), "exg_set_levelset")
+
+    def build_levelset(self, body: int, shapes):
+        """Level set of body b as the union of analytic shapes, built on the GPU."""
+        shapes = [shapes] if isinstance(shapes, LsShape) else list(shapes)
+        arr = (LsShape * len(shapes))(*shapes)
+        self._ck(self.L.exg_levelset_build_device(self.h, body, arr, len(shapes)), "exg_levelset_build_device")
+
+    def init_levelsets(self, inputs: "Inputs"):
+        """Every body of an inputs file (init_eb): analytic ones on the GPU."""
+        self._ck(self.L.exg_init_levelsets(self.h, inputs.h), "exg_init_levelsets")
+
+    def get_levelset(self, body: int) -> np.ndarray:
+        nn = [self.specs.ncells[d] + 1 for d in range(3)]
+        phi = np.empty(nn[0] * nn[1] * nn[2], dtype=np.float64)
+        self._ck(self.L.exg_get_levelset(self.h, body, dptr(phi)), "exg_get_levelset")
+        return phi
 
     # --- L5 step functions
     def Initialise_Internal_Forces(self):

@@ -196,6 +196,24 @@ void exg_specs_default(exg_specs *specs);
  * reference builds these in mpm_ebtools::init_eb (Source/mpm_eb.cpp:100-388). */
 int exg_levelset_build(const exg_inputs *in, const exg_specs *specs, int body, double *phi_nodes);
 
+/* Analytic level-set shapes (the EB2 implicit functions of
+ * build_analytic_levelset, Source/mpm_eb.cpp:150-388): exact signed distance,
+ * negative inside the solid; inside = <geom>_has_fluid_inside flips the sign. */
+enum exg_ls_kind { EXG_LS_SPHERE = 1, EXG_LS_PLANE = 2, EXG_LS_CYLINDER = 3, EXG_LS_BOX = 4 };
+typedef struct exg_ls_shape {
+    int kind;          /* exg_ls_kind */
+    int inside;        /* fluid inside the shape */
+    int dir;           /* cylinder axis 0..2 */
+    double center[3];  /* sphere / cylinder centre, plane point */
+    double normal[3];  /* plane normal, pointing into the fluid */
+    double radius;     /* sphere, cylinder */
+    double height;     /* cylinder */
+    double lo[3], hi[3]; /* box */
+} exg_ls_shape;
+/* Shape of body b from its eb2.* / <body>.* keys; EXG_ERR_UNSUPPORTED for
+ * udf_cpp and stl bodies, which have no analytic form. */
+int exg_levelset_shape(const exg_inputs *in, int body, exg_ls_shape *shape);
+
 /* ASCII particle file of InitParticles (Source/mpm_init.cpp:942-1167).
  * Arrays are allocated with malloc; release with exg_particles_free. */
 int exg_particles_read_ascii(const char *path, int use_temp, exg_particle_soa *out);
@@ -221,6 +239,16 @@ int exg_synchronize(exg_ctx *ctx);
 /* Level set of body b, nodal (ncells+1)^3, x fastest (replaces the lsphi
  * MultiFab of LevelSetBody, Source/mpm_eb.H:45-117). */
 int exg_set_levelset(exg_ctx *ctx, int body, const double *phi_nodes);
+/* Level set of body b built on the GPU as the union (minimum) of nshapes
+ * analytic shapes evaluated at every node: no host grid and no host-to-device
+ * copy of it.  Bit-identical to exg_levelset_build for one shape. */
+int exg_levelset_build_device(exg_ctx *ctx, int body, const exg_ls_shape *shapes, int nshapes);
+/* Every body of the inputs, as mpm_ebtools::init_eb (Source/mpm_eb.cpp:
+ * 402-547) builds them: analytic shapes on the GPU, udf_cpp bodies on the
+ * host (the UDF is host code) and then uploaded. */
+int exg_init_levelsets(exg_ctx *ctx, const exg_inputs *in);
+/* Copy of body b's nodal level set to the host ((ncells+1)^3 doubles). */
+int exg_get_levelset(exg_ctx *ctx, int body, double *phi_nodes);
 
 /* Upload / download particles (host FP64 SoA).  Download returns particles in
  * upload order. */
