@@ -166,8 +166,12 @@ std::string validate(const exg_specs &s) {
     return "";
 }
 
+// Particle storage of one orientation.  Fields that no kernel changes and no
+// kernel reads (radius, yield acceleration, rigid-body id) live once, in
+// upload order, shared by both orientations: the per-step reorder does not
+// carry them.
 template <class R>
-void alloc_parts(Ctx &c, Parts<R> &P, std::vector<void *> &al, long long n, bool temp) {
+void alloc_parts(Ctx &c, Parts<R> &P, std::vector<void *> &al, long long n, bool temp, const Parts<R> *home) {
     auto A = [&](auto *&ptr) {
         using T = std::remove_pointer_t<std::remove_reference_t<decltype(ptr)>>;
         ptr = dalloc<T>(n);
@@ -191,8 +195,15 @@ void alloc_parts(Ctx &c, Parts<R> &P, std::vector<void *> &al, long long n, bool
     A(P.J);
     A(P.pres);
     A(P.vol0);
-    A(P.radius);
-    A(P.yacc);
+    if (home) {
+        P.radius = home->radius;
+        P.yacc = home->yacc;
+        P.rigid = home->rigid;
+    } else {
+        A(P.radius);
+        A(P.yacc);
+        A(P.rigid);
+    }
     if (temp) {
         A(P.T);
         A(P.cp);
@@ -202,7 +213,6 @@ void alloc_parts(Ctx &c, Parts<R> &P, std::vector<void *> &al, long long n, bool
     }
     A(P.mat);
     A(P.phase);
-    A(P.rigid);
     A(P.pid);
     (void)c;
 }
@@ -291,9 +301,10 @@ void download_parts(Ctx &c, exg_particle_soa *h) {
     const long long n = c.np;
     if (n == 0) return;
     const bool f64 = sizeof(R) == 8;
-    auto get_r = [&](const R *src, int field, double add = 0.0) {
+    auto get_r = [&](const R *src, int field, double add = 0.0, bool home = false) {
         double *dst = h->rdata + (size_t)field * n;
-        f64 ? d2h_field_fp64(c, src, P.pid, dst, n, add) : d2h_field_fp32(c, src, P.pid, dst, n, add);
+        const int32_t *pid = home ? nullptr : P.pid;  // upload-order fields need no reorder
+        f64 ? d2h_field_fp64(c, src, pid, dst, n, add) : d2h_field_fp32(c, src, pid, dst, n, add);
     };
     d2h_positions(c, P.x, P.pid, h->pos, n);
     for (int d = 0; d < 3; ++d) {
@@ -312,8 +323,8 @@ void download_parts(Ctx &c, exg_particle_soa *h) {
     d2h_field_fp64(c, P.J, P.pid, h->rdata + (size_t)EXG_R_JACOBIAN * n, n, 0.0);
     get_r(P.pres, EXG_R_PRESSURE);
     get_r(P.vol0, EXG_R_VOL_INIT);
-    get_r(P.radius, EXG_R_RADIUS);
-    get_r(P.yacc, EXG_R_YACC);
+    get_r(P.radius, EXG_R_RADIUS, 0.0, true);
+    get_r(P.yacc, EXG_R_YACC, 0.0, true);
     if (c.specs.use_temp) {
         d2h_field_fp64(c, P.T, P.pid, h->rdata + (size_t)EXG_R_TEMPERATURE * n, n, 0.0);
         get_r(P.cp, EXG_R_SPHEAT);
@@ -327,7 +338,7 @@ void download_parts(Ctx &c, exg_particle_soa *h) {
             std::fill(h->rdata + (size_t)f * n, h->rdata + (size_t)(f + 1) * n, 0.0);
     }
     d2h_int(c, P.phase, 1, P.pid, h->idata + (size_t)EXG_I_PHASE * n, n);
-    d2h_int(c, P.rigid, 4, P.pid, h->idata + (size_t)EXG_I_RIGID_ID * n, n);
+    d2h_int(c, P.rigid, 4, nullptr, h->idata + (size_t)EXG_I_RIGID_ID * n, n);
     // material index in upload order, expanded to the per-particle fields
     std::vector<int32_t> mat(n);
     d2h_int(c, P.mat, 4, P.pid, mat.data(), n);
@@ -837,8 +848,8 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
             delete reinterpret_cast<Parts<double> *>(c.pa);
             delete reinterpret_cast<Parts<double> *>(c.pb);
             auto *a = new Parts<double>(), *b = new Parts<double>();
-            alloc_parts(c, *a, c.allocs_a, n, temp);
-            alloc_parts(c, *b, c.allocs_b, n, temp);
+            alloc_parts<double>(c, *a, c.allocs_a, n, temp, nullptr);
+            alloc_parts<double>(c, *b, c.allocs_b, n, temp, a);
             c.pa = a;
             c.pb = b;
             c.np = n;
@@ -847,8 +858,8 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
             delete reinterpret_cast<Parts<float> *>(c.pa);
             delete reinterpret_cast<Parts<float> *>(c.pb);
             auto *a = new Parts<float>(), *b = new Parts<float>();
-            alloc_parts(c, *a, c.allocs_a, n, temp);
-            alloc_parts(c, *b, c.allocs_b, n, temp);
+            alloc_parts<float>(c, *a, c.allocs_a, n, temp, nullptr);
+            alloc_parts<float>(c, *b, c.allocs_b, n, temp, a);
             c.pa = a;
             c.pb = b;
             c.np = n;

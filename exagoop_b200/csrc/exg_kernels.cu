@@ -755,6 +755,15 @@ constexpr int kCellThreads = 128;
 #ifndef EXG_G2P_THREADS
 #define EXG_G2P_THREADS 256
 #endif
+// FP32 quadratic momentum P2G with the z-slices split across threads: 160
+// bins at a time (480 threads) measured fastest on the dam break (P2G 0.91
+// ms against 1.01 ms unsplit; 64, 128, 144, 168 and 170 bins slower)
+#ifndef EXG_P2G_SPLIT
+#define EXG_P2G_SPLIT 1
+#endif
+#ifndef EXG_P2G_SPLIT_BINS
+#define EXG_P2G_SPLIT_BINS 160
+#endif
 #ifndef EXG_G2P_MINB
 #define EXG_G2P_MINB 2
 #endif
@@ -768,7 +777,12 @@ struct P2GCfg {
     static constexpr int W = P2GStc<ORD>::W;
     // y rows of the stencil slice accumulated per pass (register budget)
     static constexpr int ROWS = (sizeof(R) == 8) ? 1 : (THERM ? (W == 4 ? 2 : 1) : W);
-    static constexpr int THREADS = (ORD == 2) ? EXG_P2G2_THREADS : kCellThreads;
+    // FP32 quadratic momentum: the three z-slices of a bin's window go to
+    // three threads (one pass each) instead of three passes of one thread,
+    // so a block works on a third of the bins at a time and their particles
+    // stay in L1 while the three slice threads read them
+    static constexpr bool SPLIT = EXG_P2G_SPLIT && sizeof(R) == 4 && ORD == 2 && !THERM;
+    static constexpr int THREADS = SPLIT ? 3 * EXG_P2G_SPLIT_BINS : (ORD == 2) ? EXG_P2G2_THREADS : kCellThreads;
     static constexpr int MINB = (ORD == 2) ? EXG_P2G2_MINB : 1;
 };
 
@@ -787,7 +801,10 @@ __device__ __forceinline__ void p2g_tile(const SplineTables *tab, unsigned *acc_
     tile_coords(P, t, tc);
     const int s0 = start[t];
     const int *cs = cell_start + (long long)w * (T3 + 1);
-    for (int c = threadIdx.x; c < T3; c += blockDim.x) {
+    constexpr bool SPLIT = P2GCfg<R, ORD, THERM>::SPLIT;
+    const int G = SPLIT ? (int)blockDim.x / W : (int)blockDim.x;  // bins worked on at once
+    const int sz_lo = SPLIT ? (int)threadIdx.x / G : 0, sz_hi = SPLIT ? sz_lo + 1 : W;
+    for (int c = SPLIT ? (int)threadIdx.x % G : (int)threadIdx.x; c < T3; c += G) {
         const int ka = cs[c], kb = cs[c + 1];
         if (ka == kb) continue;
         const int lx = c % T, ly = (c / T) % T, lz = c / (T * T);
@@ -797,7 +814,7 @@ __device__ __forceinline__ void p2g_tile(const SplineTables *tab, unsigned *acc_
         for (int d = 0; d < 3; ++d)
             inter[d] = (ORD == 1) || P.periodic[d] ||
                        (ORD == 2 ? (iv[d] >= 3 && iv[d] <= P.nc[d] - 3) : (iv[d] >= 3 && iv[d] <= P.nc[d] - 4));
-        for (int sz = 0; sz < W; ++sz) {
+        for (int sz = sz_lo; sz < sz_hi; ++sz) {
 #pragma unroll
             for (int sy0 = 0; sy0 < W; sy0 += ROWS) {
                 P2GAcc<R, THERM> acc[ROWS][W];
@@ -1733,13 +1750,13 @@ __device__ __forceinline__ bool all_finite(const R *a, int n) {
 #define EXG_G2P_PREFETCH 1
 #endif
 template <class R>
-__device__ __forceinline__ void prefetch_particle(const Parts<R> &A, long long i) {
+__device__ __forceinline__ void prefetch_particle(const Parts<R> &A, long long i, bool with_vp) {
     auto pf = [](const void *q) { asm volatile("prefetch.global.L2 [%0];" ::"l"(q)); };
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         pf(A.x[d] + i);
         pf(A.v[d] + i);
-        pf(A.vp[d] + i);
+        if (with_vp) pf(A.vp[d] + i);
     }
 #pragma unroll
     for (int q = 0; q < 9; ++q) pf(A.E[q] + i);
@@ -1750,9 +1767,6 @@ __device__ __forceinline__ void prefetch_particle(const Parts<R> &A, long long i
     pf(A.vol0 + i);
     pf(A.mat + i);
     pf(A.phase + i);
-    pf(A.radius + i);
-    pf(A.yacc + i);
-    pf(A.rigid + i);
     pf(A.pid + i);
 }
 
@@ -1784,18 +1798,22 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
     }
     __syncthreads();
     const int s0 = start[t], n = count[t];
+    // a velocity update overwrites v' of every phase-0 particle: the stored
+    // v' is read only for rigid particles and for G2P without it
+    const bool vel_only = mode == GM_VEL, fresh_vp = vel_only || upd_vel;
     for (int k = s0 + threadIdx.x; k < s0 + n; k += blockDim.x) {
-        if (EXG_G2P_PREFETCH && k + (int)blockDim.x < s0 + n) prefetch_particle<R>(A, k + blockDim.x);
+        if (EXG_G2P_PREFETCH && k + (int)blockDim.x < s0 + n) prefetch_particle<R>(A, k + blockDim.x, !fresh_vp);
         const int p = perm[k];
         const int phase = A.phase[p];
         double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+        const bool read_vp = !vel_only && (phase != 0 || !upd_vel);
         R v[3], vp[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             v[d] = A.v[d][p];
-            vp[d] = A.vp[d][p];
+            vp[d] = read_vp ? A.vp[d][p] : R(0);
         }
-        if (mode == GM_VEL) {
+        if (vel_only) {
             if (phase == 0) {
                 int iv[3];
                 cell_of(P, x, iv);
@@ -1902,11 +1920,8 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
         Bo.pres[k] = pres;
         Bo.mass[k] = mass;
         Bo.vol0[k] = vol0;
-        Bo.radius[k] = A.radius[p];
-        Bo.yacc[k] = A.yacc[p];
         Bo.mat[k] = mi;
         Bo.phase[k] = (uint8_t)phase;
-        Bo.rigid[k] = A.rigid[p];
         Bo.pid[k] = A.pid[p];
         if (P.use_temp) {
             Bo.T[k] = A.T[p];
@@ -1980,11 +1995,8 @@ __device__ __forceinline__ void copy_particle(const Parts<R> &A, long long i, Pa
     Bo.J[j] = A.J[i];
     Bo.pres[j] = A.pres[i];
     Bo.vol0[j] = A.vol0[i];
-    Bo.radius[j] = A.radius[i];
-    Bo.yacc[j] = A.yacc[i];
     Bo.mat[j] = A.mat[i];
     Bo.phase[j] = A.phase[i];
-    Bo.rigid[j] = A.rigid[i];
     Bo.pid[j] = A.pid[i];
     if (temp) {
         Bo.T[j] = A.T[i];
@@ -2768,15 +2780,16 @@ __global__ void k_from_f64(const double *src, R *dst, long long n, double sub) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < n) dst[i] = (R)(src[i] - sub);
 }
+// pid == nullptr: the field is stored in upload order already
 template <class R>
 __global__ void k_to_f64_unperm(const R *src, const int32_t *pid, double *dst, long long n, double add) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n) dst[pid[i]] = (double)src[i] + add;
+    if (i < n) dst[pid ? pid[i] : i] = (double)src[i] + add;
 }
 template <class T>
 __global__ void k_unperm_i32(const T *src, const int32_t *pid, int32_t *dst, long long n) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n) dst[pid[i]] = (int32_t)src[i];
+    if (i < n) dst[pid ? pid[i] : i] = (int32_t)src[i];
 }
 
 }  // namespace
