@@ -804,7 +804,7 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
             if (it == idx.end()) {
                 Material m;
                 std::tie(m.E, m.nu, m.K, m.gamma, m.mu, m.model) = key;
-                m.pad = 0;
+                m.ipow = (m.gamma >= 1.0 && m.gamma <= 16.0 && m.gamma == std::floor(m.gamma)) ? (int)m.gamma : 0;
                 it = idx.emplace(key, (int)c.mats.size()).first;
                 c.mats.push_back(m);
             }

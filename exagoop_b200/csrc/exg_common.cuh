@@ -141,7 +141,7 @@ struct Parts {
 struct Material {
     double E, nu, K, gamma, mu;
     int model;
-    int pad;
+    int ipow;  // gamma when it is a whole number in 1..16 (the Tait power by multiplication), else 0
 };
 
 // Dense nodal storage, reference component order, x fastest.

@@ -397,7 +397,7 @@ template <class R>
 __device__ __forceinline__ void particle_bounds(const Params &P, const Material &mt, double m, const double v[3],
                                                 double vol, const double sig[6], double rho, double cp, double T,
                                                 double kc, const double q[3], double Q, double b[CH_ALL],
-                                                double &dtp) {
+                                                double &speed) {
     b[CH_M] = fabs(m);
     for (int d = 0; d < 3; ++d) b[CH_P + d] = fabs(m * v[d]);
     const int rowi[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
@@ -422,7 +422,11 @@ __device__ __forceinline__ void particle_bounds(const Params &P, const Material 
         Cs = sqrt((lambda + 2.0 * mu) / rho);
     }
     double vm = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-    dtp = P.dxmin / (Cs + vm);
+    // the particle's CFL step is dxmin / speed; a thread that handles many
+    // particles keeps the largest speed and divides once: correctly rounded
+    // division by a positive number is monotone, so the minimum step is the
+    // same bits
+    speed = Cs + vm;
 }
 
 __device__ __forceinline__ void block_reduce_push(unsigned long long *bounds, unsigned long long *dtmin,
@@ -474,8 +478,10 @@ __global__ void __launch_bounds__(kThreads) k_state_reduce(Params P, Parts<R> A,
                 kc = A.kc[p];
                 Q = A.Q[p];
             }
+            double speed;
             particle_bounds<R>(P, mats[A.mat[p]], (double)A.mass[p], v, (double)A.vol[p], s, (double)A.rho[p], cp, T,
-                               kc, q, Q, b, dtp);
+                               kc, q, Q, b, speed);
+            dtp = P.dxmin / speed;
         }
     }
     block_reduce_push(bounds, dtmin, b, dtp, valid);
@@ -1663,6 +1669,20 @@ __device__ __forceinline__ void move_particle(const Params &P, const NodeBCArgs 
 // updateVolume + apply_constitutive_model for one phase-0 particle
 // (mpm_particle_timestep.cpp:131-182, mpm_particle_container.cpp:43-142).
 // J, the Tait pressure and the density division are FP64.
+// (1/J)^gamma of the Tait EOS: a whole-number gamma (7 for water) by
+// repeated squaring, a few ulp from pow at a small part of its cost
+__device__ __forceinline__ double tait_power(double x, const Material &mt) {
+    int n = mt.ipow;
+    if (n == 0) return pow(x, mt.gamma);
+    double r = 1.0, b = x;
+    while (n) {
+        if (n & 1) r *= b;
+        b *= b;
+        n >>= 1;
+    }
+    return r;
+}
+
 template <class R>
 __device__ __forceinline__ void volume_stress(const Params &P, const Material &mt, const R E[9], R vol0, R mass,
                                               const R sr[6], R eps[6], R sig[6], R &vol, R &rho, double &J, R &pres,
@@ -1704,7 +1724,7 @@ __device__ __forceinline__ void volume_stress(const Params &P, const Material &m
             linear_elastic<R>(eps, sig, (R)mt.E, (R)mt.nu);
         } else if (mt.model == 1) {
             // Tait EOS p = K ((1/J)^gamma - 1) (mpm_particle_container.cpp:113-120), FP64
-            const double pj = mt.K * (pow(1.0 / det, mt.gamma) - 1.0);
+            const double pj = mt.K * (tait_power(1.0 / det, mt) - 1.0);
             pres = (R)pj;
             newtonian<R>(sr, sig, (R)mt.mu, (R)pj);
         } else {
@@ -1777,7 +1797,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
                                          const Parts<R> &Bo, const Nodes<R> &Nd, const NodeBCArgs &bc,
                                          const Material *mats, const int *active, const int *start, const int *count,
                                          const int32_t *perm, int mode, int w, double dt, double asr, bool upd_vel,
-                                         float (&run_b)[CH_ALL], double &run_dt, bool &red, unsigned &status) {
+                                         float (&run_b)[CH_ALL], double &run_speed, bool &red, unsigned &status) {
     const int B = P.B, B3 = B * B * B;
     const int t = active[w];
     int tc[3];
@@ -1891,11 +1911,11 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
                     kc = A.kc[p];
                     Q = A.Q[p];
                 }
-                double bnd[CH_ALL], dtp;
-                particle_bounds<R>(P, mt, (double)mass, vd, (double)vol, sd, (double)rho, cp, T, kc, q, Q, bnd, dtp);
+                double bnd[CH_ALL], speed;
+                particle_bounds<R>(P, mt, (double)mass, vd, (double)vol, sd, (double)rho, cp, T, kc, q, Q, bnd, speed);
 #pragma unroll
                 for (int c = 0; c < CH_ALL; ++c) run_b[c] = fmaxf(run_b[c], __double2float_ru(bnd[c]));
-                run_dt = fmin(run_dt, dtp);
+                run_speed = fmax(run_speed, speed);
                 red = true;
             }
         }
@@ -1951,7 +1971,7 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB) k_g2p_fused(Par
     float run_b[CH_ALL];
 #pragma unroll
     for (int c = 0; c < CH_ALL; ++c) run_b[c] = 0.0f;
-    double run_dt = 1.7976931348623157e308;
+    double run_speed = 0.0;  // largest CFL wave speed of the thread's particles
     bool red = false;
     const int nitems = ctl->n_active_tiles;
     __shared__ int s_item;
@@ -1962,13 +1982,13 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB) k_g2p_fused(Par
         const int w = s_item;
         if (w >= nitems) break;
         g2p_tile<R, ORD>(tab, nb, P, A, Bo, Nd, bc, mats, active, start, count, perm, mode, w, dt, asr, upd_vel, run_b,
-                         run_dt, red, status);
+                         run_speed, red, status);
     }
     if (mode != GM_VEL) {
         double rb[CH_ALL];
 #pragma unroll
         for (int c = 0; c < CH_ALL; ++c) rb[c] = (double)run_b[c];
-        block_reduce_push(&ctl->bound_bits[0], &ctl->dtmin_bits, rb, run_dt, red);
+        block_reduce_push(&ctl->bound_bits[0], &ctl->dtmin_bits, rb, P.dxmin / run_speed, red);
     }
     if (status) atomicOr(&ctl->status, status);
 }
@@ -2724,16 +2744,17 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
     unsigned status = 0;
     double dt = 0.0, asr = 0.0;
     float run_b[CH_ALL];
-    double run_dt = 1.7976931348623157e308;
+    double run_speed = 0.0;
     bool red = false;
     // the reductions of a scene go to its control block when the block moves
     // on to another scene, and at the end
-    auto flush = [&](Ctl *ctl) {
+    auto flush = [&](const SceneDesc<R> &sd) {
+        Ctl *ctl = sd.ctl;
         if (mode != GM_VEL) {
             double rb[CH_ALL];
 #pragma unroll
             for (int c = 0; c < CH_ALL; ++c) rb[c] = (double)run_b[c];
-            block_reduce_push(&ctl->bound_bits[0], &ctl->dtmin_bits, rb, run_dt, red);
+            block_reduce_push(&ctl->bound_bits[0], &ctl->dtmin_bits, rb, sd.P.dxmin / run_speed, red);
         }
         if (status) atomicOr(&ctl->status, status);
         __syncthreads();
@@ -2749,21 +2770,21 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
         if (i >= total) break;
         const SceneDesc<R> &sd = descs[s];
         if (s != cur) {
-            if (cur >= 0) flush(descs[cur].ctl);
+            if (cur >= 0) flush(descs[cur]);
             cur = s;
             dt = sd.ctl->dt;
             const double time = sd.ctl->time;
             asr = (time < sd.P.applied_sr_time) ? sd.P.applied_sr : 0.0;
 #pragma unroll
             for (int c = 0; c < CH_ALL; ++c) run_b[c] = 0.0f;
-            run_dt = 1.7976931348623157e308;
+            run_speed = 0.0;
             red = false;
             status = 0;
         }
         g2p_tile<R, ORD>(tab, nb, sd.P, sd.A, sd.Bo, sd.N, sd.bc, sd.mats, sd.active, sd.start, sd.count, sd.perm, mode,
-                         i - b->pre_active[s], dt, asr, upd_vel, run_b, run_dt, red, status);
+                         i - b->pre_active[s], dt, asr, upd_vel, run_b, run_speed, red, status);
     }
-    if (cur >= 0) flush(descs[cur].ctl);
+    if (cur >= 0) flush(descs[cur]);
 }
 
 template <class R>
