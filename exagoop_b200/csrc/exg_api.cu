@@ -280,6 +280,20 @@ void upload_parts(Ctx &c, const exg_particle_soa *h, const std::vector<int32_t> 
 
 void drop_graphs(Ctx &c);
 
+}  // namespace
+
+bool exg::g2p_lean(const Ctx &c) {
+    const exg_specs &s = c.specs;
+    if (s.use_temp || s.calculate_strain_based_on_delta || s.num_bodies > 0) return false;
+    for (int d = 0; d < 3; ++d)
+        if (s.udf_wallvel_lo[d] || s.udf_wallvel_hi[d]) return false;
+    for (const Material &m : c.mats)
+        if (m.model > 1) return false;
+    return true;
+}
+
+namespace {
+
 // FP32 state keeps nodal temperatures relative to the mean particle
 // temperature, so that differences of a few millikelvin on a few hundred
 // kelvin stay resolved; a new reference re-bases the stored nodal values.
@@ -778,6 +792,7 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
         // material table: one entry per distinct (E, nu, K, gamma, mu, model)
         std::map<std::tuple<double, double, double, double, double, int>, int> idx;
         std::vector<int32_t> mat(n);
+        const bool lean_before = g2p_lean(c);
         c.mats.clear();
         auto key_of = [&](long long i) {
             return std::make_tuple(p->rdata[(size_t)EXG_R_E * n + i], p->rdata[(size_t)EXG_R_NU * n + i],
@@ -821,6 +836,7 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
         }
         EXG_CUDA_OK(cudaMemcpy(c.mat_dev, c.mats.data(), sizeof(Material) * c.mats.size(), cudaMemcpyHostToDevice));
         const bool temp = c.specs.use_temp != 0;
+        if (g2p_lean(c) != lean_before) drop_graphs(c);  // the graphs hold the other G2P variant
         if (c.pa && n == c.np && n == c.cap) {
             // same particle count: the storage, sort buffers and step graphs stay
             if (fp64(c))
@@ -1513,7 +1529,10 @@ int exg_batch_step(exg_batch *B, int nsteps) {
         for (Ctx *c : b.scenes)
             if (c->reduce_stale) do_reduce(*c);
         const bool changed = b.precision == EXG_PREC_FP64 ? batch_descriptors_fp64(b) : batch_descriptors_fp32(b);
-        if (changed) batch_drop_graphs(b);
+        int lean = 1;
+        for (Ctx *sc : b.scenes) lean = lean && g2p_lean(*sc);
+        if (changed || lean != b.lean) batch_drop_graphs(b);
+        b.lean = lean;
         const bool use_graph = std::getenv("EXG_NO_GRAPH") == nullptr;
         for (int s = 0; s < nsteps; ++s) {
             cudaGraphExec_t &g = b.gexec[b.parity];

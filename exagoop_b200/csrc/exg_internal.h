@@ -49,6 +49,10 @@ struct SortBufs {
 };
 
 struct Ctx;
+// True when the fused G2P can run its lean variant: no level-set bodies, no
+// UDF walls, no temperature, total strain, linear-elastic and Tait materials
+// only (exg_api.cu)
+bool g2p_lean(const Ctx &c);
 // positions and integer fields back to upload order (exg_kernels.cu)
 void d2h_positions(Ctx &c, double *const x[3], const int32_t *pid, double *host, long long n);
 void d2h_int(Ctx &c, const void *src, int bytes, const int32_t *pid, int32_t *host, long long n);
@@ -102,6 +106,7 @@ struct Batch {
     int parity = 0;                      // flips every step
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool warm[2] = {false, false};
+    int lean = -1;                       // G2P variant the graphs hold (g2p_lean of every scene)
 };
 // Uploads the scene descriptors of both parities; true when they changed.
 bool batch_descriptors_fp64(Batch &b);

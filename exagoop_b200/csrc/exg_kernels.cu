@@ -1605,13 +1605,14 @@ __device__ __forceinline__ void g2p_particle(const SplineTables &tab, const Para
 
 
 // moveParticles for one particle (mpm_particle_timestep.cpp:326-576).
-template <class R>
+// LEAN: no level-set bodies and no UDF walls (compiled out)
+template <class R, bool LEAN = false>
 __device__ __forceinline__ void move_particle(const Params &P, const NodeBCArgs &bc, int phase, double x[3], R v[3],
                                               const R vp[3], double dt, unsigned &status) {
     for (int d = 0; d < 3; ++d) x[d] += (double)vp[d] * dt;
     double rin[3] = {(double)v[0], (double)v[1], (double)v[2]};
     double rout[3] = {rin[0], rin[1], rin[2]};
-    if (P.num_bodies > 0 && phase == 0) {
+    if (!LEAN && P.num_bodies > 0 && phase == 0) {
         int hit = -1;
         double minphi = kTiny;
         for (int b = 0; b < P.num_bodies; ++b) {
@@ -1642,7 +1643,7 @@ __device__ __forceinline__ void move_particle(const Params &P, const NodeBCArgs 
         if (!lo && !hi) continue;
         double wv[3];
         for (int d = 0; d < 3; ++d) wv[d] = lo ? P.wvel_lo[dir * 3 + d] : P.wvel_hi[dir * 3 + d];
-        const double *tab = bc.udf[hi ? 1 : 0][dir];
+        const double *tab = LEAN ? nullptr : bc.udf[hi ? 1 : 0][dir];
         if (tab) {
             const int p0 = (dir == 0) ? 1 : 0, p1 = (dir == 2) ? 1 : 2;
             double f0 = (x[p0] - P.plo[p0]) / P.dx[p0], f1 = (x[p1] - P.plo[p1]) / P.dx[p1];
@@ -1683,7 +1684,9 @@ __device__ __forceinline__ double tait_power(double x, const Material &mt) {
     return r;
 }
 
-template <class R>
+// LEAN: total strain, linear-elastic and Tait materials only (the others
+// compiled out)
+template <class R, bool LEAN = false>
 __device__ __forceinline__ void volume_stress(const Params &P, const Material &mt, const R E[9], R vol0, R mass,
                                               const R sr[6], R eps[6], R sig[6], R &vol, R &rho, double &J, R &pres,
                                               double dt, double asr, bool do_volume, bool do_stress) {
@@ -1701,12 +1704,15 @@ __device__ __forceinline__ void volume_stress(const Params &P, const Material &m
         rho = (R)((double)mass / V);
     }
     if (do_stress) {
+        // one rounding, written out: left to the compiler, the contraction of
+        // this product could differ between the kernel variants that inline
+        // it (lean or full G2P, single-scene or batched)
 #pragma unroll
-        for (int d = 0; d < 6; ++d) eps[d] += (R)dt * sr[d];
+        for (int d = 0; d < 6; ++d) eps[d] = fma((R)dt, sr[d], eps[d]);
         eps[0] += (R)(dt * asr);
         eps[3] += (R)(dt * asr);
         eps[5] += (R)(dt * asr);
-        if (P.delta_strain) {
+        if (!LEAN && P.delta_strain) {
             // apply_constitutive_model_delta (mpm_particle_container.cpp:178-272):
             // sigma += C : (dt D + applied strain-rate increment), linear elastic
             if (mt.model == 0) {
@@ -1722,7 +1728,7 @@ __device__ __forceinline__ void volume_stress(const Params &P, const Material &m
             }
         } else if (mt.model == 0) {
             linear_elastic<R>(eps, sig, (R)mt.E, (R)mt.nu);
-        } else if (mt.model == 1) {
+        } else if (LEAN || mt.model == 1) {
             // Tait EOS p = K ((1/J)^gamma - 1) (mpm_particle_container.cpp:113-120), FP64
             const double pj = mt.K * (tait_power(1.0 / det, mt) - 1.0);
             pres = (R)pj;
@@ -1792,7 +1798,7 @@ __device__ __forceinline__ void prefetch_particle(const Parts<R> &A, long long i
 
 // One tile of the fused G2P: stage the tile's node block (v, dv and halo)
 // in shared memory, then update each of the tile's particles.
-template <class R, int ORD>
+template <class R, int ORD, bool LEAN>
 __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const Params &P, const Parts<R> &A,
                                          const Parts<R> &Bo, const Nodes<R> &Nd, const NodeBCArgs &bc,
                                          const Material *mats, const int *active, const int *start, const int *count,
@@ -1865,7 +1871,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
             }
             vol = A.vol[p];
             rho = A.rho[p];
-        } else if (P.delta_strain) {
+        } else if (!LEAN && P.delta_strain) {
             // the incremental formulation adds to the stored stress
 #pragma unroll
             for (int c = 0; c < 6; ++c) sig[c] = A.sig[c][p];
@@ -1877,7 +1883,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
             cell_of(P, x, iv);
             g2p_particle_smem<R, ORD>(*tab, P, na, x, iv, upd_vel, true, v, vp, E, sr, dt, jf);
         }
-        move_particle<R>(P, bc, phase, x, v, vp, dt, status);
+        move_particle<R, LEAN>(P, bc, phase, x, v, vp, dt, status);
         // Redistribute's periodic wrap
 #pragma unroll
         for (int d = 0; d < 3; ++d)
@@ -1891,7 +1897,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
         const Material mt = mats[mi];
         if (phase == 0) {
             J *= jf;  // FP32 state: J follows F multiplicatively in FP64
-            volume_stress<R>(P, mt, E, vol0, mass, sr, eps, sig, vol, rho, J, pres, dt, asr, true, true);
+            volume_stress<R, LEAN>(P, mt, E, vol0, mass, sr, eps, sig, vol, rho, J, pres, dt, asr, true, true);
             if (!all_finite(v, 3) || !all_finite(sig, 6) || !isfinite((double)J)) status |= ST_NAN;
             // reductions for the next step (running per thread)
             int iv2[3];
@@ -1904,7 +1910,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
 #pragma unroll
                 for (int c = 0; c < 6; ++c) sd[c] = (double)sig[c];
                 double q[3] = {0, 0, 0}, cp = 0, T = 0, kc = 0, Q = 0;
-                if (P.use_temp) {
+                if (!LEAN && P.use_temp) {
                     for (int d = 0; d < 3; ++d) q[d] = (double)A.q[d][p];
                     cp = A.cp[p];
                     T = A.T[p];
@@ -1943,7 +1949,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
         Bo.mat[k] = mi;
         Bo.phase[k] = (uint8_t)phase;
         Bo.pid[k] = A.pid[p];
-        if (P.use_temp) {
+        if (!LEAN && P.use_temp) {
             Bo.T[k] = A.T[p];
             Bo.cp[k] = A.cp[p];
             Bo.kc[k] = A.kc[p];
@@ -1954,7 +1960,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
     __syncthreads();
 }
 
-template <class R, int ORD>
+template <class R, int ORD, bool LEAN>
 __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
                                                         const Material *mats, const int *active, const int *start,
                                                         const int *count, const int32_t *perm, Ctl *ctl, int mode) {
@@ -1981,7 +1987,7 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB) k_g2p_fused(Par
         __syncthreads();
         const int w = s_item;
         if (w >= nitems) break;
-        g2p_tile<R, ORD>(tab, nb, P, A, Bo, Nd, bc, mats, active, start, count, perm, mode, w, dt, asr, upd_vel, run_b,
+        g2p_tile<R, ORD, LEAN>(tab, nb, P, A, Bo, Nd, bc, mats, active, start, count, perm, mode, w, dt, asr, upd_vel, run_b,
                          run_speed, red, status);
     }
     if (mode != GM_VEL) {
@@ -2730,7 +2736,7 @@ __global__ void __launch_bounds__(kThreads) k_nodes_batch(const SceneDesc<R> *__
     if (cur >= 0 && status) atomicOr(&descs[cur].ctl->status, status);
 }
 
-template <class R, int ORD>
+template <class R, int ORD, bool LEAN>
 __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
     k_g2p_batch(const SceneDesc<R> *__restrict__ descs, BatchCtl *b, int mode) {
     __shared__ int s_item, s_scene;
@@ -2781,7 +2787,7 @@ __global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB)
             red = false;
             status = 0;
         }
-        g2p_tile<R, ORD>(tab, nb, sd.P, sd.A, sd.Bo, sd.N, sd.bc, sd.mats, sd.active, sd.start, sd.count, sd.perm, mode,
+        g2p_tile<R, ORD, LEAN>(tab, nb, sd.P, sd.A, sd.Bo, sd.N, sd.bc, sd.mats, sd.active, sd.start, sd.count, sd.perm, mode,
                          i - b->pre_active[s], dt, asr, upd_vel, run_b, run_speed, red, status);
     }
     if (cur >= 0) flush(descs[cur]);
@@ -2964,11 +2970,11 @@ void EXG_SFX(launch_nodes)(Ctx &c, int mode, int flags, bool all_tiles) {
     EXG_CUDA_OK(cudaGetLastError());
 }
 
-template <class R, int ORD>
-static void g2p_t(Ctx &c, int mode) {
+template <class R, int ORD, bool LEAN>
+static void g2p_lt(Ctx &c, int mode) {
     const int B3 = c.P.B * c.P.B * c.P.B;
     size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(R) * SmemNodes<R>::NS * B3;
-    auto kern = k_g2p_fused<R, ORD>;
+    auto kern = k_g2p_fused<R, ORD, LEAN>;
     EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     static int grid = 0;
     static size_t gsm = 0;
@@ -2979,6 +2985,13 @@ static void g2p_t(Ctx &c, int mode) {
     kern<<<grid, EXG_G2P_THREADS, sm, c.stream>>>(c.P, c.A<R>(), c.Bp<R>(), c.N<R>(), make_bc(c), c.mat_dev, c.sb.active,
                                            c.sb.tile_start, c.sb.tile_count, c.sb.perm, c.ctl, mode);
     EXG_CUDA_OK(cudaGetLastError());
+}
+template <class R, int ORD>
+static void g2p_t(Ctx &c, int mode) {
+    if (g2p_lean(c))
+        g2p_lt<R, ORD, true>(c, mode);
+    else
+        g2p_lt<R, ORD, false>(c, mode);
 }
 void EXG_SFX(launch_g2p_fused)(Ctx &c, int mode) {
     using R = EXG_R;
@@ -3177,6 +3190,21 @@ static bool batch_descriptors_t(Batch &b) {
 }
 bool EXG_SFX(batch_descriptors)(Batch &b) { return batch_descriptors_t<EXG_R>(b); }
 
+template <class R, int ORD, bool LEAN>
+static void batch_g2p_t(Batch &b, const SceneDesc<R> *d, int B3) {
+    const size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(R) * SmemNodes<R>::NS * B3;
+    auto kern = k_g2p_batch<R, ORD, LEAN>;
+    EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    static int grid = 0;
+    static size_t gsm = 0;
+    if (!grid || gsm != sm) {
+        grid = persistent_grid(kern, sm, EXG_G2P_THREADS);
+        gsm = sm;
+    }
+    kern<<<grid, EXG_G2P_THREADS, sm, b.stream>>>(d, b.bctl, GM_FULL);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
 template <class R, int ORD>
 static void batch_core_t(Batch &b) {
     Ctx &c0 = *b.scenes[0];
@@ -3204,19 +3232,12 @@ static void batch_core_t(Batch &b) {
         k_nodes_batch<R, false><<<grid, kThreads, 0, b.stream>>>(d, b.bctl, NM_FUSED, flags);
         EXG_CUDA_OK(cudaGetLastError());
     }
-    {
-        const size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(R) * SmemNodes<R>::NS * B3;
-        auto kern = k_g2p_batch<R, ORD>;
-        EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        static int grid = 0;
-        static size_t gsm = 0;
-        if (!grid || gsm != sm) {
-            grid = persistent_grid(kern, sm, EXG_G2P_THREADS);
-            gsm = sm;
-        }
-        kern<<<grid, EXG_G2P_THREADS, sm, b.stream>>>(d, b.bctl, GM_FULL);
-        EXG_CUDA_OK(cudaGetLastError());
-    }
+    bool lean = true;
+    for (Ctx *s : b.scenes) lean = lean && g2p_lean(*s);
+    if (lean)
+        batch_g2p_t<R, ORD, true>(b, d, B3);
+    else
+        batch_g2p_t<R, ORD, false>(b, d, B3);
 }
 void EXG_SFX(launch_batch_core)(Batch &b) {
     using R = EXG_R;
