@@ -507,6 +507,9 @@ class Context:
         self._ck(self.L.exg_get_time(self.h, C.byref(t), C.byref(dt), C.byref(n)), "exg_get_time")
         return t.value, dt.value, n.value
 
+    def set_time(self, t: float, nsteps: int = 0):
+        self._ck(self.L.exg_set_time(self.h, float(t), int(nsteps)), "exg_set_time")
+
     def diagnostics(self) -> dict:
         d = Diag()
         self._ck(self.L.exg_diagnostics(self.h, C.byref(d)), "exg_diagnostics")

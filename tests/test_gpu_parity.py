@@ -304,6 +304,34 @@ def test_reupload_same_size_reuses_storage():
     assert np.array_equal(pa.rdata, pb.rdata) and np.array_equal(pa.pos, pb.pos)
 
 
+def test_reupload_that_changes_the_g2p_variant_rebuilds_graphs():
+    # a fluid-only set runs the lean fused G2P; re-uploading the same count
+    # as neo-Hookean solids must rebuild the step graphs with the full one
+    s, p = small_dam(seed=23)
+    s.precision = nt.PREC_FP64
+    ctx = nt.Context(s)
+    ctx.upload(p)
+    ctx.Initialise_Internal_Forces()
+    ctx.step(4)
+    q = p.copy()
+    q.idata[nt.I_MODEL] = 2
+    q.rdata[nt.R_E] = 2e5
+    q.rdata[nt.R_NU] = 0.3
+    ctx.upload(q)
+    ctx.set_time(0.0, 0)
+    ctx.Initialise_Internal_Forces()
+    ctx.step(6)
+    got = ctx.download()
+    o = orc.Oracle(s)
+    o.upload(q)
+    o.init_internal_forces()
+    assert o.step(6) == 0
+    r = o.download()
+    for name, f, k in [("vel", nt.R_VEL, 3), ("stress", nt.R_STRESS, 6), ("defgrad", nt.R_DEFGRAD, 9)]:
+        e = np.abs(got.rdata[f:f + k] - r.rdata[f:f + k]).max() / np.abs(r.rdata[f:f + k]).max()
+        assert e < 1e-10, (name, e)
+
+
 def test_pinned_particle_sets_round_trip():
     s, p = small_dam(seed=22)
     hp = p.pinned_copy()
