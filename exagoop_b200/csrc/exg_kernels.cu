@@ -1272,8 +1272,16 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
     }
 }
 
+// Four 256-thread blocks per SM (64 registers, some spilled): the per-node
+// work is a chain of dependent loads (slot, then up to eight staging
+// blocks), so occupancy decides its speed (the dam break's nodal update
+// 0.171 ms with one block per SM and no register cap, 0.108 / 0.086 / 0.080
+// ms with two / three / four blocks)
+#ifndef EXG_NODES_MINB
+#define EXG_NODES_MINB 4
+#endif
 template <class R, bool THERM>
-__global__ void __launch_bounds__(kThreads) k_nodes(Params P, Nodes<R> Nd, NodeBCArgs bc, const int *tiles,
+__global__ void __launch_bounds__(kThreads, EXG_NODES_MINB) k_nodes(Params P, Nodes<R> Nd, NodeBCArgs bc, const int *tiles,
                                                     const int *slot, const long long *staging, Ctl *ctl, int mode,
                                                     int flags) {
     constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
@@ -2728,7 +2736,7 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
 }
 
 template <class R, bool THERM>
-__global__ void __launch_bounds__(kThreads) k_nodes_batch(const SceneDesc<R> *__restrict__ descs, BatchCtl *b, int mode,
+__global__ void __launch_bounds__(kThreads, EXG_NODES_MINB) k_nodes_batch(const SceneDesc<R> *__restrict__ descs, BatchCtl *b, int mode,
                                                           int flags) {
     constexpr int NCH = THERM ? CH_ALL : CH_MOM_END;
     __shared__ int s_item, s_scene;
@@ -2981,9 +2989,11 @@ void EXG_SFX(launch_p2g)(Ctx &c, int flags) {
 void EXG_SFX(launch_nodes)(Ctx &c, int mode, int flags, bool all_tiles) {
     using R = EXG_R;
     const bool th = (flags & (PF_TEMP | PF_SRC)) != 0;
-    static int pgrid = 0;
-    if (!pgrid) pgrid = persistent_grid(k_nodes<R, true>, 0);
-    int grid = all_tiles ? (int)std::min<long long>(c.P.ntiles, pgrid) : pgrid;
+    static int pgrid = 0, pgrid_th = 0;
+    if (!pgrid) pgrid = persistent_grid(k_nodes<R, false>, 0);
+    if (!pgrid_th) pgrid_th = persistent_grid(k_nodes<R, true>, 0);
+    const int pg = th ? pgrid_th : pgrid;  // the grid of the variant launched
+    int grid = all_tiles ? (int)std::min<long long>(c.P.ntiles, pg) : pg;
     const int *tiles = all_tiles ? nullptr : c.sb.touched;
     NodeBCArgs bc = make_bc(c);
     if (th)
