@@ -9,6 +9,7 @@
 #include <map>
 #include <memory>
 #include <stdexcept>
+#include <thread>
 #include <tuple>
 #include "exg_internal.h"
 #include "exg_levelset.h"
@@ -49,6 +50,27 @@ T *dalloc(size_t n) {
     if (n == 0) n = 1;
     EXG_CUDA_OK(cudaMalloc(&p, n * sizeof(T)));
     return reinterpret_cast<T *>(p);
+}
+
+// Host loops over the particles (material table, upload order, download
+// expansion) split over the host's cores: at millions of particles they are
+// a visible part of an upload or download otherwise.  fn(chunk, begin, end)
+// must not throw.
+int host_chunks(long long n) {
+    if (n < (1ll << 20)) return 1;
+    const unsigned hc = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(hc ? hc : 1u, 32u));
+}
+template <class F>
+void parallel_chunks(long long n, int nchunks, F fn) {
+    if (nchunks <= 1) {
+        fn(0, 0ll, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(nchunks);
+    for (int t = 0; t < nchunks; ++t) th.emplace_back(fn, t, n * t / nchunks, n * (t + 1) / nchunks);
+    for (auto &x : th) x.join();
 }
 
 int ilog2(int v) {
@@ -267,10 +289,12 @@ void upload_parts(Ctx &c, const exg_particle_soa *h, const std::vector<int32_t> 
     EXG_CUDA_OK(cudaMemcpyAsync(P.mat, mat.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, c.stream));
     std::vector<uint8_t> ph(n);
     std::vector<int32_t> pid(n);
-    for (long long i = 0; i < n; ++i) {
-        ph[i] = (uint8_t)h->idata[(size_t)EXG_I_PHASE * n + i];
-        pid[i] = (int32_t)i;
-    }
+    parallel_chunks(n, host_chunks(n), [&](int, long long a, long long b) {
+        for (long long i = a; i < b; ++i) {
+            ph[i] = (uint8_t)h->idata[(size_t)EXG_I_PHASE * n + i];
+            pid[i] = (int32_t)i;
+        }
+    });
     EXG_CUDA_OK(cudaMemcpyAsync(P.phase, ph.data(), n, cudaMemcpyHostToDevice, c.stream));
     EXG_CUDA_OK(cudaMemcpyAsync(P.rigid, h->idata + (size_t)EXG_I_RIGID_ID * n, sizeof(int32_t) * n,
                                 cudaMemcpyHostToDevice, c.stream));
@@ -348,8 +372,9 @@ void download_parts(Ctx &c, exg_particle_soa *h) {
     } else {
         const int tf[7] = {EXG_R_TEMPERATURE, EXG_R_SPHEAT,         EXG_R_THERMCOND, EXG_R_HEATFLUX,
                            EXG_R_HEATFLUX + 1, EXG_R_HEATFLUX + 2, EXG_R_HEATSRC};
-        for (int f : tf)
-            std::fill(h->rdata + (size_t)f * n, h->rdata + (size_t)(f + 1) * n, 0.0);
+        parallel_chunks(n, host_chunks(n), [&](int, long long a, long long b) {
+            for (int f : tf) std::fill(h->rdata + (size_t)f * n + a, h->rdata + (size_t)f * n + b, 0.0);
+        });
     }
     d2h_int(c, P.phase, 1, P.pid, h->idata + (size_t)EXG_I_PHASE * n, n);
     d2h_int(c, P.rigid, 4, nullptr, h->idata + (size_t)EXG_I_RIGID_ID * n, n);
@@ -357,15 +382,17 @@ void download_parts(Ctx &c, exg_particle_soa *h) {
     std::vector<int32_t> mat(n);
     d2h_int(c, P.mat, 4, P.pid, mat.data(), n);
     EXG_CUDA_OK(cudaStreamSynchronize(c.stream));
-    for (long long j = 0; j < n; ++j) {
-        const Material &m = c.mats[mat[j]];
-        h->rdata[(size_t)EXG_R_E * n + j] = m.E;
-        h->rdata[(size_t)EXG_R_NU * n + j] = m.nu;
-        h->rdata[(size_t)EXG_R_BULK * n + j] = m.K;
-        h->rdata[(size_t)EXG_R_GAMMA * n + j] = m.gamma;
-        h->rdata[(size_t)EXG_R_VISC * n + j] = m.mu;
-        h->idata[(size_t)EXG_I_MODEL * n + j] = m.model;
-    }
+    parallel_chunks(n, host_chunks(n), [&](int, long long a, long long b) {
+        for (long long j = a; j < b; ++j) {
+            const Material &m = c.mats[mat[j]];
+            h->rdata[(size_t)EXG_R_E * n + j] = m.E;
+            h->rdata[(size_t)EXG_R_NU * n + j] = m.nu;
+            h->rdata[(size_t)EXG_R_BULK * n + j] = m.K;
+            h->rdata[(size_t)EXG_R_GAMMA * n + j] = m.gamma;
+            h->rdata[(size_t)EXG_R_VISC * n + j] = m.mu;
+            h->idata[(size_t)EXG_I_MODEL * n + j] = m.model;
+        }
+    });
 }
 
 void sync(Ctx &c) { EXG_CUDA_OK(cudaStreamSynchronize(c.stream)); }
@@ -794,39 +821,68 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
         std::vector<int32_t> mat(n);
         const bool lean_before = g2p_lean(c);
         c.mats.clear();
+        using Key = std::tuple<double, double, double, double, double, int>;
         auto key_of = [&](long long i) {
             return std::make_tuple(p->rdata[(size_t)EXG_R_E * n + i], p->rdata[(size_t)EXG_R_NU * n + i],
                                    p->rdata[(size_t)EXG_R_BULK * n + i], p->rdata[(size_t)EXG_R_GAMMA * n + i],
                                    p->rdata[(size_t)EXG_R_VISC * n + i], (int)p->idata[(size_t)EXG_I_MODEL * n + i]);
         };
-        std::tuple<double, double, double, double, double, int> last;
-        int last_id = -1;
-        for (long long i = 0; i < n; ++i) {
-            const auto key = key_of(i);
-            if (last_id >= 0 && key == last) {  // runs of one material: no map lookup
-                mat[i] = last_id;
-                continue;
+        // per chunk: its distinct materials in order of first appearance and
+        // chunk-local indices (runs of one material need no lookup); the
+        // merge in chunk order numbers the materials by first appearance
+        const int nch = host_chunks(n);
+        std::vector<std::vector<Key>> local(nch);
+        parallel_chunks(n, nch, [&](int t, long long a, long long b) {
+            std::vector<Key> &keys = local[t];
+            Key last;
+            int last_id = -1;
+            for (long long i = a; i < b; ++i) {
+                const Key key = key_of(i);
+                if (last_id >= 0 && key == last) {
+                    mat[i] = last_id;
+                    continue;
+                }
+                int id = -1;
+                for (size_t q = 0; q < keys.size(); ++q)
+                    if (keys[q] == key) {
+                        id = (int)q;
+                        break;
+                    }
+                if (id < 0) {
+                    id = (int)keys.size();
+                    keys.push_back(key);
+                }
+                mat[i] = id;
+                last = key;
+                last_id = id;
             }
-            const int model = std::get<5>(key);
-            if (model < 0 || model > 2)
-                return fail(ctx, EXG_ERR_UNSUPPORTED, "unknown constitutive model " + std::to_string(model));
-            if (model != 0 && c.specs.calculate_strain_based_on_delta == 1)
-                // apply_constitutive_model_delta aborts on these models
-                // (mpm_particle_container.cpp:251-262)
-                return fail(ctx, EXG_ERR_UNSUPPORTED, "calculate_strain_based_on_delta = 1 supports the "
-                                                      "linear-elastic model only");
-            auto it = idx.find(key);
-            if (it == idx.end()) {
-                Material m;
-                std::tie(m.E, m.nu, m.K, m.gamma, m.mu, m.model) = key;
-                m.ipow = (m.gamma >= 1.0 && m.gamma <= 16.0 && m.gamma == std::floor(m.gamma)) ? (int)m.gamma : 0;
-                it = idx.emplace(key, (int)c.mats.size()).first;
-                c.mats.push_back(m);
+        });
+        std::vector<std::vector<int32_t>> trans(nch);
+        for (int t = 0; t < nch; ++t)
+            for (const Key &key : local[t]) {
+                const int model = std::get<5>(key);
+                if (model < 0 || model > 2)
+                    return fail(ctx, EXG_ERR_UNSUPPORTED, "unknown constitutive model " + std::to_string(model));
+                if (model != 0 && c.specs.calculate_strain_based_on_delta == 1)
+                    // apply_constitutive_model_delta aborts on these models
+                    // (mpm_particle_container.cpp:251-262)
+                    return fail(ctx, EXG_ERR_UNSUPPORTED, "calculate_strain_based_on_delta = 1 supports the "
+                                                          "linear-elastic model only");
+                auto it = idx.find(key);
+                if (it == idx.end()) {
+                    Material m;
+                    std::tie(m.E, m.nu, m.K, m.gamma, m.mu, m.model) = key;
+                    m.ipow = (m.gamma >= 1.0 && m.gamma <= 16.0 && m.gamma == std::floor(m.gamma)) ? (int)m.gamma
+                                                                                                       : 0;
+                    it = idx.emplace(key, (int)c.mats.size()).first;
+                    c.mats.push_back(m);
+                }
+                trans[t].push_back(it->second);
             }
-            mat[i] = it->second;
-            last = key;
-            last_id = it->second;
-        }
+        parallel_chunks(n, nch, [&](int t, long long a, long long b) {
+            const std::vector<int32_t> &tr = trans[t];
+            for (long long i = a; i < b; ++i) mat[i] = tr[mat[i]];
+        });
         if (c.mats.empty()) c.mats.push_back(Material{});
         if (!c.mat_dev || c.mat_cap < c.mats.size()) {
             if (c.mat_dev) cudaFree(c.mat_dev);

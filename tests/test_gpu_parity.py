@@ -332,6 +332,40 @@ def test_reupload_that_changes_the_g2p_variant_rebuilds_graphs():
         assert e < 1e-10, (name, e)
 
 
+def test_large_upload_material_table_round_trip():
+    # above 2^20 particles the host loops of upload and download run in
+    # chunks on several threads: materials that alternate in runs across
+    # the chunk boundaries come back per particle as they went in
+    s, _ = small_dam(seed=24)
+    n = 1_500_000
+    rng = np.random.default_rng(24)
+    p = nt.Particles(n)
+    for d in range(3):
+        p.pos[d] = s.plo[d] + (s.phi[d] - s.plo[d]) * rng.uniform(0.05, 0.95, n)
+    p.rdata[nt.R_MASS] = 1e-3
+    p.rdata[nt.R_VOLUME] = 1e-6
+    p.rdata[nt.R_VOL_INIT] = 1e-6
+    p.rdata[nt.R_DENSITY] = 1000.0
+    p.rdata[nt.R_JACOBIAN] = 1.0
+    for q in (0, 4, 8):
+        p.rdata[nt.R_DEFGRAD + q] = 1.0
+    run = (np.arange(n) // 7919) % 5
+    table = [(1e5, 0.3, 0.0, 0.0, 0.0, 0), (2e6, 0.0, 2e6, 7.0, 1e-3, 1), (3e5, 0.25, 0.0, 0.0, 0.0, 2),
+             (4e5, 0.2, 0.0, 0.0, 0.0, 0), (0.0, 0.0, 1e6, 1.5, 2e-3, 1)]
+    for f, k in [(nt.R_E, 0), (nt.R_NU, 1), (nt.R_BULK, 2), (nt.R_GAMMA, 3), (nt.R_VISC, 4)]:
+        p.rdata[f] = np.array([t[k] for t in table])[run]
+    p.idata[nt.I_MODEL] = np.array([t[5] for t in table])[run]
+    p.idata[nt.I_RIGID_ID] = np.arange(n) % 11
+    ctx = nt.Context(s)
+    ctx.upload(p)
+    got = ctx.download()
+    for f in (nt.R_E, nt.R_NU, nt.R_BULK, nt.R_GAMMA, nt.R_VISC, nt.R_RADIUS, nt.R_YACC):
+        assert np.array_equal(got.rdata[f], p.rdata[f]), f
+    assert np.array_equal(got.idata, p.idata)
+    assert np.array_equal(got.pos, p.pos)
+    ctx.close()
+
+
 def test_pinned_particle_sets_round_trip():
     s, p = small_dam(seed=22)
     hp = p.pinned_copy()
