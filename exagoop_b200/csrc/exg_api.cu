@@ -505,8 +505,6 @@ void do_reduce(Ctx &c) {
     c.reduce_stale = false;
 }
 
-void ensure_nodes_clean(Ctx &c);
-
 // One fused step, enqueued on c.stream (capturable).
 void enqueue_step(Ctx &c) {
     EXG_CUDA_OK(cudaMemcpyAsync(c.bounds_cur, &c.ctl->bound_bits[0], sizeof(unsigned long long) * CH_ALL,
