@@ -761,9 +761,10 @@ constexpr int kCellThreads = 128;
 #ifndef EXG_G2P_THREADS
 #define EXG_G2P_THREADS 256
 #endif
-// FP32 quadratic momentum P2G with the z-slices split across threads: 160
-// bins at a time (480 threads) measured fastest on the dam break (P2G 0.91
-// ms against 1.01 ms unsplit; 64, 128, 144, 168 and 170 bins slower)
+// Quadratic momentum P2G with the z-slices split across threads: 160
+// bins at a time (480 threads) measured fastest on the dam break (FP32 P2G
+// 0.91 ms against 1.01 ms unsplit, FP64 2.35 against 2.51 ms; 64, 128, 144,
+// 168 and 170 bins slower)
 #ifndef EXG_P2G_SPLIT
 #define EXG_P2G_SPLIT 1
 #endif
@@ -788,11 +789,12 @@ struct P2GCfg {
     static constexpr int W = P2GStc<ORD>::W;
     // y rows of the stencil slice accumulated per pass (register budget)
     static constexpr int ROWS = (sizeof(R) == 8) ? 1 : (THERM ? (W == 4 ? 2 : 1) : W);
-    // FP32 quadratic momentum: the three z-slices of a bin's window go to
-    // three threads (one pass each) instead of three passes of one thread,
-    // so a block works on a third of the bins at a time and their particles
-    // stay in L1 while the three slice threads read them
-    static constexpr bool SPLIT = EXG_P2G_SPLIT && sizeof(R) == 4 && ORD == 2 && !THERM;
+    // quadratic momentum: the three z-slices of a bin's window go to three
+    // threads (FP32: one pass each, FP64: one pass per y row) instead of one
+    // thread walking them in turn, so a block works on a third of the bins
+    // at a time and their particles stay in L1 while the three slice threads
+    // read them
+    static constexpr bool SPLIT = EXG_P2G_SPLIT && ORD == 2 && !THERM;
     static constexpr int THREADS = SPLIT ? 3 * EXG_P2G_SPLIT_BINS : (ORD == 2) ? EXG_P2G2_THREADS : kCellThreads;
     static constexpr int MINB = (ORD == 2) ? EXG_P2G2_MINB : 1;
 };
