@@ -175,8 +175,14 @@ __global__ void k_keys(Params P, double *x0, double *x1, double *x2, long long n
             key[i] = ((uint32_t)t << (3 * ts)) | loc;
         }
     }
-    // warp-aggregated tile histogram (particles arrive nearly sorted)
+    // warp-aggregated tile histogram (particles arrive nearly sorted, so a
+    // warp's lanes usually share one tile: then one lane adds for all)
     unsigned act = __ballot_sync(0xffffffffu, t >= 0);
+    const int t0 = __shfl_sync(0xffffffffu, t, 0);
+    if (act == 0xffffffffu && __all_sync(0xffffffffu, t == t0)) {
+        if ((threadIdx.x & 31) == 0) atomicAdd(&tile_count[t0], 32);
+        return;
+    }
     if (t >= 0) {
         unsigned peers = __match_any_sync(act, t);
         int leader = __ffs(peers) - 1;
@@ -265,9 +271,18 @@ __global__ void k_scatter(long long n, const uint32_t *key, int tshift3, const i
         if (k != 0xFFFFFFFFu) t = (int)(k >> tshift3);
     }
     unsigned act = __ballot_sync(0xffffffffu, t >= 0);
+    const int lane = threadIdx.x & 31;
+    const int t0 = __shfl_sync(0xffffffffu, t, 0);
+    if (act == 0xffffffffu && __all_sync(0xffffffffu, t == t0)) {
+        // the whole warp in one tile (the usual case): one add, lane order
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&fill[t0], 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        bucket[start[t0] + base + lane] = (int32_t)i;
+        return;
+    }
     if (t >= 0) {
         unsigned peers = __match_any_sync(act, t);
-        int lane = threadIdx.x & 31;
         int leader = __ffs(peers) - 1;
         int base = 0;
         if (lane == leader) base = atomicAdd(&fill[t], __popc(peers));
@@ -2070,6 +2085,7 @@ __device__ __forceinline__ void copy_particle(const Parts<R> &A, long long i, Pa
 
 template <class R>
 __global__ void k_copy_lost(Parts<R> A, Parts<R> Bo, const uint32_t *key, long long np, Ctl *ctl, int temp) {
+    if (ctl->lost == 0) return;  // the usual case: nothing to copy, no key to read
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= np || key[i] != 0xFFFFFFFFu) return;
     long long j = ctl->n_sorted + (long long)atomicAdd(&ctl->lost_fill, 1ull);
