@@ -294,7 +294,12 @@ __global__ void k_scatter(long long n, const uint32_t *key, int tshift3, const i
 
 // Per-tile stable ordering: particles of one tile sorted by (cell, storage
 // index), which equals a stable sort of the whole array by key.
-constexpr int kSortCap = 12288;
+// Entries of a tile sorted in shared memory (larger tiles use the global
+// scratch after the bucket array).  5120 (26 KB a block, a tile of 8^3
+// bins at ten particles per bin) measured fastest on the dam break, where
+// occupancy sets the sort's speed: 0.223 ms against 0.257 ms at 12288 and
+// 0.237 / 0.228 / 0.224 ms at 8192 / 6144 / 4608.
+constexpr int kSortCap = 5120;
 __global__ void __launch_bounds__(kThreads) k_tile_sort(const int *active, const int *start, const int *count,
                                                         const uint32_t *key, const int32_t *bucket, int32_t *scratch,
                                                         int32_t *perm, int *cell_start, int ncell, Ctl *ctl) {
