@@ -781,10 +781,10 @@ constexpr int kCellThreads = 128;
 #ifndef EXG_G2P_THREADS
 #define EXG_G2P_THREADS 256
 #endif
-// Quadratic momentum P2G with the z-slices split across threads: 160
-// bins at a time (480 threads) measured fastest on the dam break (FP32 P2G
-// 0.91 ms against 1.01 ms unsplit, FP64 2.35 against 2.51 ms; 64, 128, 144,
-// 168 and 170 bins slower)
+// Quadratic momentum P2G with the z-slices split across threads, a bin's
+// three slices in adjacent threads (FP32 P2G 0.77 ms on the dam break
+// against 1.01 ms unsplit and 0.87 ms with the slices in separate thirds of
+// the block; FP64 1.47 against 2.51 ms unsplit)
 #ifndef EXG_P2G_SPLIT
 #define EXG_P2G_SPLIT 1
 #endif
@@ -793,9 +793,7 @@ constexpr int kCellThreads = 128;
 #ifndef EXG_P2G_PREFETCH
 #define EXG_P2G_PREFETCH 1
 #endif
-#ifndef EXG_P2G_SPLIT_BINS
-#define EXG_P2G_SPLIT_BINS 160
-#endif
+
 #ifndef EXG_G2P_MINB
 #define EXG_G2P_MINB 2
 #endif
@@ -810,12 +808,11 @@ struct P2GCfg {
     // y rows of the stencil slice accumulated per pass (register budget)
     static constexpr int ROWS = (sizeof(R) == 8) ? 1 : (THERM ? (W == 4 ? 2 : 1) : W);
     // quadratic momentum: the three z-slices of a bin's window go to three
-    // threads (FP32: one pass each, FP64: one pass per y row) instead of one
-    // thread walking them in turn, so a block works on a third of the bins
-    // at a time and their particles stay in L1 while the three slice threads
-    // read them
+    // adjacent threads (FP32: one pass each, FP64: one pass per y row)
+    // instead of one thread walking them in turn, so the bin's particles are
+    // read by the three together and stay in L1
     static constexpr bool SPLIT = EXG_P2G_SPLIT && ORD == 2 && !THERM;
-    static constexpr int THREADS = SPLIT ? 3 * EXG_P2G_SPLIT_BINS : (ORD == 2) ? EXG_P2G2_THREADS : kCellThreads;
+    static constexpr int THREADS = (ORD == 2) ? EXG_P2G2_THREADS : kCellThreads;
     static constexpr int MINB = (ORD == 2) ? EXG_P2G2_MINB : 1;
 };
 
@@ -835,14 +832,19 @@ __device__ __forceinline__ void p2g_tile(const SplineTables *tab, unsigned *acc_
     const int s0 = start[t];
     const int *cs = cell_start + (long long)w * (T3 + 1);
     constexpr bool SPLIT = P2GCfg<R, ORD, THERM>::SPLIT;
-    const int G = SPLIT ? (int)blockDim.x / W : (int)blockDim.x;  // bins worked on at once
-    const int sz_lo = SPLIT ? (int)threadIdx.x / G : 0, sz_hi = SPLIT ? sz_lo + 1 : W;
-    for (int c = SPLIT ? (int)threadIdx.x % G : (int)threadIdx.x; c < T3; c += G) {
+    // split: tasks (bin, slice) with the three slices of a bin in adjacent
+    // threads, so they read the bin's particles together and every thread of
+    // a 512-thread block takes exactly three tasks of an 8^3 tile
+    const int ntask = SPLIT ? W * T3 : T3, step = (int)blockDim.x;
+    for (int u = threadIdx.x; u < ntask; u += step) {
+        const int c = SPLIT ? u / W : u;
+        const int sz_lo = SPLIT ? u - c * W : 0, sz_hi = SPLIT ? sz_lo + 1 : W;
+        const int cnext = SPLIT ? (u + step) / W : u + step;
         const int ka = cs[c], kb = cs[c + 1];
-        if (EXG_P2G_PREFETCH && sz_lo == 0 && c + G < T3) {
+        if (EXG_P2G_PREFETCH && sz_lo == 0 && cnext < T3) {
             // L2 prefetch of the first particle of the bin this thread takes next
-            const int kn = cs[c + G];
-            if (kn < cs[c + G + 1]) {
+            const int kn = cs[cnext];
+            if (kn < cs[cnext + 1]) {
                 const int pn = perm[s0 + kn];
                 auto pf = [](const void *q) { asm volatile("prefetch.global.L2 [%0];" ::"l"(q)); };
 #pragma unroll
