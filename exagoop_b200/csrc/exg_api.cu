@@ -1429,6 +1429,8 @@ int exg_last_step_timing(exg_ctx *ctx, double *ms5) {
 int exg_p2g_momentum_noalloc(const exg_specs *specs, const exg_particle_soa *dev_particles, double *node_mass,
                              double *node_vel, double *node_frc, void *stream) {
     if (!specs || !dev_particles || !node_mass || !node_vel || !node_frc || dev_particles->np < 0) return EXG_ERR_ARG;
+    if (dev_particles->np > 0 && (!dev_particles->pos || !dev_particles->rdata || !dev_particles->idata))
+        return EXG_ERR_ARG;
     const std::string v = validate(*specs);
     if (!v.empty()) {
         fprintf(stderr, "exg_p2g_momentum_noalloc: %s\n", v.c_str());

@@ -9,7 +9,9 @@
 // reductions on the device so that a whole step can be replayed from a CUDA
 // graph without a host round trip.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <mutex>
 #include <cstdio>
 #include <cstdlib>
 #include <stdexcept>
@@ -3326,9 +3328,11 @@ void launch_batch_plan(Batch &b) {
 namespace {
 constexpr long long kNaNodes = EXG_NOALLOC_MAX_NODES;
 constexpr int kNaCh = CH_MOM_END;  // mass, momentum(3), force(3)
-// [kNaCh * kNaNodes] node sums, 8 bound words, 8 scale words, one word for
-// the largest particle count of a cell, then kNaNodes 32-bit cell counts
+// [kNaCh * kNaNodes] node sums, then 17 header words -- 7 bound words and a
+// flag word (set when an input term is not finite), 8 scale words, one word
+// for the largest particle count of a cell -- then kNaNodes 32-bit cell counts
 constexpr long long kNaWords = kNaCh * kNaNodes + 17 + kNaNodes / 2;
+constexpr int kNaFlagWord = 7;  // header word after the kNaCh bound words
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNaWords];
 
 struct NaArgs {
@@ -3340,9 +3344,22 @@ struct NaArgs {
     unsigned long long *acc;  // device address of g_noalloc_scratch
 };
 
-__global__ void k_na_clear(unsigned long long *acc, long long n) {
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n) acc[i] = 0ull;
+// Zeroes the words this call uses: each channel's first nnodes sums, the 17
+// header words and the count words of the grid's cells (the rest of the
+// array keeps whatever an earlier, larger grid left there and is not read).
+__global__ void k_na_clear(Params P, unsigned long long *acc) {
+    const long long ncells = (long long)P.nc[0] * P.nc[1] * P.nc[2];
+    const long long nsum = kNaCh * P.nnodes, ncnt = (ncells + 1) / 2;
+    const long long n = nsum + 17 + ncnt;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long w;
+        if (i < nsum)
+            w = (i / P.nnodes) * kNaNodes + i % P.nnodes;
+        else
+            w = kNaCh * kNaNodes + (i - nsum);
+        acc[w] = 0ull;
+    }
 }
 
 // particles per cell, and the largest count (the fixed-point range bound
@@ -3391,6 +3408,10 @@ __global__ void k_na_scale(NaArgs a, int stencil_cells) {
         int ex;
         frexp(S, &ex);
         sc = ldexp(1.0, max(-100, min(100, 61 - ex)));
+    } else if (!(S >= 0.0) || S >= 1e300) {
+        // a non-finite (or absurdly large) input term: no fixed-point scale
+        // can hold it, so k_na_finish writes NaN to every output
+        atomicOr(&bnd[kNaFlagWord], 1ull);
     }
     bnd[8 + c] = dbits(sc);
 }
@@ -3457,8 +3478,10 @@ __global__ void k_na_finish(Params P, NaArgs a) {
     int id[3] = {(int)(n % P.nn[0]), (int)((n / P.nn[0]) % P.nn[1]), (int)(n / ((long long)P.nn[0] * P.nn[1]))};
     const long long src = node_index(P, id[0], id[1], id[2]);
     double v[kNaCh];
+    const bool bad = bnd[kNaFlagWord] != 0ull;
     for (int c = 0; c < kNaCh; ++c)
-        v[c] = (double)(long long)a.acc[(long long)c * kNaNodes + src] * (1.0 / bitsd(bnd[8 + c]));
+        v[c] = bad ? __longlong_as_double(0x7ff8000000000000ll)
+                   : (double)(long long)a.acc[(long long)c * kNaNodes + src] * (1.0 / bitsd(bnd[8 + c]));
     const double m = v[CH_M];
     a.mass[n] = m;
     for (int d = 0; d < 3; ++d) {
@@ -3469,7 +3492,10 @@ __global__ void k_na_finish(Params P, NaArgs a) {
     }
 }
 
-unsigned long long *g_na_addr[64] = {};
+// per device: the scratch array's device address, set once under its flag
+constexpr int kNaMaxDevices = 64;
+std::once_flag g_na_once[kNaMaxDevices];
+std::atomic<unsigned long long *> g_na_addr[kNaMaxDevices];
 }  // namespace
 
 // Builds the kernel parameters of a specs (also used by the context).
@@ -3486,26 +3512,27 @@ int noalloc_p2g(const exg_specs *specs, const exg_particle_soa *dev, double *mas
         return EXG_ERR_OVERFLOW;
     }
     int dev_id = 0;
-    if (cudaGetDevice(&dev_id) != cudaSuccess || dev_id < 0 || dev_id >= 64) {
+    if (cudaGetDevice(&dev_id) != cudaSuccess || dev_id < 0 || dev_id >= kNaMaxDevices) {
         err = "exg_p2g_momentum_noalloc: no current CUDA device";
         return EXG_ERR_CUDA;
     }
-    if (!g_na_addr[dev_id]) {
-        // one-time set-up on this device (outside any stream capture): the
-        // device address of the scratch array and the spline tables
-        void *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr) {
-            err = std::string("exg_p2g_momentum_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
-            return EXG_ERR_CUDA;
-        }
-        try {
+    // one-time set-up on this device (outside any stream capture): the
+    // device address of the scratch array and the spline tables.  A failed
+    // set-up throws out of call_once, which leaves the flag unset, so the
+    // next call retries it.
+    try {
+        std::call_once(g_na_once[dev_id], [dev_id] {
+            void *ptr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess || !ptr)
+                throw std::runtime_error(std::string("exg_p2g_momentum_noalloc: cudaGetSymbolAddress failed: ") +
+                                         cudaGetErrorString(e));
             upload_tables_fp64();
-        } catch (const std::exception &ex) {
-            err = ex.what();
-            return EXG_ERR_CUDA;
-        }
-        g_na_addr[dev_id] = reinterpret_cast<unsigned long long *>(ptr);
+            g_na_addr[dev_id].store(reinterpret_cast<unsigned long long *>(ptr), std::memory_order_release);
+        });
+    } catch (const std::exception &ex) {
+        err = ex.what();
+        return EXG_ERR_CUDA;
     }
     NaArgs a;
     a.pos = dev->pos;
@@ -3515,9 +3542,12 @@ int noalloc_p2g(const exg_specs *specs, const exg_particle_soa *dev, double *mas
     a.mass = mass;
     a.vel = vel;
     a.frc = frc;
-    a.acc = g_na_addr[dev_id];
-    const long long nclear = kNaWords;
-    k_na_clear<<<nblocks(nclear), kThreads, 0, stream>>>(a.acc, nclear);
+    a.acc = g_na_addr[dev_id].load(std::memory_order_acquire);
+    {
+        const long long ncells = (long long)P.nc[0] * P.nc[1] * P.nc[2];
+        const long long nclear = kNaCh * P.nnodes + 17 + (ncells + 1) / 2;
+        k_na_clear<<<std::min(nblocks(nclear), 4096), kThreads, 0, stream>>>(P, a.acc);
+    }
     if (a.np > 0) {
         k_na_bounds<<<nblocks(a.np), kThreads, 0, stream>>>(P, a);
         k_na_count<<<nblocks(a.np), kThreads, 0, stream>>>(P, a);

@@ -314,8 +314,40 @@ class Particles:
 
 
 def default_specs() -> Specs:
+    """exg_specs_default through the C ABI (read_mpm_specs defaults)."""
     s = Specs()
     lib().exg_specs_default(C.byref(s))
+    return s
+
+
+def specs_defaults() -> Specs:
+    """The same defaults as exg_specs_default, set in Python without loading
+    libexg.so (the CPU-only legs of the benchmark use it, so that timing the
+    CPU oracle never maps the GPU library): gravity (0, -9.81, 0)
+    (mpm_specs.H:83), num_redist 10, max_steps 1, output times 1e200, order 1
+    on every axis, dt limits [1e-12, 1], CFL 0.1, mass_tolerance 1e-8, FLIP
+    0.95, USL, slip walls with friction 0.1, adiabatic thermal walls, FP64,
+    tile 0 (chosen by the library)."""
+    s = Specs()  # ctypes zero-fills every field, as the C memset does
+    s.gravity[1] = -9.81
+    s.num_redist = 10
+    s.max_steps = 1
+    s.write_output_time = 1e200
+    s.write_diag_output_time = 1e200
+    s.order_scheme = 1
+    for d in range(3):
+        s.order[d] = 1
+        s.bclo[d] = s.bchi[d] = BC_SLIP
+        s.wall_mu_lo[d] = s.wall_mu_hi[d] = 0.1
+        s.bclo_temp[d] = s.bchi_temp[d] = BCT_ADIABATIC
+    s.dt_max_limit = 1e0
+    s.dt_min_limit = 1e-12
+    s.cfl = 0.1
+    s.mass_tolerance = 1e-8
+    s.alpha_pic_flip = 0.95
+    s.stress_update_scheme = 0
+    s.precision = PREC_FP64
+    s.tile = 0
     return s
 
 

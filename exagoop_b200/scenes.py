@@ -58,7 +58,7 @@ def make_particles(pos: np.ndarray, dx, ppc, density, model: int, E=0.0, nu=0.0,
 
 
 def base_specs(plo, phi, ncells, order, precision=nt.PREC_FP64):
-    s = nt.default_specs()
+    s = nt.specs_defaults()
     for d in range(3):
         s.plo[d], s.phi[d], s.ncells[d] = plo[d], phi[d], ncells[d]
         s.gravity[d] = 0.0
@@ -126,7 +126,15 @@ def sphere_collision(n=256, radius=0.2, precision=nt.PREC_FP64, order=3, speed=0
     dx = 1.0 / n
     s = base_specs((0, 0, 0), (1, 1, 1), (n, n, n), order, precision)
     s.alpha_pic_flip = 0.99
-    pos = lattice((0, 0, 0), (1, 1, 1), (dx, dx, dx), (2, 2, 2))
+    # the unit cube's lattice restricted to the spheres' bounding box: the
+    # same points, in the same (x fastest) order, as filtering the whole cube
+    h = dx / 2
+    axes = []
+    for lo_c, hi_c in ((0.3 - radius, 0.7 + radius), (0.5 - radius, 0.5 + radius), (0.5 - radius, 0.5 + radius)):
+        pts = 0.5 * h + h * np.arange(2 * n)
+        axes.append(pts[(pts > lo_c - h) & (pts < hi_c + h)])
+    g = np.meshgrid(*axes, indexing="ij")
+    pos = np.stack([a.ravel(order="F") for a in g])
     c1 = np.array([0.3, 0.5, 0.5])[:, None]
     c2 = np.array([0.7, 0.5, 0.5])[:, None]
     in1 = ((pos - c1) ** 2).sum(0) < radius ** 2

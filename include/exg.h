@@ -373,9 +373,12 @@ int exg_get_stream(exg_ctx *ctx, void **stream);
  *   stream         cudaStream_t the work is issued on (NULL = legacy stream)
  * The first call on a device looks up the scratch array's device address and
  * loads the spline tables there; make that first call before any stream
- * capture begins.  All calls share the one array: it is cleared at the start
- * of every call, and calls that overlap on the GPU (different streams, no
- * ordering between them) race on it. */
+ * capture begins.  All calls share the one array: the part of it a call uses
+ * is cleared at the start of that call, and calls that overlap on the GPU
+ * (different streams, no ordering between them) race on it.  A non-finite
+ * mass, velocity, volume or stress among the phase-0 particles makes every
+ * output value NaN (the call itself still returns EXG_OK: it does not wait
+ * for the GPU). */
 #define EXG_NOALLOC_MAX_NODES 262144
 int exg_p2g_momentum_noalloc(const exg_specs *specs, const exg_particle_soa *dev_particles, double *node_mass,
                              double *node_vel, double *node_frc, void *stream);

@@ -16,23 +16,44 @@ from exagoop_b200 import native as nt
 
 ORACLE_DIR = Path(__file__).resolve().parent
 LIB = ORACLE_DIR / "_build" / "liborc.so"
+LIB_NATIVE = ORACLE_DIR / "_build" / "liborc_native.so"
 REFPIN = ORACLE_DIR / "_ref" / "libexg_refpin.so"
 _lib = None
+_lib_path = None
 
 
-def build(quiet: bool = True):
-    out = subprocess.run(["make", "-C", str(ORACLE_DIR)], capture_output=True, text=True)
+def build(quiet: bool = True, target: str = "all", force: bool = False):
+    cmd = ["make", "-C", str(ORACLE_DIR)] + (["-B"] if force else []) + [target]
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+
+
+def use_native() -> str:
+    """Load the oracle built with -march=native for this host (the timed CPU
+    baseline) instead of the portable x86-64-v2 build.  Builds it on first
+    use; returns a description of the ISA, or of why the portable build is
+    used.  Must run before the first lib() call."""
+    global _lib_path
+    if _lib is not None:
+        return "x86-64-v2 (oracle already loaded)"
+    try:
+        # always rebuilt: a copy built on another host may target another ISA
+        build(target="native", force=True)
+        _lib_path = LIB_NATIVE
+        return "-march=native"
+    except Exception as e:  # no compiler on this host: the portable build
+        return f"x86-64-v2 (native build failed: {str(e).splitlines()[0][:80]})"
 
 
 def lib():
     global _lib
     if _lib is not None:
         return _lib
-    if not LIB.exists():
+    path = _lib_path or LIB
+    if not path.exists():
         build()
-    L = C.CDLL(str(LIB))
+    L = C.CDLL(str(path))
     vp, i, d, i64 = C.c_void_p, C.c_int, C.c_double, C.c_int64
     pd, pi = C.POINTER(C.c_double), C.POINTER(C.c_int)
     sig = {

@@ -40,6 +40,15 @@ def test_struct_sizes_match_header():
     assert g.s.mass_tolerance == 1e-8 and g.s.alpha_pic_flip == 0.95 and g.s.cfl == 0.1
 
 
+def test_python_specs_defaults_match_the_library():
+    # the CPU-only benchmark legs build specs without loading libexg.so; the
+    # Python mirror must equal exg_specs_default byte for byte
+    import ctypes as C
+
+    a, b = nt.default_specs(), nt.specs_defaults()
+    assert C.string_at(C.addressof(a), C.sizeof(a)) == C.string_at(C.addressof(b), C.sizeof(b))
+
+
 INPUTS = """
 # inputs in the reference's key set
 mpm.prob_lo = 0.0 0.0 0.0

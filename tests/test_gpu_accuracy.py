@@ -1,14 +1,26 @@
 """Long-run accuracy: every output field of the FP64 and the mixed-precision
 GPU paths against the FP64 oracle after 1000 steps, relative L2 over all
 particles (the per-field table of the design notes comes from this test:
-run it with -s to print it).  Bounds per workload: the FP64 path within
-1e-8; the mixed path within 1e-4 in velocity and stress on the elastic
-workloads and within 1e-5 in temperature and 1e-4 in heat flux on the
-thermal ones (nodal temperatures are held relative to a reference
-temperature, so FP32 resolves millikelvin differences at 300 K); on the dam
-break the splashing flow against slip walls grows rounding by ~1e5 over 1000
-steps (the FP64 path's own 1e-16 reaches 1e-11), so its mixed bound is the
-measured 5e-2."""
+run it with -s to print it).
+
+FP64 bound.  The GPU's nodal sums are exact fixed-point sums, the oracle's
+are sequential FP64 sums: the two differ by rounding (~1e-16) every step,
+and a workload amplifies such differences at its own rate (reflections at
+walls and obstacles are discontinuous in position).  The test measures that
+rate directly: the oracle against itself with every initial position and
+velocity component moved by one ulp.  The FP64 GPU path must stay within
+max(1e-10, 10 x that self-divergence) in every field; on the workloads whose
+self-divergence stays below 1e-11 (the elastic spheres, the dam break) that
+is the 1e-10 of the parity tests.  Measured self-divergence after 1000 steps
+(relative L2): twisted column stress 5e-10 (velocity-ulp alone 1e-9), heated
+block velocity 3e-9, dam break stress 2e-12, spheres stress 3e-14.
+
+Mixed bounds per workload: 1e-4 in velocity and stress on the elastic
+workloads, 1e-5 in temperature and 1e-4 in heat flux on the thermal ones
+(nodal temperatures are held relative to a reference temperature, so FP32
+resolves millikelvin differences at 300 K); on the dam break the splashing
+flow against slip walls grows rounding by ~1e5 over 1000 steps, so its mixed
+bound is the measured 5e-2."""
 import json
 import os
 
@@ -55,16 +67,31 @@ MIXED = {"spheres": (1e-4, 1e-4), "twisted_column": (1e-4, 1e-4), "heated_block"
          "dam_break": (5e-3, 5e-2)}
 
 
-@pytest.mark.parametrize("name", ["spheres", "dam_break", "twisted_column", "heated_block"])
-def test_thousand_steps_against_oracle(name):
-    s, p, phi = workload(name)
+def oracle_1000(s, p, phi):
     o = orc.Oracle(s, threads=os.cpu_count() or 1)
     o.upload(p)
     if phi is not None:
         o.set_levelset(0, phi)
     o.init_internal_forces()
     assert o.step(1000) == 0
-    r = o.download()
+    return o.download()
+
+
+@pytest.mark.parametrize("name", ["spheres", "dam_break", "twisted_column", "heated_block"])
+def test_thousand_steps_against_oracle(name):
+    s, p, phi = workload(name)
+    r = oracle_1000(s, p, phi)
+    # the workload's own amplification of rounding: every initial position
+    # and velocity component one ulp away (up or down, seeded)
+    q = p.copy()
+    rng = np.random.default_rng(1)
+
+    def ulp(a):
+        return np.where(rng.random(a.shape) < 0.5, np.nextafter(a, -np.inf), np.nextafter(a, np.inf))
+
+    q.pos[:] = ulp(q.pos)
+    q.rdata[nt.R_VEL:nt.R_VEL + 3] = ulp(q.rdata[nt.R_VEL:nt.R_VEL + 3])
+    self_div = l2_errors(oracle_1000(s, q, phi), r, bool(s.use_temp))
     res = {}
     for prec, tag in [(nt.PREC_FP64, "fp64"), (nt.PREC_MIXED, "mixed")]:
         s2 = s.copy()
@@ -76,8 +103,10 @@ def test_thousand_steps_against_oracle(name):
         ctx.Initialise_Internal_Forces()
         ctx.step(1000)
         res[tag] = l2_errors(ctx.download(), r, bool(s.use_temp))
-    print(json.dumps({"workload": name, "particles": int(p.n), **res}))
-    assert max(res["fp64"].values()) < 1e-8, res["fp64"]
+    print(json.dumps({"workload": name, "particles": int(p.n), **res, "oracle_one_ulp_self_divergence": self_div}))
+    for k, e in res["fp64"].items():
+        bound = max(1e-10, 10.0 * self_div.get(k, 0.0))
+        assert e < bound, (k, e, bound, self_div)
     bv, bs = MIXED[name]
     assert res["mixed"]["vel"] < bv and res["mixed"]["stress"] < bs, res["mixed"]
     if s.use_temp:
