@@ -261,13 +261,17 @@ def measure(args, config, rank, world, dev, with_e2e, with_accuracy):
     ms, n_total = job_reduce(ms, p.n, world)
     value = n_total * args.steps / (ms * 1e-3)
     stages = stage_times(ctx, max(3, min(10, args.steps)))
+    variants = ctx.variants()
     w = 4 if prec == nt.PREC_MIXED else 8
     peak, peak_kind = read_peaks()
     out = {"name": name, "particles": int(p.n), "grid": list(s.ncells), "order": int(s.order[0]),
            "tile": ctx.tile(), "value": value, "ms": ms, "clocks": clk.summary(),
            "stages_ms": {k: round(v, 4) for k, v in stages.items()},
            "roofline": roofline(stages, w, p.n, name, peak, peak_kind),
-           "musl": int(s.stress_update_scheme != 0), "n_total": n_total}
+           "musl": int(s.stress_update_scheme != 0), "n_total": n_total,
+           "variants": {"p2g": variants["p2g"], "g2p": variants["g2p"],
+                        "p2g_ms": [round(x, 4) for x in variants["p2g_ms"]],
+                        "g2p_ms": [round(x, 4) for x in variants["g2p_ms"]]}}
     if with_e2e:
         # end to end through the C ABI with host buffers in page-locked
         # memory: upload, steps, download into a pinned result set
@@ -321,7 +325,8 @@ def run_ours(args, rank, world):
         "data": "synthetic (seeded lattice)",
         "config": {"workload": head["name"], "particles": head["particles"], "grid": head["grid"],
                    "order": head["order"], "precision": args.precision, "tile": head["tile"],
-                   "l2": "inputs larger than L2", "parallelism": f"replicas{world}" if world > 1 else "single"},
+                   "l2": "inputs larger than L2", "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "autotuned_variants": head["variants"]},
         "clocks": head["clocks"],
         "e2e": head["e2e"],
         "gpu_launches": launches,
@@ -340,25 +345,43 @@ def run_ours(args, rank, world):
             "value": sec["value"], "ms_per_step": sec["ms"] / args.steps, "stages_ms": sec["stages_ms"],
             "roofline": sec["roofline"], "fp64_value": sec.get("fp64_value"),
             "fp64_stages_ms": sec.get("fp64_stages_ms"), "mixed_over_fp64": sec.get("mixed_over_fp64"),
-            "clocks": sec["clocks"]}
+            "clocks": sec["clocks"], "autotuned_variants": sec["variants"]}
     return line
+
+
+BATCH_SEED = 2024
+
+
+def batch_share(n_scenes, rank, world):
+    """This rank's scenes of the one seeded batch: the scenes are dealt to
+    the ranks by particle count (scenes.partition_scenes), every rank
+    computing the same partition without communication."""
+    from exagoop_b200 import scenes
+    counts = scenes.batched_scene_particle_counts(n_scenes=n_scenes, seed=BATCH_SEED)
+    parts = scenes.partition_scenes(counts, world)
+    return parts[rank], counts
 
 
 def run_batch(args, rank, world):
     """The batched uneven scenes: 64 independent dam breaks (grid sides from
     {32,48,64,96,128}, fill fractions in [0.1,0.4], seeded) advanced by
-    exg_batch_step, one launch per hot kernel over all scenes."""
+    exg_batch_step, one launch per hot kernel over all scenes.  With N ranks
+    the same 64 scenes are partitioned over the GPUs by particle count
+    (strong scaling: the total work is fixed); no collective is on the data
+    path."""
     import torch
     from exagoop_b200 import native as nt, scenes
 
     torch.cuda.set_device(rank % torch.cuda.device_count())
     dev = torch.cuda.current_device()
     prec = nt.PREC_MIXED if args.precision == "mixed" else nt.PREC_FP64
-    seed = 2024 + rank
-    specs = scenes.batched_specs(n_scenes=args.scenes, seed=seed, precision=prec)
+    mine, counts = batch_share(args.scenes, rank, world)
+    seed = BATCH_SEED
+    specs = scenes.batched_specs(n_scenes=args.scenes, seed=seed, precision=prec, only=set(mine))
     b = nt.Batch(specs, device=dev)
     total = 0
-    for sc, (s, p) in zip(b.scenes, scenes.batched_dam_breaks(n_scenes=args.scenes, seed=seed, precision=prec)):
+    for sc, (s, p) in zip(b.scenes, scenes.batched_dam_breaks(n_scenes=args.scenes, seed=seed, precision=prec,
+                                                              only=set(mine))):
         sc.upload(p)
         sc.Initialise_Internal_Forces()
         total += p.n
@@ -373,13 +396,14 @@ def run_batch(args, rank, world):
     sides = [int(s.ncells[0]) for s in specs]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32+f64" if prec == nt.PREC_MIXED else "f64",
         "data": "synthetic (seeded lattices, jittered)",
-        "config": {"workload": f"batched_dam_breaks_{len(specs)}_scenes", "particles": total_all,
-                   "particles_per_gpu": total, "grid_sides": sides, "order": 2, "precision": args.precision,
-                   "tile": 8, "l2": "inputs larger than L2",
-                   "parallelism": f"replicas{world}" if world > 1 else "single"},
+        "config": {"workload": f"batched_dam_breaks_{args.scenes}_scenes", "particles": total_all,
+                   "particles_rank0": total, "scenes_rank0": len(mine), "grid_sides_rank0": sides, "order": 2,
+                   "precision": args.precision, "tile": 8, "l2": "inputs larger than L2",
+                   "parallelism": f"scenes partitioned over {world} GPUs by particle count" if world > 1
+                   else "single"},
         "clocks": clk.summary(),
         "e2e": None,
         # per scene: dt_finalize, keys, tile_scan, touched, scatter,

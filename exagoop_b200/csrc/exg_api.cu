@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <thread>
 #include <tuple>
@@ -511,15 +512,19 @@ void enqueue_step(Ctx &c) {
                                 cudaMemcpyDeviceToDevice, c.stream));
     launch_dt_finalize(c, true);
     if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[0], c.stream));
+    nvtxRangePushA("step: sort (Redistribute)");
     launch_keys(c);
     launch_sort_rest(c, true);
+    nvtxRangePop();
     if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[1], c.stream));
     launch_scales_from(c, c.bounds_cur);
     const bool th = c.specs.use_temp != 0;
     const bool musl = c.specs.stress_update_scheme != 0;
     const int tflags = th ? (PF_TEMP | PF_SRC) : 0;
     const int udfT = has_udf_temp(c) ? 1 : 0;
+    nvtxRangePushA("step: P2G");
     DISPATCH(launch_p2g, c, PF_MASS | PF_VEL | PF_FORCE | tflags);
+    nvtxRangePop();
     if (c.timing) EXG_CUDA_OK(cudaEventRecord(c.ev[2], c.stream));
     DISPATCH(launch_nodes, c, NM_FUSED, PF_MASS | PF_VEL | PF_FORCE | tflags, false);
     if (th) {
@@ -809,6 +814,7 @@ int exg_set_levelset(exg_ctx *ctx, int body, const double *phi) {
 }
 
 int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
+    EXG_RANGE("exg_particles_upload");
     if (!ctx || !p || p->np < 0) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     if (p->np > (long long)0x7fffffff) return fail(ctx, EXG_ERR_ARG, "more than 2^31-1 particles");
@@ -951,6 +957,7 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
 }
 
 int exg_particles_download(exg_ctx *ctx, exg_particle_soa *p) {
+    EXG_RANGE("exg_particles_download");
     if (!ctx || !p) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     if (p->np != c.np) return fail(ctx, EXG_ERR_ARG, "np mismatch");
@@ -1043,6 +1050,7 @@ int exg_nodes_download(exg_ctx *ctx, int comp, double *out) {
 
 // ----------------------------------------------------- L5 step functions
 int exg_redistribute(exg_ctx *ctx) {
+    EXG_RANGE("Redistribute");
     if (!ctx) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     EXG_TRY(ctx, {
@@ -1059,6 +1067,7 @@ int exg_redistribute(exg_ctx *ctx) {
 }
 
 int exg_calculate_time_step(exg_ctx *ctx, double *dt) {
+    EXG_RANGE("Calculate_time_step");
     if (!ctx || !dt) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     EXG_TRY(ctx, {
@@ -1077,6 +1086,7 @@ int exg_reset_nodaldata(exg_ctx *ctx) {
 }
 
 int exg_p2g_momentum(exg_ctx *ctx, int update_mass, int update_vel, int update_forces) {
+    EXG_RANGE("P2G_Momentum");
     if (!ctx) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     if (c.np == 0) return fail(ctx, EXG_ERR_NOT_READY, "no particles");
@@ -1110,6 +1120,7 @@ int exg_nodal_time_update_momentum(exg_ctx *ctx, double dt) {
 }
 
 int exg_apply_nodal_bcs(exg_ctx *ctx, double dt, double time) {
+    EXG_RANGE("Apply_Nodal_BCs");
     if (!ctx) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     (void)dt;
@@ -1121,6 +1132,7 @@ int exg_apply_nodal_bcs(exg_ctx *ctx, double dt, double time) {
 }
 
 int exg_g2p_momentum(exg_ctx *ctx, int update_vel, int update_strainrate, double dt) {
+    EXG_RANGE("G2P_Momentum");
     if (!ctx) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     EXG_TRY(ctx, {
@@ -1131,6 +1143,7 @@ int exg_g2p_momentum(exg_ctx *ctx, int update_vel, int update_strainrate, double
 }
 
 int exg_update_mp_positions(exg_ctx *ctx, double dt) {
+    EXG_RANGE("Update_MP_Positions");
     if (!ctx) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     EXG_TRY(ctx, {
@@ -1142,6 +1155,7 @@ int exg_update_mp_positions(exg_ctx *ctx, double dt) {
 }
 
 int exg_update_mp_volume(exg_ctx *ctx) {
+    EXG_RANGE("Update_MP_Volume");
     if (!ctx) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     EXG_TRY(ctx, {
@@ -1152,6 +1166,7 @@ int exg_update_mp_volume(exg_ctx *ctx) {
 }
 
 int exg_calculate_mp_stress_strain(exg_ctx *ctx, double time, double dt) {
+    EXG_RANGE("Calculate_MP_Stress_Strain");
     if (!ctx) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     EXG_TRY(ctx, {
@@ -1162,6 +1177,7 @@ int exg_calculate_mp_stress_strain(exg_ctx *ctx, double time, double dt) {
 }
 
 int exg_init_internal_forces(exg_ctx *ctx) {
+    EXG_RANGE("Initialise_Internal_Forces");
     if (!ctx) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     int rc = exg_p2g_momentum(ctx, 1, 1, 1);
@@ -1197,6 +1213,7 @@ static int need_temp(exg_ctx *ctx) {
 }
 
 int exg_p2g_temperature(exg_ctx *ctx, int reset, int update_temp, int update_source) {
+    EXG_RANGE("P2G_Temperature");
     if (!ctx) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     if (int rc = need_temp(ctx)) return rc;
@@ -1267,11 +1284,155 @@ int exg_g2p_temperature(exg_ctx *ctx, int update_temperature, int update_heatflu
 }
 
 // ------------------------------------------------------------ fused step
+}  // extern "C"
+
+namespace {
+// Tuning choices shared by the contexts of one process: (device, precision,
+// order, tile, lean G2P, particle-count decade) -> (p2g, g2p) variants.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int, int>, std::pair<int, int>> g_tune_cache;
+
+std::tuple<int, int, int, int, int, int> tune_key(const Ctx &c) {
+    const int decade = c.np > 0 ? (int)std::floor(std::log10((double)c.np)) : 0;
+    return {c.device, c.precision, c.P.uniform_order, c.P.T, g2p_lean(c) ? 1 : 0, decade};
+}
+
+// Mean device ms of `reps` launches of fn() after one untimed launch.
+template <class F>
+double time_launches(Ctx &c, int reps, F fn) {
+    cudaEvent_t e0, e1;
+    EXG_CUDA_OK(cudaEventCreate(&e0));
+    EXG_CUDA_OK(cudaEventCreate(&e1));
+    fn();
+    EXG_CUDA_OK(cudaEventRecord(e0, c.stream));
+    for (int r = 0; r < reps; ++r) fn();
+    EXG_CUDA_OK(cudaEventRecord(e1, c.stream));
+    EXG_CUDA_OK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    EXG_CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return (double)ms / reps;
+}
+
+// Times every P2G and G2P variant on the current particles.  The P2G writes
+// only the staging blocks; the nodal pass that follows rebuilds the nodal
+// fields the G2P reads; the G2P writes only the re-order target storage and
+// the control block's reductions, which are saved before and restored after.
+void autotune_impl(Ctx &c) {
+    Ctl *saved = nullptr;
+    EXG_CUDA_OK(cudaMalloc(&saved, sizeof(Ctl)));
+    EXG_CUDA_OK(cudaMemcpyAsync(saved, c.ctl, sizeof(Ctl), cudaMemcpyDeviceToDevice, c.stream));
+    const int p2g0 = c.p2g_var, g2p0 = c.g2p_var;
+    try {
+        EXG_CUDA_OK(cudaMemsetAsync(&c.ctl->maxppc, 0, sizeof(int), c.stream));
+        do_sort(c, true);
+        launch_reset_accum(c, c.bounds2, c.dtmin2);
+        DISPATCH(launch_state_reduce, c, c.bounds2, c.dtmin2);
+        const int flags = PF_MASS | PF_VEL | PF_FORCE;
+        for (int v = 0; v < EXG_NUM_VARIANTS; ++v) {
+            c.p2g_var = v;
+            c.tune_ms[0][v] = time_launches(c, 3, [&] {
+                launch_scales_from(c, c.bounds2);  // also resets the P2G tile counter
+                DISPATCH(launch_p2g, c, flags);
+            });
+        }
+        DISPATCH(launch_nodes, c, NM_FUSED, flags, false);
+        for (int v = 0; v < EXG_NUM_VARIANTS; ++v) {
+            c.g2p_var = v;
+            c.tune_ms[1][v] = time_launches(c, 3, [&] {
+                EXG_CUDA_OK(cudaMemsetAsync(&c.ctl->next_g2p, 0, sizeof(int), c.stream));
+                DISPATCH(launch_g2p_fused, c, GM_FULL);
+            });
+        }
+    } catch (...) {
+        c.p2g_var = p2g0;
+        c.g2p_var = g2p0;
+        cudaMemcpyAsync(c.ctl, saved, sizeof(Ctl), cudaMemcpyDeviceToDevice, c.stream);
+        cudaStreamSynchronize(c.stream);
+        cudaFree(saved);
+        throw;
+    }
+    EXG_CUDA_OK(cudaMemcpyAsync(c.ctl, saved, sizeof(Ctl), cudaMemcpyDeviceToDevice, c.stream));
+    EXG_CUDA_OK(cudaStreamSynchronize(c.stream));
+    EXG_CUDA_OK(cudaFree(saved));
+    c.p2g_var = (int)(std::min_element(c.tune_ms[0], c.tune_ms[0] + EXG_NUM_VARIANTS) - c.tune_ms[0]);
+    c.g2p_var = (int)(std::min_element(c.tune_ms[1], c.tune_ms[1] + EXG_NUM_VARIANTS) - c.tune_ms[1]);
+    c.parts_sorted = false;
+    c.tuned = true;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[tune_key(c)] = {c.p2g_var, c.g2p_var};
+}
+
+// The choice for this context: the process cache when it holds one for this
+// kind of context, otherwise a tuning run.  Graphs captured with other
+// variants are dropped.
+void ensure_tuned(Ctx &c) {
+    if (c.tuned) return;
+    const int p0 = c.p2g_var, g0 = c.g2p_var;
+    bool hit = false;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(tune_key(c));
+        if (it != g_tune_cache.end()) {
+            c.p2g_var = it->second.first;
+            c.g2p_var = it->second.second;
+            hit = true;
+        }
+    }
+    if (hit)
+        c.tuned = true;
+    else
+        autotune_impl(c);
+    if (c.p2g_var != p0 || c.g2p_var != g0) drop_graphs(c);
+}
+}  // namespace
+
+extern "C" {
+
+int exg_autotune(exg_ctx *ctx) {
+    EXG_RANGE("exg_autotune");
+    if (!ctx) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    if (c.np == 0) return fail(ctx, EXG_ERR_NOT_READY, "no particles");
+    EXG_TRY(ctx, {
+        const int p0 = c.p2g_var, g0 = c.g2p_var;
+        autotune_impl(c);
+        if (c.p2g_var != p0 || c.g2p_var != g0) drop_graphs(c);
+    });
+    return EXG_OK;
+}
+
+int exg_set_variants(exg_ctx *ctx, int p2g, int g2p) {
+    if (!ctx || p2g < -1 || p2g >= EXG_NUM_VARIANTS || g2p < -1 || g2p >= EXG_NUM_VARIANTS) return EXG_ERR_ARG;
+    Ctx &c = ctx->c;
+    const int p0 = c.p2g_var, g0 = c.g2p_var;
+    if (p2g >= 0) c.p2g_var = p2g;
+    if (g2p >= 0) c.g2p_var = g2p;
+    c.tuned = true;
+    EXG_TRY(ctx, if (c.p2g_var != p0 || c.g2p_var != g0) drop_graphs(c));
+    return EXG_OK;
+}
+
+int exg_get_variants(exg_ctx *ctx, int *p2g, int *g2p, double *p2g_ms, double *g2p_ms) {
+    if (!ctx) return EXG_ERR_ARG;
+    const Ctx &c = ctx->c;
+    if (p2g) *p2g = c.p2g_var;
+    if (g2p) *g2p = c.g2p_var;
+    for (int v = 0; v < EXG_NUM_VARIANTS; ++v) {
+        if (p2g_ms) p2g_ms[v] = c.tune_ms[0][v];
+        if (g2p_ms) g2p_ms[v] = c.tune_ms[1][v];
+    }
+    return EXG_OK;
+}
+
 int exg_step(exg_ctx *ctx, int nsteps) {
+    EXG_RANGE("exg_step");
     if (!ctx || nsteps < 0) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     if (c.np == 0) return fail(ctx, EXG_ERR_NOT_READY, "no particles");
     EXG_TRY(ctx, {
+        if (c.specs.autotune && nsteps > 0) ensure_tuned(c);
         if (c.reduce_stale) do_reduce(c);
         const bool host_dep = has_udf(c) || (c.specs.use_temp && has_udf_temp(c));
         const bool use_graph = !host_dep && !c.timing && std::getenv("EXG_NO_GRAPH") == nullptr;
@@ -1352,6 +1513,7 @@ int exg_set_time(exg_ctx *ctx, double time, int64_t steps) {
 }
 
 int exg_diagnostics(exg_ctx *ctx, exg_diag *out) {
+    EXG_RANGE("Do_All_Diagnostics");
     if (!ctx || !out) return EXG_ERR_ARG;
     Ctx &c = ctx->c;
     EXG_TRY(ctx, {

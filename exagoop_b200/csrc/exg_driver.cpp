@@ -58,16 +58,23 @@ void mkdirs(const std::string &path) {
     }
 }
 
-// One line per particle: x y z, the EXG_NREAL real fields in realData
-// order, the EXG_NINT int fields; five header lines (count, 0, 0, number of
-// real fields, number of int fields).
-void write_ascii(const std::string &file, const exg_particle_soa &p) {
+// One line per particle: x y z, the real fields in realData order, the
+// int fields in intData order (the layout the reference's post-processing
+// reads: column = realData index + 3 in 3-D, e.g. build_field_dict in
+// Tests/1D_Heat_Conduction/PostProcess/validate.py:40-58 and vx in column 4
+// in Tests/1D_Axial_Bar_Vibration/PostProcess/Calculate_Error.py:74-86),
+// after five header lines: particle count, real and int field counts of the
+// particle struct, and two zero counts of extra runtime fields.  The real
+// field count is realData::count of the reference's build: 53 with
+// mpm.use_temp, 46 (no thermal fields) without.
+void write_ascii(const std::string &file, const exg_particle_soa &p, int use_temp) {
+    const int nreal = use_temp ? EXG_NREAL : EXG_R_TEMPERATURE;
     std::ofstream f(file);
-    f << p.np << "\n0\n0\n" << EXG_NREAL << "\n" << EXG_NINT << "\n";
+    f << p.np << "\n" << nreal << "\n" << EXG_NINT << "\n0\n0\n";
     f << std::setprecision(12);
     for (int64_t i = 0; i < p.np; ++i) {
         for (int d = 0; d < 3; ++d) f << p.pos[d * p.np + i] << ' ';
-        for (int k = 0; k < EXG_NREAL; ++k) f << p.rdata[(size_t)k * p.np + i] << ' ';
+        for (int k = 0; k < nreal; ++k) f << p.rdata[(size_t)k * p.np + i] << ' ';
         for (int k = 0; k < EXG_NINT; ++k) f << p.idata[(size_t)k * p.np + i] << (k + 1 < EXG_NINT ? ' ' : '\n');
     }
 }
@@ -128,11 +135,14 @@ int main(int argc, char **argv) {
     const int digits = std::atoi(get_str(in, "mpm.num_of_digits_in_filenames", "6").c_str());
     auto dump = [&](double t) {
         if (!write_ascii_on) return;
-        mkdirs(ascii_dir);
         check(exg_particles_download(ctx, &parts), ctx, "exg_particles_download");
         std::ostringstream oss;
         oss << ascii_dir << ascii_prefix << "_t" << std::fixed << std::setprecision(digits) << t;
-        write_ascii(oss.str(), parts);
+        // the prefix may hold folders of its own (the reference's
+        // pre-processor writes "<tag>/matpnt")
+        const std::string path = oss.str();
+        mkdirs(path.substr(0, path.find_last_of('/') + 1));
+        write_ascii(path, parts, s.use_temp);
     };
 
     int steps = 0;

@@ -279,6 +279,7 @@ void exg_specs_default(exg_specs *s) {
     }
     s->precision = EXG_PREC_FP64;
     s->tile = 0;
+    s->autotune = 1;
 }
 
 int exg_specs_from_inputs(const exg_inputs *cin, exg_specs *s, char *errbuf, size_t errlen) {
@@ -458,6 +459,7 @@ int exg_specs_from_inputs(const exg_inputs *cin, exg_specs *s, char *errbuf, siz
     else
         return bad("exg.precision must be fp64 or mixed");
     r.integer("exg.tile", s->tile);
+    r.integer("exg.autotune", s->autotune);
     if (!r.err.empty()) return bad(r.err);
     return EXG_OK;
 }

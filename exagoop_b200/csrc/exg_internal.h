@@ -2,11 +2,25 @@
 // launchers shared by the translation units of libexg.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <string>
 #include <vector>
 #include "exg_common.cuh"
 
 namespace exg {
+
+// NVTX range over a scope (the counterpart of the reference's BL_PROFILE
+// regions, e.g. MPMParticleContainer::updateVolume in
+// mpm_particle_timestep.cpp:133): the entry points and the stages of a step
+// show up by name in Nsight timelines.  Header-only NVTX3: without a
+// profiler attached each push/pop is a no-op call.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+#define EXG_RANGE(name) ::exg::NvtxRange exg_nvtx_range_(name)
 
 enum P2GFlags { PF_MASS = 1, PF_VEL = 2, PF_FORCE = 4, PF_TEMP = 8, PF_SRC = 16 };
 // Nodal kernel modes.
@@ -170,6 +184,12 @@ struct Ctx {
     cudaEvent_t ev[6] = {};
     double stage_ms[5] = {};
     bool timing = false;
+    // launch variants of the P2G and fused G2P kernels (rows per pass and
+    // threads per block; every variant gives bit-identical results), chosen
+    // by the autotuner (exg_autotune) or set by exg_set_variants
+    int p2g_var = 0, g2p_var = 0;
+    bool tuned = false;
+    double tune_ms[2][4] = {};   // measured ms of each variant: [p2g/g2p][variant]
 
     template <class R>
     Parts<R> &A() { return *reinterpret_cast<Parts<R> *>(pa); }

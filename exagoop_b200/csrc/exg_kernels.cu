@@ -804,18 +804,44 @@ constexpr int kCellThreads = 128;
 // quadratic accumulators fit 128 registers; one 512-thread block per SM (a
 // thread per bin of an 8^3 tile) measured fastest on the dam break, ahead
 // of 2 x 256, 4 x 128 and 1 x 256 with 255 registers.
+// Launch variants of the factorized momentum P2G (uniform quadratic and
+// cubic): rows per pass, threads per block and the minimum resident blocks
+// per SM (the register cap).  Variant 0 is the default; the autotuner
+// measures all kP2GVariants on the context's own particles and keeps the
+// fastest.  FP32 cubic holds a 4 x 4 slice (112 accumulators) at 256 or 384
+// threads, or half a slice at 512; FP64 holds one or two rows.
+constexpr int kP2GVariants = 3;
+static_assert(kP2GVariants == EXG_NUM_VARIANTS, "the launchers dispatch EXG_NUM_VARIANTS P2G variants");
+// rows per pass, threads per block, minimum blocks per SM
+//   FP32 cubic:     (4, 256, 1)  (2, 512, 1)  (2, 256, 2)
+//   FP32 quadratic: (3, 512, 1)  (3, 256, 2)  (1, 256, 2)
+//   FP64 cubic:     (1, 512, 1)  (2, 256, 1)  (1, 256, 1)
+//   FP64 quadratic: (1, 512, 1)  (3, 256, 1)  (1, 256, 1)
+template <class R, int ORD, int V>
+struct P2GVar {
+    static constexpr int K = (sizeof(R) == 4 ? 0 : 2) + (ORD == 3 ? 0 : 1);
+    static constexpr int TAB[4][3][3] = {{{4, 256, 1}, {2, 512, 1}, {2, 256, 2}},
+                                         {{3, 512, 1}, {3, 256, 2}, {1, 256, 2}},
+                                         {{1, 512, 1}, {2, 256, 1}, {1, 256, 1}},
+                                         {{1, 512, 1}, {3, 256, 1}, {1, 256, 1}}};
+    static constexpr int ROWS = TAB[K][V][0], THREADS = TAB[K][V][1], MINB = TAB[K][V][2];
+};
+
 template <class R, int ORD, bool THERM>
 struct P2GCfg {
     static constexpr int W = P2GStc<ORD>::W;
+    static constexpr bool FACT = (ORD == 2 || ORD == 3) && !THERM;
     // y rows of the stencil slice accumulated per pass (register budget)
-    static constexpr int ROWS = (sizeof(R) == 8) ? 1 : (THERM ? (W == 4 ? 2 : 1) : W);
+    static constexpr int ROWS = FACT ? P2GVar<R, (FACT ? ORD : 2), 0>::ROWS
+                                     : ((sizeof(R) == 8) ? 1 : (THERM ? (W == 4 ? 2 : 1) : W));
     // quadratic momentum: the three z-slices of a bin's window go to three
     // adjacent threads (FP32: one pass each, FP64: one pass per y row)
     // instead of one thread walking them in turn, so the bin's particles are
     // read by the three together and stay in L1
     static constexpr bool SPLIT = EXG_P2G_SPLIT && ORD == 2 && !THERM;
-    static constexpr int THREADS = (ORD == 2) ? EXG_P2G2_THREADS : kCellThreads;
-    static constexpr int MINB = (ORD == 2) ? EXG_P2G2_MINB : 1;
+    static constexpr int THREADS = FACT ? P2GVar<R, (FACT ? ORD : 2), 0>::THREADS
+                                        : ((ORD == 2) ? EXG_P2G2_THREADS : kCellThreads);
+    static constexpr int MINB = FACT ? P2GVar<R, (FACT ? ORD : 2), 0>::MINB : ((ORD == 2) ? EXG_P2G2_MINB : 1);
 };
 
 // One tile of the per-cell P2G into its fixed-point node block (zeroed by
@@ -1001,7 +1027,266 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
     }
 }
 
-// ---------------------------------------------------------------- nodal BCs
+// ---------------------------------------------------------------- K2 factorized P2G
+// Momentum P2G of uniform quadratic (nearest-node bins) and cubic (cells)
+// B-splines with the deposit of deposit_onto_grid_momentum
+// (mpm_particle_grid_ops.cpp:484-577) in factorized form.  With
+// N = wx wy wz and grad N = (dwx wy wz, wx dwy wz, wx wy dwz), s_dj =
+// -V sigma_dj and b_d = m g_d (+ f_ext,d inside the force slab):
+//   m N          = wx (wy (m wz))
+//   m v_d N      = wx (wy (m v_d wz))
+//   f_d          = wx (wy A_d + dwy B_d) + dwx (wy C_d),
+//   A_d = b_d wz + s_d2 dwz,  B_d = s_d1 wz,  C_d = s_d0 wz,
+// so a node costs 4 packed FP32 FMAs and 2 scalar ones (10 FMAs in FP64)
+// instead of forming N and grad N.  Tasks are (cell, z-slice, row group):
+// the W x NPASS tasks of a cell sit in adjacent threads, read the cell's
+// particles together (they stay in L1) and each accumulates ROWS rows of its
+// slice in registers, then adds the cell's sums to the tile's fixed-point
+// node block.  Every node's register sum runs over the cell's particles in
+// storage order with the same expression whatever ROWS and the block size
+// are, so all launch variants give bit-identical results.
+template <class R, int ROWS>
+struct FactRow;  // row terms (wy and dwy folded into the z-level terms)
+template <int ROWS>
+struct FactRow<float, ROWS> {
+    float2 mp0, p12, a01, c01;
+    float a2, c2;
+};
+template <int ROWS>
+struct FactRow<double, ROWS> {
+    double m, p[3], a[3], c[3];
+};
+
+template <class R>
+struct FactAcc;
+template <>
+struct FactAcc<float> {
+    float2 mp0, p12, f01;
+    float f2;
+    __device__ __forceinline__ void zero() {
+        mp0 = p12 = f01 = make_float2(0.f, 0.f);
+        f2 = 0.f;
+    }
+    __device__ __forceinline__ void add(const FactRow<float, 1> &r, float2 wxx, float2 dxx) {
+        mp0 = __ffma2_rn(wxx, r.mp0, mp0);
+        p12 = __ffma2_rn(wxx, r.p12, p12);
+        f01 = __ffma2_rn(wxx, r.a01, f01);
+        f01 = __ffma2_rn(dxx, r.c01, f01);
+        f2 = fmaf(wxx.x, r.a2, f2);
+        f2 = fmaf(dxx.x, r.c2, f2);
+    }
+    __device__ __forceinline__ float get(int ch) const {
+        switch (ch) {
+            case CH_M: return mp0.x;
+            case CH_P: return mp0.y;
+            case CH_P + 1: return p12.x;
+            case CH_P + 2: return p12.y;
+            case CH_F: return f01.x;
+            case CH_F + 1: return f01.y;
+            default: return f2;
+        }
+    }
+};
+template <>
+struct FactAcc<double> {
+    double c[CH_MOM_END];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < CH_MOM_END; ++i) c[i] = 0.0;
+    }
+    __device__ __forceinline__ void add(const FactRow<double, 1> &r, double wx, double dwx) {
+        c[CH_M] = fma(wx, r.m, c[CH_M]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) c[CH_P + d] = fma(wx, r.p[d], c[CH_P + d]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            c[CH_F + d] = fma(wx, r.a[d], c[CH_F + d]);
+            c[CH_F + d] = fma(dwx, r.c[d], c[CH_F + d]);
+        }
+    }
+    __device__ __forceinline__ double get(int ch) const { return c[ch]; }
+};
+
+// z-level terms of one particle for one node plane
+template <class R>
+struct FactZ {
+    R m, p[3], a[3], b[3], c[3];
+};
+
+template <class R>
+__device__ __forceinline__ FactRow<R, 1> fact_row(const FactZ<R> &z, R wy, R dwy) {
+    FactRow<R, 1> r;
+    if constexpr (sizeof(R) == 4) {
+        const float2 wyy = make_float2(wy, wy), dyy = make_float2(dwy, dwy);
+        r.mp0 = __fmul2_rn(wyy, make_float2(z.m, z.p[0]));
+        r.p12 = __fmul2_rn(wyy, make_float2(z.p[1], z.p[2]));
+        r.a01 = __ffma2_rn(dyy, make_float2(z.b[0], z.b[1]), __fmul2_rn(wyy, make_float2(z.a[0], z.a[1])));
+        r.a2 = fmaf(dwy, z.b[2], wy * z.a[2]);
+        r.c01 = __fmul2_rn(wyy, make_float2(z.c[0], z.c[1]));
+        r.c2 = wy * z.c[2];
+    } else {
+        r.m = wy * z.m;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            r.p[d] = wy * z.p[d];
+            r.a[d] = fma(dwy, z.b[d], wy * z.a[d]);
+            r.c[d] = wy * z.c[d];
+        }
+    }
+    return r;
+}
+
+template <class R, int ORD, int ROWS>
+__device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned *acc_lo, int *acc_hi, const Params &P,
+                                              const Parts<R> &A, const int *active, const int *start,
+                                              const int *cell_start, const int32_t *perm, long long *staging,
+                                              const R *sc, const R *grav, int w) {
+    constexpr int W = P2GStc<ORD>::W;
+    static_assert(W % ROWS == 0, "rows per pass must divide the stencil width");
+    constexpr int NPASS = W / ROWS, LANES = W * NPASS, NCH = CH_MOM_END;
+    const int B = P.B, B3 = B * B * B, T = P.T, T3 = T * T * T;
+    const int t = active[w];
+    int tc[3];
+    tile_coords(P, t, tc);
+    const int s0 = start[t];
+    const int *cs = cell_start + (long long)w * (T3 + 1);
+    const int ntask = LANES * T3, step = (int)blockDim.x;
+    for (int u = threadIdx.x; u < ntask; u += step) {
+        const int c = u / LANES, sub = u - c * LANES;
+        const int sz = sub / NPASS, rg = sub - sz * NPASS;
+        const int cnext = (u + step) / LANES;
+        const int ka = cs[c], kb = cs[c + 1];
+        if (EXG_P2G_PREFETCH && sub == 0 && cnext < T3) {
+            // L2 prefetch of the first particle of the cell this thread takes next
+            const int kn = cs[cnext];
+            if (kn < cs[cnext + 1]) {
+                const int pn = perm[s0 + kn];
+                auto pf = [](const void *q) { asm volatile("prefetch.global.L2 [%0];" ::"l"(q)); };
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    pf(A.x[d] + pn);
+                    pf(A.v[d] + pn);
+                }
+#pragma unroll
+                for (int c6 = 0; c6 < 6; ++c6) pf(A.sig[c6] + pn);
+                pf(A.mass + pn);
+                pf(A.vol + pn);
+                pf(A.phase + pn);
+            }
+        }
+        if (ka == kb) continue;
+        const int lx = c % T, ly = (c / T) % T, lz = c / (T * T);
+        const int iv[3] = {tc[0] * T + lx, tc[1] * T + ly, tc[2] * T + lz};
+        bool inter[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            inter[d] = P.periodic[d] ||
+                       (ORD == 2 ? (iv[d] >= 3 && iv[d] <= P.nc[d] - 3) : (iv[d] >= 3 && iv[d] <= P.nc[d] - 4));
+        FactAcc<R> acc[ROWS][W];
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+            for (int sx = 0; sx < W; ++sx) acc[r][sx].zero();
+        bool any = false;
+        for (int k = ka; k < kb; ++k) {
+            const int p = perm[s0 + k];
+            if (A.phase[p] != 0) continue;
+            const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+            AxisW<R, W> az;
+            p2g_axis_weights<R, ORD>(*tab, P, 2, dual_x(P, 2, x[2]), iv[2], inter[2], az);
+            const R wz = pick<W>(az.w, sz), dwz = pick<W>(az.dw, sz);
+            if (wz == R(0) && dwz == R(0)) continue;
+            any = true;
+            AxisW<R, W> ax, ay;
+            p2g_axis_weights<R, ORD>(*tab, P, 0, dual_x(P, 0, x[0]), iv[0], inter[0], ax);
+            p2g_axis_weights<R, ORD>(*tab, P, 1, dual_x(P, 1, x[1]), iv[1], inter[1], ay);
+            const R m = A.mass[p], vol = A.vol[p];
+            const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
+                              x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] &&
+                              x[2] < P.slab_hi[2];
+            R sg[6];
+#pragma unroll
+            for (int c6 = 0; c6 < 6; ++c6) sg[c6] = -vol * A.sig[c6][p];
+            // rows of the symmetric stress in packed XX XY XZ YY YZ ZZ order
+            const R s0r[3] = {sg[0], sg[1], sg[2]}, s1r[3] = {sg[1], sg[3], sg[4]}, s2r[3] = {sg[2], sg[4], sg[5]};
+            FactZ<R> z;
+            z.m = m * wz;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const R bd = fma(m, grav[d], slab ? (R)P.extforce[d] : R(0));
+                const R sd0 = d == 0 ? s0r[0] : (d == 1 ? s1r[0] : s2r[0]);
+                const R sd1 = d == 0 ? s0r[1] : (d == 1 ? s1r[1] : s2r[1]);
+                const R sd2 = d == 0 ? s0r[2] : (d == 1 ? s1r[2] : s2r[2]);
+                z.p[d] = (m * A.v[d][p]) * wz;
+                z.a[d] = fma(sd2, dwz, bd * wz);
+                z.b[d] = sd1 * wz;
+                z.c[d] = sd0 * wz;
+            }
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r) {
+                const int sy = rg * ROWS + r;
+                const R wy = NPASS == 1 ? ay.w[r] : pick<W>(ay.w, sy);
+                const R dwy = NPASS == 1 ? ay.dw[r] : pick<W>(ay.dw, sy);
+                const FactRow<R, 1> row = fact_row<R>(z, wy, dwy);
+#pragma unroll
+                for (int sx = 0; sx < W; ++sx) {
+                    if constexpr (sizeof(R) == 4)
+                        acc[r][sx].add(row, make_float2(ax.w[sx], ax.w[sx]), make_float2(ax.dw[sx], ax.dw[sx]));
+                    else
+                        acc[r][sx].add(row, ax.w[sx], ax.dw[sx]);
+                }
+            }
+        }
+        if (!any) continue;
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+            for (int sx = 0; sx < W; ++sx) {
+                const int idx = ((lz + sz) * B + (ly + rg * ROWS + r)) * B + (lx + sx);
+#pragma unroll
+                for (int ch = 0; ch < NCH; ++ch) fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, acc[r][sx].get(ch), sc[ch]);
+            }
+    }
+    __syncthreads();
+    long long *dst = staging + (long long)w * NCH * B3;
+    for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) dst[i] = fx_value<R>(acc_lo[i], acc_hi[i]);
+    __syncthreads();
+}
+
+template <class R, int ORD, int V>
+__global__ void __launch_bounds__(P2GVar<R, ORD, V>::THREADS, P2GVar<R, ORD, V>::MINB)
+    k_p2g_fact(Params P, Parts<R> A, const int *active, const int *start, const int *cell_start, const int32_t *perm,
+               long long *staging, Ctl *ctl) {
+    constexpr int NCH = CH_MOM_END;
+    __shared__ int s_item;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
+    const int B3 = P.B * P.B * P.B;
+    unsigned *acc_lo = reinterpret_cast<unsigned *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
+    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3);
+    load_tables(tab);
+    R sc[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) sc[c] = (R)ctl->scale[c];
+    R grav[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) grav[d] = (R)P.gravity[d];
+    const int nitems = ctl->n_active_tiles;
+    for (;;) {
+        // tiles are taken in turn from a device counter
+        if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_p2g, 1);
+        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) {
+            acc_lo[i] = 0u;
+            acc_hi[i] = 0;
+        }
+        __syncthreads();
+        const int w = s_item;
+        if (w >= nitems) break;
+        p2g_tile_fact<R, ORD, P2GVar<R, ORD, V>::ROWS>(tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm,
+                                                        staging, sc, grav, w);
+    }
+}
+
 // Domain-wall BCs of one node (nodal_bcs, nodal_data_ops.cpp:663-766),
 // UDF walls (apply_udf_nodal_bcs, :1061-1175) and level-set bodies
 // (nodal_levelset_bcs, :129-220).  v is updated in place.
@@ -1501,10 +1786,15 @@ __device__ __forceinline__ void g2p_particle_generic(const SplineTables &tab, co
     g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt, jfac);
 }
 
-// Interpolation over a WN^3 window of the shared-memory node block.  FP32
-// accumulates channel pairs with the packed FP32 FMA of sm_100:
-// (vpic_x, vpic_y), (vpic_z, dpic_x), (dpic_y, dpic_z) and the first two
-// rows of grad v per column, (gv[0][c], gv[1][c]).
+// Interpolation over a WN^3 window of the shared-memory node block
+// (interpolate_from_grid, mpm_particle_grid_ops.cpp:972-1094), sum-factorized:
+// along each x row  a = sum wx v,  b = sum dwx v,  c = sum wx dv;  over the
+// rows of a z-slice  Sv = sum wy a,  Sy = sum dwy a,  Sx = sum wy b,
+// Sd = sum wy c;  over the slices  v_pic = sum wz Sv,  dv_pic = sum wz Sd and
+// grad v = (sum wz Sx, sum wz Sy, sum dwz Sv)  (the columns of
+// sum v (x) grad N with grad N = (dwx wy wz, wx dwy wz, wx wy dwz)).  A node
+// costs 5 FMAs (FP32: 4 packed and 1 scalar) instead of 15 plus the
+// products N and grad N.
 template <class R, int WN>
 __device__ __forceinline__ void g2p_window(const SmemNodes<R> &na, const int base[3], const R wx[WN], const R dwx[WN],
                                            const R wy[WN], const R dwy[WN], const R wz[WN], const R dwz[WN],
@@ -1514,89 +1804,120 @@ __device__ __forceinline__ void g2p_window(const SmemNodes<R> &na, const int bas
     const int i0 = ((base[2] - na.org[2]) * B + (base[1] - na.org[1])) * B + (base[0] - na.org[0]);
     const R *nb = na.nb;
     if constexpr (sizeof(R) == 4) {
-        float2 a01 = make_float2(0.f, 0.f), a2d = a01, d12 = a01;
-        float2 gc[3] = {a01, a01, a01};
-        float g2r[3] = {0.f, 0.f, 0.f};
+        const float2 z2 = make_float2(0.f, 0.f);
+        // slice-summed (x, y) pairs: v_pic (x, y), (v_pic z, dv_pic x),
+        // dv_pic (y, z); gradient columns 0, 1, 2 for rows (x, y) and z
+        float2 V01 = z2, V2D0 = z2, D12 = z2, G0 = z2, G1 = z2, G2 = z2;
+        float g0z = 0.f, g1z = 0.f, g2z = 0.f;
 #pragma unroll
         for (int sz = 0; sz < WN; ++sz) {
-            const float2 wzz = make_float2(wz[sz], wz[sz]), dzz = make_float2(dwz[sz], dwz[sz]);
+            float2 Sv01 = z2, Sv2d0 = z2, Sd12 = z2, Sy01 = z2, Sx01 = z2;
+            float Sy2 = 0.f, Sx2 = 0.f;
 #pragma unroll
             for (int sy = 0; sy < WN; ++sy) {
-                const float2 wyy = make_float2(wy[sy], wy[sy]), dyy = make_float2(dwy[sy], dwy[sy]);
-                const float2 wyz = __fmul2_rn(wyy, wzz), dyz = __fmul2_rn(dyy, wzz), wdz = __fmul2_rn(wyy, dzz);
                 const int row = i0 + (sz * B + sy) * B;
+                float2 a01 = z2, a2c0 = z2, c12 = z2, b01 = z2;
+                float b2 = 0.f;
 #pragma unroll
                 for (int sx = 0; sx < WN; ++sx) {
                     const float *q = nb + (row + sx) * NS;
                     const float4 va = *reinterpret_cast<const float4 *>(q);
-                    const float2 v01 = make_float2(va.x, va.y);
                     const float2 wxx = make_float2(wx[sx], wx[sx]);
-                    if (upd_vel) {
-                        const float2 vb = *reinterpret_cast<const float2 *>(q + 4);
-                        const float2 NN = __fmul2_rn(wxx, wyz);
-                        a01 = __ffma2_rn(v01, NN, a01);
-                        a2d = __ffma2_rn(make_float2(va.z, va.w), NN, a2d);
-                        d12 = __ffma2_rn(vb, NN, d12);
-                    }
+                    a01 = __ffma2_rn(wxx, make_float2(va.x, va.y), a01);
+                    a2c0 = __ffma2_rn(wxx, make_float2(va.z, va.w), a2c0);
+                    if (upd_vel) c12 = __ffma2_rn(wxx, *reinterpret_cast<const float2 *>(q + 4), c12);
                     if (upd_sr) {
-                        const float2 dxx = make_float2(dwx[sx], dwx[sx]);
-                        const float2 G0 = __fmul2_rn(dxx, wyz), G1 = __fmul2_rn(wxx, dyz), G2 = __fmul2_rn(wxx, wdz);
-                        gc[0] = __ffma2_rn(v01, G0, gc[0]);
-                        gc[1] = __ffma2_rn(v01, G1, gc[1]);
-                        gc[2] = __ffma2_rn(v01, G2, gc[2]);
-                        g2r[0] = fmaf(va.z, G0.x, g2r[0]);
-                        g2r[1] = fmaf(va.z, G1.x, g2r[1]);
-                        g2r[2] = fmaf(va.z, G2.x, g2r[2]);
+                        b01 = __ffma2_rn(make_float2(dwx[sx], dwx[sx]), make_float2(va.x, va.y), b01);
+                        b2 = fmaf(dwx[sx], va.z, b2);
                     }
                 }
+                const float2 wyy = make_float2(wy[sy], wy[sy]), dyy = make_float2(dwy[sy], dwy[sy]);
+                Sv01 = __ffma2_rn(wyy, a01, Sv01);
+                Sv2d0 = __ffma2_rn(wyy, a2c0, Sv2d0);
+                if (upd_vel) Sd12 = __ffma2_rn(wyy, c12, Sd12);
+                if (upd_sr) {
+                    Sy01 = __ffma2_rn(dyy, a01, Sy01);
+                    Sy2 = fmaf(dwy[sy], a2c0.x, Sy2);
+                    Sx01 = __ffma2_rn(wyy, b01, Sx01);
+                    Sx2 = fmaf(wy[sy], b2, Sx2);
+                }
+            }
+            const float2 wzz = make_float2(wz[sz], wz[sz]), dzz = make_float2(dwz[sz], dwz[sz]);
+            V01 = __ffma2_rn(wzz, Sv01, V01);
+            V2D0 = __ffma2_rn(wzz, Sv2d0, V2D0);
+            D12 = __ffma2_rn(wzz, Sd12, D12);
+            if (upd_sr) {
+                G0 = __ffma2_rn(wzz, Sx01, G0);
+                g0z = fmaf(wz[sz], Sx2, g0z);
+                G1 = __ffma2_rn(wzz, Sy01, G1);
+                g1z = fmaf(wz[sz], Sy2, g1z);
+                G2 = __ffma2_rn(dzz, Sv01, G2);
+                g2z = fmaf(dwz[sz], Sv2d0.x, g2z);
             }
         }
-        vpic[0] += a01.x;
-        vpic[1] += a01.y;
-        vpic[2] += a2d.x;
-        dpic[0] += a2d.y;
-        dpic[1] += d12.x;
-        dpic[2] += d12.y;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            gv[0][c] += gc[c].x;
-            gv[1][c] += gc[c].y;
-            gv[2][c] += g2r[c];
-        }
+        vpic[0] += V01.x;
+        vpic[1] += V01.y;
+        vpic[2] += V2D0.x;
+        dpic[0] += V2D0.y;
+        dpic[1] += D12.x;
+        dpic[2] += D12.y;
+        gv[0][0] += G0.x;
+        gv[1][0] += G0.y;
+        gv[2][0] += g0z;
+        gv[0][1] += G1.x;
+        gv[1][1] += G1.y;
+        gv[2][1] += g1z;
+        gv[0][2] += G2.x;
+        gv[1][2] += G2.y;
+        gv[2][2] += g2z;
     } else {
+        R V[3] = {R(0), R(0), R(0)}, D[3] = {R(0), R(0), R(0)};
+        R G[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
 #pragma unroll
         for (int sz = 0; sz < WN; ++sz) {
+            R Sv[3] = {R(0), R(0), R(0)}, Sd[3] = {R(0), R(0), R(0)}, Sy[3] = {R(0), R(0), R(0)},
+              Sx[3] = {R(0), R(0), R(0)};
 #pragma unroll
             for (int sy = 0; sy < WN; ++sy) {
-                const R wyz = wy[sy] * wz[sz], dyz = dwy[sy] * wz[sz], wdz = wy[sy] * dwz[sz];
                 const int row = i0 + (sz * B + sy) * B;
+                R a[3] = {R(0), R(0), R(0)}, bx[3] = {R(0), R(0), R(0)}, c[3] = {R(0), R(0), R(0)};
 #pragma unroll
                 for (int sx = 0; sx < WN; ++sx) {
                     const R *q = nb + (row + sx) * NS;
-                    const R v0 = q[0], v1 = q[1], v2 = q[2];
-                    if (upd_vel) {
-                        const R N = wx[sx] * wyz;
-                        vpic[0] = fma(N, v0, vpic[0]);
-                        vpic[1] = fma(N, v1, vpic[1]);
-                        vpic[2] = fma(N, v2, vpic[2]);
-                        dpic[0] = fma(N, q[3], dpic[0]);
-                        dpic[1] = fma(N, q[4], dpic[1]);
-                        dpic[2] = fma(N, q[5], dpic[2]);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        a[d] = fma(wx[sx], q[d], a[d]);
+                        if (upd_vel) c[d] = fma(wx[sx], q[3 + d], c[d]);
+                        if (upd_sr) bx[d] = fma(dwx[sx], q[d], bx[d]);
                     }
+                }
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    Sv[d] = fma(wy[sy], a[d], Sv[d]);
+                    if (upd_vel) Sd[d] = fma(wy[sy], c[d], Sd[d]);
                     if (upd_sr) {
-                        const R g0 = dwx[sx] * wyz, g1 = wx[sx] * dyz, g2 = wx[sx] * wdz;
-                        gv[0][0] = fma(v0, g0, gv[0][0]);
-                        gv[0][1] = fma(v0, g1, gv[0][1]);
-                        gv[0][2] = fma(v0, g2, gv[0][2]);
-                        gv[1][0] = fma(v1, g0, gv[1][0]);
-                        gv[1][1] = fma(v1, g1, gv[1][1]);
-                        gv[1][2] = fma(v1, g2, gv[1][2]);
-                        gv[2][0] = fma(v2, g0, gv[2][0]);
-                        gv[2][1] = fma(v2, g1, gv[2][1]);
-                        gv[2][2] = fma(v2, g2, gv[2][2]);
+                        Sy[d] = fma(dwy[sy], a[d], Sy[d]);
+                        Sx[d] = fma(wy[sy], bx[d], Sx[d]);
                     }
                 }
             }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                V[d] = fma(wz[sz], Sv[d], V[d]);
+                D[d] = fma(wz[sz], Sd[d], D[d]);
+                if (upd_sr) {
+                    G[d][0] = fma(wz[sz], Sx[d], G[d][0]);
+                    G[d][1] = fma(wz[sz], Sy[d], G[d][1]);
+                    G[d][2] = fma(dwz[sz], Sv[d], G[d][2]);
+                }
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            vpic[d] += V[d];
+            dpic[d] += D[d];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) gv[d][j] += G[d][j];
         }
     }
 }
@@ -1624,6 +1945,23 @@ __device__ __forceinline__ void g2p_particle_smem(const SplineTables &tab, const
             base[d] = n0 - 1;
         }
         g2p_window<R, 3>(na, base, a[0].w, a[0].dw, a[1].w, a[1].dw, a[2].w, a[2].dw, upd_vel, upd_sr, vpic, dpic,
+                         gv);
+        g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt, jfac);
+        return;
+    }
+    if constexpr (ORD == 3) {
+        // cubic: the 4x4x4 window of the particle's cell; fixed spline pieces
+        // on interior axes, the boundary-aware tables (zero outside
+        // compute_bounds) elsewhere; nodes outside the domain are 0 in the block
+        AxisW<R, 4> a[3];
+        int base[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const bool in = P.periodic[d] || (iv[d] >= 3 && iv[d] <= P.nc[d] - 4);
+            cell_axis_weights<R, 3>(tab, P, d, x[d], iv[d], in, a[d]);
+            base[d] = iv[d] - 1;
+        }
+        g2p_window<R, 4>(na, base, a[0].w, a[0].dw, a[1].w, a[1].dw, a[2].w, a[2].dw, upd_vel, upd_sr, vpic, dpic,
                          gv);
         g2p_finish<R>(P, upd_vel, upd_sr, vpic, dpic, gv, v, vp, E, sr, dt, jfac);
         return;
@@ -2019,8 +2357,22 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
     __syncthreads();
 }
 
-template <class R, int ORD, bool LEAN>
-__global__ void __launch_bounds__(EXG_G2P_THREADS, EXG_G2P_MINB) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
+// Launch variants of the fused G2P (threads per block, minimum resident
+// blocks per SM); variant 0 is the default, the autotuner measures the
+// others on the lean quadratic and cubic kernels.  Each particle's update is
+// independent of the launch shape, so all variants give identical results.
+constexpr int kG2PVariants = 3;
+static_assert(kG2PVariants == EXG_NUM_VARIANTS, "the launchers dispatch EXG_NUM_VARIANTS G2P variants");
+// threads per block, minimum blocks per SM:
+//   FP32: (256, 2)  (128, 4)  (384, 1);   FP64: (256, 2)  (256, 1)  (384, 1)
+template <class R, int V>
+struct G2PVar {
+    static constexpr int THREADS = (V == 0) ? EXG_G2P_THREADS : (V == 1 ? (sizeof(R) == 4 ? 128 : 256) : 384);
+    static constexpr int MINB = (V == 0) ? EXG_G2P_MINB : (V == 1 ? (sizeof(R) == 4 ? 4 : 1) : 1);
+};
+
+template <class R, int ORD, bool LEAN, int V = 0>
+__global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
                                                         const Material *mats, const int *active, const int *start,
                                                         const int *count, const int32_t *perm, Ctl *ctl, int mode) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -2757,8 +3109,13 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
 #pragma unroll
             for (int d = 0; d < 3; ++d) grav[d] = (R)sd.P.gravity[d];
         }
-        p2g_tile<R, ORD, THERM>(tab, acc_lo, acc_hi, sd.P, sd.A, sd.active, sd.start, sd.cell_start, sd.perm,
-                                sd.staging, sc, grav, i - b->pre_active[s]);
+        if constexpr (P2GCfg<R, ORD, THERM>::FACT)
+            p2g_tile_fact<R, ORD, P2GCfg<R, ORD, THERM>::ROWS>(tab, acc_lo, acc_hi, sd.P, sd.A, sd.active, sd.start,
+                                                                sd.cell_start, sd.perm, sd.staging, sc, grav,
+                                                                i - b->pre_active[s]);
+        else
+            p2g_tile<R, ORD, THERM>(tab, acc_lo, acc_hi, sd.P, sd.A, sd.active, sd.start, sd.cell_start, sd.perm,
+                                    sd.staging, sc, grav, i - b->pre_active[s]);
     }
 }
 
@@ -2997,9 +3354,39 @@ static void p2g_cell_t(Ctx &c, int flags) {
     EXG_CUDA_OK(cudaGetLastError());
 }
 
+template <class R, int ORD, int V>
+static void p2g_fact_v(Ctx &c) {
+    const int B3 = c.P.B * c.P.B * c.P.B;
+    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * CH_MOM_END * B3;
+    auto kern = k_p2g_fact<R, ORD, V>;
+    constexpr int nthr = P2GVar<R, ORD, V>::THREADS;
+    EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    static int grid = 0;
+    static size_t gsm = 0;
+    if (!grid || gsm != sm) {
+        int dev = 0, nsm = 0, per = 0;
+        EXG_CUDA_OK(cudaGetDevice(&dev));
+        EXG_CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        EXG_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, nthr, sm));
+        grid = nsm * (per < 1 ? 1 : per);
+        gsm = sm;
+    }
+    kern<<<grid, nthr, sm, c.stream>>>(c.P, c.A<R>(), c.sb.active, c.sb.tile_start, c.sb.cell_start, c.sb.perm,
+                                       c.staging, c.ctl);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
 template <class R, int ORD, bool TH>
 static void p2g_t(Ctx &c, int flags) {
-    p2g_cell_t<R, ORD, TH>(c, flags);
+    if constexpr (P2GCfg<R, ORD, TH>::FACT) {
+        switch (c.p2g_var) {
+            case 1: p2g_fact_v<R, ORD, 1>(c); break;
+            case 2: p2g_fact_v<R, ORD, 2>(c); break;
+            default: p2g_fact_v<R, ORD, 0>(c); break;
+        }
+    } else {
+        p2g_cell_t<R, ORD, TH>(c, flags);
+    }
 }
 
 void EXG_SFX(launch_p2g)(Ctx &c, int flags) {
@@ -3032,28 +3419,37 @@ void EXG_SFX(launch_nodes)(Ctx &c, int mode, int flags, bool all_tiles) {
     EXG_CUDA_OK(cudaGetLastError());
 }
 
-template <class R, int ORD, bool LEAN>
+template <class R, int ORD, bool LEAN, int V = 0>
 static void g2p_lt(Ctx &c, int mode) {
     const int B3 = c.P.B * c.P.B * c.P.B;
     size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(R) * SmemNodes<R>::NS * B3;
-    auto kern = k_g2p_fused<R, ORD, LEAN>;
+    auto kern = k_g2p_fused<R, ORD, LEAN, V>;
+    constexpr int nthr = G2PVar<R, V>::THREADS;
     EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     static int grid = 0;
     static size_t gsm = 0;
     if (!grid || gsm != sm) {
-        grid = persistent_grid(kern, sm, EXG_G2P_THREADS);
+        grid = persistent_grid(kern, sm, nthr);
         gsm = sm;
     }
-    kern<<<grid, EXG_G2P_THREADS, sm, c.stream>>>(c.P, c.A<R>(), c.Bp<R>(), c.N<R>(), make_bc(c), c.mat_dev, c.sb.active,
-                                           c.sb.tile_start, c.sb.tile_count, c.sb.perm, c.ctl, mode);
+    kern<<<grid, nthr, sm, c.stream>>>(c.P, c.A<R>(), c.Bp<R>(), c.N<R>(), make_bc(c), c.mat_dev, c.sb.active,
+                                       c.sb.tile_start, c.sb.tile_count, c.sb.perm, c.ctl, mode);
     EXG_CUDA_OK(cudaGetLastError());
 }
 template <class R, int ORD>
 static void g2p_t(Ctx &c, int mode) {
-    if (g2p_lean(c))
+    if (g2p_lean(c)) {
+        if constexpr (ORD == 2 || ORD == 3) {
+            switch (c.g2p_var) {
+                case 1: g2p_lt<R, ORD, true, 1>(c, mode); return;
+                case 2: g2p_lt<R, ORD, true, 2>(c, mode); return;
+                default: break;
+            }
+        }
         g2p_lt<R, ORD, true>(c, mode);
-    else
+    } else {
         g2p_lt<R, ORD, false>(c, mode);
+    }
 }
 void EXG_SFX(launch_g2p_fused)(Ctx &c, int mode) {
     using R = EXG_R;

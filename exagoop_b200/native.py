@@ -82,7 +82,7 @@ class Specs(C.Structure):
         ("write_diag_output_time", C.c_double),
         ("print_diagnostics", C.c_int), ("do_calculate_tke_tse", C.c_int), ("do_calculate_mwa_velcomp", C.c_int),
         ("do_calculate_mwa_velmag", C.c_int), ("do_calculate_minmaxpos", C.c_int),
-        ("precision", C.c_int), ("tile", C.c_int),
+        ("precision", C.c_int), ("tile", C.c_int), ("autotune", C.c_int),
     ]
 
     def copy(self) -> "Specs":
@@ -149,7 +149,7 @@ EXPORTED = [
     "exg_get_stream", "exg_p2g_momentum_noalloc", "exg_batch_create", "exg_batch_destroy", "exg_batch_scene",
     "exg_batch_num_scenes", "exg_batch_step", "exg_batch_last_error", "exg_particles_alloc_pinned",
     "exg_particles_free_pinned", "exg_levelset_shape", "exg_levelset_build_device", "exg_init_levelsets",
-    "exg_get_levelset",
+    "exg_get_levelset", "exg_autotune", "exg_set_variants", "exg_get_variants",
 ]
 
 _lib = None
@@ -226,6 +226,9 @@ def lib() -> C.CDLL:
         "exg_batch_num_scenes": (i, [vp]),
         "exg_batch_step": (i, [vp, i]),
         "exg_batch_last_error": (C.c_char_p, [vp]),
+        "exg_autotune": (i, [vp]),
+        "exg_set_variants": (i, [vp, i, i]),
+        "exg_get_variants": (i, [vp, C.POINTER(i), C.POINTER(i), pd, pd]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -327,7 +330,7 @@ def specs_defaults() -> Specs:
     (mpm_specs.H:83), num_redist 10, max_steps 1, output times 1e200, order 1
     on every axis, dt limits [1e-12, 1], CFL 0.1, mass_tolerance 1e-8, FLIP
     0.95, USL, slip walls with friction 0.1, adiabatic thermal walls, FP64,
-    tile 0 (chosen by the library)."""
+    tile 0 (the library's default), launch-variant autotuning on."""
     s = Specs()  # ctypes zero-fills every field, as the C memset does
     s.gravity[1] = -9.81
     s.num_redist = 10
@@ -348,6 +351,7 @@ def specs_defaults() -> Specs:
     s.stress_update_scheme = 0
     s.precision = PREC_FP64
     s.tile = 0
+    s.autotune = 1
     return s
 
 
@@ -553,6 +557,19 @@ class Context:
         self._ck(self.L.exg_sort_keys(self.h, keys.ctypes.data_as(C.POINTER(C.c_uint32)),
                                       perm.ctypes.data_as(C.POINTER(C.c_int32))), "exg_sort_keys")
         return keys, perm
+
+    def autotune(self):
+        """exg_autotune: time the launch variants on the current particles."""
+        self._ck(self.L.exg_autotune(self.h), "exg_autotune")
+
+    def set_variants(self, p2g: int = -1, g2p: int = -1):
+        self._ck(self.L.exg_set_variants(self.h, p2g, g2p), "exg_set_variants")
+
+    def variants(self) -> dict:
+        p, g = C.c_int(), C.c_int()
+        pm, gm = (C.c_double * 3)(), (C.c_double * 3)()
+        self._ck(self.L.exg_get_variants(self.h, C.byref(p), C.byref(g), pm, gm), "exg_get_variants")
+        return {"p2g": p.value, "g2p": g.value, "p2g_ms": list(pm), "g2p_ms": list(gm)}
 
     def tile(self) -> int:
         t = C.c_int()

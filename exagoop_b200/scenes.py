@@ -254,23 +254,65 @@ def heated_block(n=(24, 16, 20), size=(1.2, 0.8, 1.0), fill=0.7, order=2, seed=7
     return s, p, phi
 
 
-def batched_dam_breaks(n_scenes=64, sides=(32, 48, 64, 96, 128), fill=(0.1, 0.4), seed=2024, precision=nt.PREC_MIXED):
+def batched_dam_breaks(n_scenes=64, sides=(32, 48, 64, 96, 128), fill=(0.1, 0.4), seed=2024, precision=nt.PREC_MIXED,
+                       only=None):
     """Generator of the batched uneven scenes: n_scenes independent dam
     breaks (the dam_break fluid and walls) in unit cubes with a cubic grid
     side drawn from `sides` and a water fill fraction f drawn uniformly from
     `fill`; the block spans x in [0, 2f], all of y and z in [0, 0.5] (volume
     fraction f) at 2x2x2 particles per cell, jittered.  Yields (specs,
-    particles) one scene at a time, so the host holds one scene's arrays."""
+    particles) one scene at a time, so the host holds one scene's arrays.
+    `only` restricts it to the listed scene indices (each scene keeps its own
+    seed, so a subset is the same scenes as in the whole set)."""
     draws = batched_scene_sizes(n_scenes, sides, fill, seed)
     for i, (n, f) in enumerate(draws):
+        if only is not None and i not in only:
+            continue
         yield dam_break(n=(n, n, n), size=(1.0, 1.0, 1.0), block=(2.0 * f, 1.0, 0.5), seed=seed + 1 + i,
                         precision=precision)
 
 
-def batched_specs(n_scenes=64, sides=(32, 48, 64, 96, 128), fill=(0.1, 0.4), seed=2024, precision=nt.PREC_MIXED):
+def batched_specs(n_scenes=64, sides=(32, 48, 64, 96, 128), fill=(0.1, 0.4), seed=2024, precision=nt.PREC_MIXED,
+                  only=None):
     """Specs of the scenes batched_dam_breaks yields, without particles."""
     return [dam_break_specs((n, n, n), (1.0, 1.0, 1.0), precision)
-            for n, _ in batched_scene_sizes(n_scenes, sides, fill, seed)]
+            for i, (n, _) in enumerate(batched_scene_sizes(n_scenes, sides, fill, seed))
+            if only is None or i in only]
+
+
+def lattice_count(lo, hi, dx, ppc) -> int:
+    """Number of points lattice(lo, hi, dx, ppc) generates, without them."""
+    n = 1
+    for d in range(3):
+        h = dx[d] / ppc[d]
+        k = int(np.floor((hi[d] - lo[d]) / h + 1e-9))
+        pts = lo[d] + 0.5 * h + h * np.arange(k)
+        n *= int((pts < hi[d]).sum())
+    return n
+
+
+def batched_scene_particle_counts(n_scenes=64, sides=(32, 48, 64, 96, 128), fill=(0.1, 0.4), seed=2024):
+    """Particles of every scene batched_dam_breaks generates (jitter and
+    clipping keep the lattice count), computed without generating them."""
+    return [lattice_count((0, 0, 0), (2.0 * f, 1.0, 0.5), (1.0 / n,) * 3, (2, 2, 2))
+            for n, f in batched_scene_sizes(n_scenes, sides, fill, seed)]
+
+
+def partition_scenes(counts, nparts):
+    """Scenes dealt to nparts ranks by particle count, largest first, each
+    to the rank with the fewest particles so far (ties to the lower rank and
+    the lower scene index): the scene-level counterpart of the reference's
+    DistributionMapping of its boxes over MPI ranks (Source/mpm_init.cpp:
+    154-158).  Returns each rank's ascending list of scene indices; every
+    rank computes the same lists, with no communication."""
+    order = sorted(range(len(counts)), key=lambda i: (-counts[i], i))
+    load = [0] * nparts
+    parts = [[] for _ in range(nparts)]
+    for i in order:
+        r = min(range(nparts), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += counts[i]
+    return [sorted(p) for p in parts]
 
 
 def batched_scene_sizes(n_scenes=64, sides=(32, 48, 64, 96, 128), fill=(0.1, 0.4), seed=2024):

@@ -162,7 +162,8 @@ typedef struct exg_specs {
         do_calculate_minmaxpos;
     /* B200 execution keys (exg.* namespace, no counterpart in the reference) */
     int precision; /* EXG_PREC_FP64 or EXG_PREC_MIXED */
-    int tile;      /* tile edge in cells: 0 = autotune, else 4 or 8 */
+    int tile;      /* tile edge in cells: 0 = the default (8), else 4 or 8 */
+    int autotune;  /* 1 (default): the first exg_step times the launch variants (exg_autotune) */
 } exg_specs;
 
 typedef struct exg_diag {
@@ -350,6 +351,31 @@ int exg_set_stage_timing(exg_ctx *ctx, int on);
 int exg_last_step_timing(exg_ctx *ctx, double *ms5);
 /* The CUDA stream (cudaStream_t) the context issues all its work on. */
 int exg_get_stream(exg_ctx *ctx, void **stream);
+
+/* ------------------------------------------------ launch-variant autotuner
+ * No counterpart in the reference, whose only tiling knob is
+ * mpm.max_grid_size (the box size of its BoxArray, Source/mpm_init.cpp:
+ * 154-155).  The P2G and the fused G2P kernels each come in EXG_NUM_VARIANTS
+ * launch variants (P2G: rows of the stencil slice per pass and threads per
+ * block; G2P: threads per block and resident blocks per SM).  Every variant
+ * gives bit-identical results; only their speed differs with the GPU, the
+ * B-spline order, the precision and the particle distribution.
+ * exg_autotune times each variant on the context's current particles (a few
+ * launches each, on the context's stream, outside any graph) and keeps the
+ * fastest; choices are cached per (device, precision, order, tile, G2P
+ * kind, particle-count decade) so later contexts of the same kind reuse them
+ * without timing.  With specs.autotune = 1 the first exg_step calls it.
+ * It leaves the particle state and the step's control block as it found
+ * them; nodal data is recomputed by the next step. */
+#define EXG_NUM_VARIANTS 3
+int exg_autotune(exg_ctx *ctx);
+/* Select variants explicitly (0 .. EXG_NUM_VARIANTS-1; -1 keeps the current
+ * one); disables the automatic tuning of the next exg_step. */
+int exg_set_variants(exg_ctx *ctx, int p2g, int g2p);
+/* Current variants and, after a tuning run, each variant's measured ms per
+ * launch (arrays of EXG_NUM_VARIANTS; 0 where not measured; either pointer
+ * may be NULL). */
+int exg_get_variants(exg_ctx *ctx, int *p2g, int *g2p, double *p2g_ms, double *g2p_ms);
 
 /* ------------------------------------------------ P2G without allocation */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc:

@@ -7,8 +7,10 @@ FP64 bound.  The GPU's nodal sums are exact fixed-point sums, the oracle's
 are sequential FP64 sums: the two differ by rounding (~1e-16) every step,
 and a workload amplifies such differences at its own rate (reflections at
 walls and obstacles are discontinuous in position).  The test measures that
-rate directly: the oracle against itself with every initial position and
-velocity component moved by one ulp.  The FP64 GPU path must stay within
+rate directly: the oracle against itself with every initial position,
+velocity component and diagonal entry of F moved by one ulp (an ulp of J
+moves the Tait pressure p = K((1/J)^gamma - 1) by gamma K ulp, ~3e-9 Pa for
+water: the fluid's pressure and stress are that sensitive to rounding).  The FP64 GPU path must stay within
 max(1e-10, 10 x that self-divergence) in every field; on the workloads whose
 self-divergence stays below 1e-11 (the elastic spheres, the dam break) that
 is the 1e-10 of the parity tests.  Measured self-divergence after 1000 steps
@@ -91,6 +93,8 @@ def test_thousand_steps_against_oracle(name):
 
     q.pos[:] = ulp(q.pos)
     q.rdata[nt.R_VEL:nt.R_VEL + 3] = ulp(q.rdata[nt.R_VEL:nt.R_VEL + 3])
+    for a in (0, 4, 8):  # F's diagonal: one ulp of J (the Tait pressure's sensitivity)
+        q.rdata[nt.R_DEFGRAD + a] = ulp(q.rdata[nt.R_DEFGRAD + a])
     self_div = l2_errors(oracle_1000(s, q, phi), r, bool(s.use_temp))
     res = {}
     for prec, tag in [(nt.PREC_FP64, "fp64"), (nt.PREC_MIXED, "mixed")]:
