@@ -252,6 +252,8 @@ def measure(args, config, rank, world, dev, with_e2e, with_accuracy):
     ctx = nt.Context(with_precision(s, prec), device=dev)
     ctx.upload(p)
     ctx.Initialise_Internal_Forces()
+    if args.p2g_variant >= 0 or args.g2p_variant >= 0:
+        ctx.set_variants(args.p2g_variant, args.g2p_variant)  # pinned: no tuning run
     # device-timed steps (inputs resident; particle state 8-9 M x ~300 B >> L2)
     if world > 1:
         torch.distributed.barrier()
@@ -394,6 +396,47 @@ def run_batch(args, rank, world):
     ms, total_all = job_reduce(ms, total, world)
     value = total_all * args.steps / (ms * 1e-3)
     sides = [int(s.ncells[0]) for s in specs]
+    # per-stage device times (eager steps, CUDA events between the stages)
+    b.stage_timing(True)
+    b.step(max(3, min(10, args.steps)))
+    st = b.last_step_timing()
+    b.stage_timing(False)
+    stages = {"sort": st[0], "p2g": st[1], "nodal": st[2], "g2p": st[3]}
+    peak, peak_kind = read_peaks()
+    w = 4 if prec == nt.PREC_MIXED else 8
+    name = f"batched_dam_breaks_{args.scenes}_scenes"
+    rl = roofline(stages, w, total, name, peak, peak_kind)
+    # end to end through the C ABI with host buffers: every scene of this
+    # rank uploaded from page-locked host memory (one staging set, filled
+    # from the scene's host arrays in turn), the steps, every scene
+    # downloaded back through it
+    e2e = None
+    if not args.no_e2e:
+        host = [p for _, p in scenes.batched_dam_breaks(n_scenes=args.scenes, seed=seed, precision=prec,
+                                                        only=set(mine))]
+        big = max(p.n for p in host)
+        stage = nt.Particles(big, pinned=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for sc, p in zip(b.scenes, host):
+            sub = stage.view(p.n)
+            sub.pos[:] = p.pos
+            sub.rdata[:] = p.rdata
+            sub.idata[:] = p.idata
+            sc.upload(sub)
+        b.step(args.steps)
+        for sc, p in zip(b.scenes, host):
+            sub = stage.view(p.n)
+            sc.download_into(sub)
+            p.pos[:] = sub.pos
+            p.rdata[:] = sub.rdata
+            p.idata[:] = sub.idata
+        e2e_s = time.perf_counter() - t0
+        nbytes = sum(p.pos.nbytes + p.rdata.nbytes + p.idata.nbytes for p in host)
+        e2e_s = job_reduce(e2e_s * 1e3, 0, world)[0] * 1e-3
+        e2e = {"value": total_all * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(nbytes / args.steps), "d2h_bytes_per_step": int(nbytes / args.steps)}
+        del host, stage
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
@@ -405,12 +448,13 @@ def run_batch(args, rank, world):
                    "parallelism": f"scenes partitioned over {world} GPUs by particle count" if world > 1
                    else "single"},
         "clocks": clk.summary(),
-        "e2e": None,
-        # per scene: dt_finalize, keys, tile_scan, touched, scatter,
-        # tile_sort, scales, copy_lost, time_advance; per batch: plan and the
-        # batched P2G, nodal and G2P kernels
-        "gpu_launches": args.steps * (len(specs) * 9 + 4),
-        "roofline": None,
+        "e2e": e2e,
+        # per step, whatever the number of scenes: step start, keys, tile
+        # scan, scatter, plan, tile sort, touched, scales, plan, then the
+        # batched P2G, nodal and G2P kernels, lost particles, time advance
+        "gpu_launches": args.steps * 14,
+        "stages_ms": {k: round(v, 4) for k, v in stages.items()},
+        "roofline": rl,
         "cpu_baseline": None,
     }
     b.close()
@@ -454,6 +498,31 @@ def cpu_sample(config, scale, tile, threads, nsteps, warmup=1, budget_s=None):
     return p.n * done / spent, desc, name, done
 
 
+def cpu_sample_batch(n_scenes, threads, nsteps=2):
+    """Oracle on a bounded sample of the batch: the first four scenes of the
+    seeded set, one warm-up step and nsteps timed steps each, FP64."""
+    import orc
+    from exagoop_b200 import scenes
+    isa = orc.use_native()
+    pts, spent = 0, 0.0
+    picked = list(range(min(4, n_scenes)))
+    for s, p in scenes.batched_dam_breaks(n_scenes=n_scenes, seed=BATCH_SEED, only=set(picked)):
+        s = s.copy()
+        from exagoop_b200 import native as nt
+        s.precision = nt.PREC_FP64
+        o = orc.Oracle(s, threads=threads)
+        o.upload(p)
+        o.init_internal_forces()
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(nsteps)
+        spent += time.perf_counter() - t0
+        pts += p.n * nsteps
+    desc = (f"batched dam breaks: scenes {picked} of the {n_scenes}-scene set, 1 warm-up + {nsteps} timed steps "
+            f"each, FP64, oracle {isa}, {threads} threads on {cpu_model()}")
+    return pts / spent, desc
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -468,7 +537,10 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 error measurement (0 skips it)")
     ap.add_argument("--scenes", type=int, default=64, help="scenes of --config batch")
+    ap.add_argument("--p2g-variant", type=int, default=-1, help="pin the P2G launch variant (-1: autotune)")
+    ap.add_argument("--g2p-variant", type=int, default=-1, help="pin the G2P launch variant (-1: autotune)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (batch)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     args = ap.parse_args()
@@ -504,6 +576,9 @@ def main():
     if args.config == "batch":
         line = run_batch(args, rank, world)
         if rank == 0:
+            if not args.no_cpu:
+                v, desc = cpu_sample_batch(args.scenes, threads)
+                line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
             print(json.dumps(line))
         if world > 1:
             import torch

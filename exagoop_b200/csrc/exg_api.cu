@@ -269,7 +269,8 @@ void upload_parts(Ctx &c, const exg_particle_soa *h, const std::vector<int32_t> 
         put_r(P.eps[k], EXG_R_STRAIN + k);
         put_r(P.sig[k], EXG_R_STRESS + k);
     }
-    for (int k = 0; k < 9; ++k) put_r(P.E[k], EXG_R_DEFGRAD + k, (k % 4 == 0) ? 1.0 : 0.0);
+    // FP32 state keeps E = F - I, FP64 state F itself
+    for (int k = 0; k < 9; ++k) put_r(P.E[k], EXG_R_DEFGRAD + k, (k % 4 == 0 && !fp64(c)) ? 1.0 : 0.0);
     put_r(P.vol, EXG_R_VOLUME);
     put_r(P.mass, EXG_R_MASS);
     put_r(P.rho, EXG_R_DENSITY);
@@ -355,7 +356,7 @@ void download_parts(Ctx &c, exg_particle_soa *h) {
         get_r(P.eps[k], EXG_R_STRAIN + k);
         get_r(P.sig[k], EXG_R_STRESS + k);
     }
-    for (int k = 0; k < 9; ++k) get_r(P.E[k], EXG_R_DEFGRAD + k, (k % 4 == 0) ? 1.0 : 0.0);
+    for (int k = 0; k < 9; ++k) get_r(P.E[k], EXG_R_DEFGRAD + k, (k % 4 == 0 && !fp64(c)) ? 1.0 : 0.0);
     get_r(P.vol, EXG_R_VOLUME);
     get_r(P.mass, EXG_R_MASS);
     get_r(P.rho, EXG_R_DENSITY);
@@ -1631,30 +1632,26 @@ std::string batch_compatible(const exg_specs *s, int n) {
     }
     return "";
 }
+// One batch step: the batched sort and bookkeeping of every scene, the
+// batched P2G, nodal and G2P kernels, the batched end of step -- a fixed
+// sequence of launches whatever the number of scenes.
 void enqueue_batch_step(exg_batch *B) {
     Batch &b = B->b;
-    for (Ctx *cp : b.scenes) {
-        Ctx &c = *cp;
-        EXG_CUDA_OK(cudaMemcpyAsync(c.bounds_cur, &c.ctl->bound_bits[0], sizeof(unsigned long long) * CH_ALL,
-                                    cudaMemcpyDeviceToDevice, c.stream));
-        launch_dt_finalize(c, true);
-        launch_keys(c);
-        launch_sort_rest(c, true);
-        launch_scales_from(c, c.bounds_cur);
-    }
+    const bool f64 = b.precision == EXG_PREC_FP64;
+    auto mark = [&](int k) {
+        if (b.timing) EXG_CUDA_OK(cudaEventRecord(b.ev[k], b.stream));
+    };
+    mark(0);
+    launch_batch_sort(b);
     launch_batch_plan(b);
-    if (b.precision == EXG_PREC_FP64)
-        launch_batch_core_fp64(b);
-    else
-        launch_batch_core_fp32(b);
-    for (Ctx *cp : b.scenes) {
-        Ctx &c = *cp;
-        if (c.precision == EXG_PREC_FP64)
-            launch_copy_lost_fp64(c);
-        else
-            launch_copy_lost_fp32(c);
-        launch_time_advance(c);
-    }
+    mark(1);
+    f64 ? launch_batch_p2g_fp64(b) : launch_batch_p2g_fp32(b);
+    mark(2);
+    f64 ? launch_batch_nodes_fp64(b) : launch_batch_nodes_fp32(b);
+    mark(3);
+    f64 ? launch_batch_g2p_fp64(b) : launch_batch_g2p_fp32(b);
+    f64 ? launch_batch_finish_fp64(b) : launch_batch_finish_fp32(b);
+    mark(4);
 }
 void batch_flip(Batch &b) {
     for (Ctx *c : b.scenes) swap_parts(*c);
@@ -1724,8 +1721,34 @@ int exg_batch_destroy(exg_batch *B) {
     cudaFree(b.bctl);
     cudaFree(b.ctls);
     for (void *d : b.desc) cudaFree(d);
+    for (SortDesc *d : b.sdesc) cudaFree(d);
+    for (cudaEvent_t e : b.ev)
+        if (e) cudaEventDestroy(e);
     if (b.stream) cudaStreamDestroy(b.stream);
     delete B;
+    return EXG_OK;
+}
+
+int exg_batch_set_stage_timing(exg_batch *B, int on) {
+    if (!B) return EXG_ERR_ARG;
+    Batch &b = B->b;
+    try {
+        for (cudaEvent_t &e : b.ev)
+            if (!e) EXG_CUDA_OK(cudaEventCreate(&e));
+    } catch (const std::exception &e) {
+        return bfail(B, EXG_ERR_CUDA, e.what());
+    }
+    b.timing = on != 0;
+    for (double &v : b.stage_ms) v = 0.0;
+    return EXG_OK;
+}
+
+int exg_batch_last_step_timing(exg_batch *B, double *ms5) {
+    if (!B || !ms5) return EXG_ERR_ARG;
+    const Batch &b = B->b;
+    const double n = b.stage_ms[4] > 0 ? b.stage_ms[4] : 1.0;
+    for (int k = 0; k < 4; ++k) ms5[k] = b.stage_ms[k] / n;
+    ms5[4] = b.stage_ms[4];
     return EXG_OK;
 }
 
@@ -1751,13 +1774,20 @@ int exg_batch_step(exg_batch *B, int nsteps) {
         for (Ctx *sc : b.scenes) lean = lean && g2p_lean(*sc);
         if (changed || lean != b.lean) batch_drop_graphs(b);
         b.lean = lean;
-        const bool use_graph = std::getenv("EXG_NO_GRAPH") == nullptr;
+        const bool use_graph = std::getenv("EXG_NO_GRAPH") == nullptr && !b.timing;
         for (int s = 0; s < nsteps; ++s) {
             cudaGraphExec_t &g = b.gexec[b.parity];
             if (!use_graph || !b.warm[b.parity]) {
                 // the first step of each parity runs eagerly (kernel
                 // attributes, occupancy queries), later ones replay a graph
                 enqueue_batch_step(B);
+                if (b.timing) {
+                    EXG_CUDA_OK(cudaEventSynchronize(b.ev[4]));
+                    float ms[4];
+                    for (int k = 0; k < 4; ++k) EXG_CUDA_OK(cudaEventElapsedTime(&ms[k], b.ev[k], b.ev[k + 1]));
+                    for (int k = 0; k < 4; ++k) b.stage_ms[k] += ms[k];
+                    b.stage_ms[4] += 1.0;
+                }
                 b.warm[b.parity] = true;
                 batch_flip(b);
                 continue;

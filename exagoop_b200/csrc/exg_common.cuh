@@ -66,10 +66,18 @@ struct Ctl {
 constexpr int kMaxScenes = 1024;
 struct BatchCtl {
     int nscenes;
-    int next_p2g, next_nodes, next_g2p;
+    int next_p2g, next_nodes, next_g2p, next_sort;
     int pre_active[kMaxScenes + 1];   // scene s owns items [pre[s], pre[s+1]) of the active-tile list
     int pre_touched[kMaxScenes + 1];  // the same for the tiles the nodal kernel writes
+    // set on the host when the scenes' particle counts change: scene s owns
+    // blocks [pre_blocks[s], pre_blocks[s+1]) of the per-particle batched
+    // kernels (kBatchThreads particles each, so no block spans two scenes)
+    // and tiles [pre_tiles[s], pre_tiles[s+1]) of the per-tile ones
+    int pre_blocks[kMaxScenes + 1];
+    int pre_tiles[kMaxScenes + 1];
 };
+constexpr int kBatchThreads = 256;
+
 
 struct Body {
     int mom_bc;
@@ -116,6 +124,22 @@ struct Params {
     int bclo_temp[3], bchi_temp[3];
     double Twall_lo[3], Twall_hi[3], qflux_lo[3], qflux_hi[3], hc_lo[3], hc_hi[3], Tinf_lo[3], Tinf_hi[3];
     int udfT_lo[3], udfT_hi[3];  // wall-temperature table present
+};
+
+// What the batched sort and bookkeeping kernels need of one scene: its grid,
+// the positions of the storage the step starts from, its sort buffers, its
+// control block and the P2G bounds the step uses.
+struct SortDesc {
+    Params P;
+    double *x[3];
+    long long np;
+    int cap;  // sort scratch (tiles above the shared-memory cap) starts at bucket + cap
+    uint32_t *key;
+    int *tile_count, *tile_fill, *tile_start, *active, *slot, *touched, *cell_start;
+    long long *touched_step;
+    int32_t *bucket, *perm;
+    Ctl *ctl;
+    unsigned long long *bounds_cur;
 };
 
 // Particle storage (structure of arrays).  Positions are FP64 in both
@@ -339,13 +363,18 @@ EXG_HD void newtonian(const R ed[6], R s[6], R mu, R p) {
     s[4] = R(2) * mu * ed[4];
 }
 
-// det(I + E) in FP64 (updateVolume, mpm_particle_timestep.cpp:160-163, on
-// F = I + E).
-EXG_HD double det_IpE(const double e[9]) {
-    double a = 1.0 + e[0], b = e[1], c = e[2];
-    double d = e[3], f = 1.0 + e[4], g = e[5];
-    double h = e[6], k = e[7], m = 1.0 + e[8];
-    return a * (f * m - g * k) - b * (d * m - g * h) + c * (d * k - f * h);
+// det F in the order of updateVolume (mpm_particle_timestep.cpp:160-163),
+// every product and difference rounded on its own (no fused multiply-add),
+// as the reference's host build evaluates it.
+EXG_HD double det_ref(const double F[9]) {
+#ifdef __CUDA_ARCH__
+    const double t1 = __dsub_rn(__dmul_rn(F[4], F[8]), __dmul_rn(F[5], F[7]));
+    const double t2 = __dsub_rn(__dmul_rn(F[3], F[8]), __dmul_rn(F[5], F[6]));
+    const double t3 = __dsub_rn(__dmul_rn(F[3], F[7]), __dmul_rn(F[4], F[6]));
+    return __dadd_rn(__dsub_rn(__dmul_rn(F[0], t1), __dmul_rn(F[1], t2)), __dmul_rn(F[2], t3));
+#else
+    return F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) + F[2] * (F[3] * F[7] - F[4] * F[6]);
+#endif
 }
 
 // Node linear index with periodic wrap; -1 outside a non-periodic domain.

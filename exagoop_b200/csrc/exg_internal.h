@@ -116,6 +116,14 @@ struct Batch {
     Ctl **ctls = nullptr;                // device: each scene's control block
     void *desc[2] = {nullptr, nullptr};  // device SceneDesc<R>[n], one array per parity
     std::vector<unsigned char> desc_host[2];
+    SortDesc *sdesc[2] = {nullptr, nullptr};  // device SortDesc[n], one array per parity
+    std::vector<unsigned char> sdesc_host[2];
+    int total_blocks = 0, total_tiles = 0;    // of the per-particle and per-tile batched kernels
+    // per-stage device timing (exg_batch_set_stage_timing): events between
+    // the sort, P2G, nodal and G2P launches of eager steps
+    bool timing = false;
+    cudaEvent_t ev[5] = {};
+    double stage_ms[5] = {};
     size_t desc_bytes = 0;
     int parity = 0;                      // flips every step
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -125,6 +133,20 @@ struct Batch {
 // Uploads the scene descriptors of both parities; true when they changed.
 bool batch_descriptors_fp64(Batch &b);
 bool batch_descriptors_fp32(Batch &b);
+// Batched sort and bookkeeping of every scene (one launch per kernel):
+// step start (dt, accumulators, bounds), keys, tile scan, scatter, tile
+// sort, touched tiles, fixed-point scales, then k_batch_plan.
+void launch_batch_sort(Batch &b);
+// The batched P2G, nodal and G2P launches separately (stage timing).
+void launch_batch_p2g_fp64(Batch &b);
+void launch_batch_p2g_fp32(Batch &b);
+void launch_batch_nodes_fp64(Batch &b);
+void launch_batch_nodes_fp32(Batch &b);
+void launch_batch_g2p_fp64(Batch &b);
+void launch_batch_g2p_fp32(Batch &b);
+// Batched end of step: particles outside the domain and the time advance.
+void launch_batch_finish_fp64(Batch &b);
+void launch_batch_finish_fp32(Batch &b);
 // k_batch_plan + batched P2G, nodal and fused G2P kernels (USL step).
 void launch_batch_plan(Batch &b);
 void launch_batch_core_fp64(Batch &b);

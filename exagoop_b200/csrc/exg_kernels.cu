@@ -139,9 +139,9 @@ __device__ __forceinline__ void tile_coords(const Params &P, int t, int tc[3]) {
 // B-splines the key's "cell" is the nearest-node bin (dual_bin): particles
 // of one bin share a 3x3x3 node window.  Particles outside the domain's
 // cells are dropped either way.
-__global__ void k_keys(Params P, double *x0, double *x1, double *x2, long long n, uint32_t *key, int *tile_count,
-                       Ctl *ctl, int wrap) {
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+// (every lane of a warp calls it: the tile histogram is warp-aggregated)
+__device__ __forceinline__ void keys_body(const Params &P, double *x0, double *x1, double *x2, long long n,
+                                          uint32_t *key, int *tile_count, Ctl *ctl, int wrap, long long i) {
     int t = -1;
     if (i < n) {
         double x[3] = {x0[i], x1[i], x2[i]};
@@ -191,10 +191,15 @@ __global__ void k_keys(Params P, double *x0, double *x1, double *x2, long long n
         if ((int)(threadIdx.x & 31) == leader) atomicAdd(&tile_count[t], __popc(peers));
     }
 }
+__global__ void k_keys(Params P, double *x0, double *x1, double *x2, long long n, uint32_t *key, int *tile_count,
+                       Ctl *ctl, int wrap) {
+    keys_body(P, x0, x1, x2, n, key, tile_count, ctl, wrap, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+}
 
 // Exclusive scan of tile counts (one block): tile starts, the ascending
 // list of non-empty tiles and each tile's slot in it.
-__global__ void k_tile_scan(int ntiles, const int *count, int *start, int *active, int *slot, Ctl *ctl) {
+__device__ __forceinline__ void tile_scan_block(int ntiles, const int *count, int *start, int *active, int *slot,
+                                                Ctl *ctl) {
     __shared__ int sh[34];
     __shared__ int carry, acarry;
     if (threadIdx.x == 0) {
@@ -230,13 +235,16 @@ __global__ void k_tile_scan(int ntiles, const int *count, int *start, int *activ
         ctl->n_sorted = carry;
     }
 }
+__global__ void k_tile_scan(int ntiles, const int *count, int *start, int *active, int *slot, Ctl *ctl) {
+    tile_scan_block(ntiles, count, start, active, slot, ctl);
+}
 
 // Tiles whose owned nodes the nodal kernel writes this step: tiles next to
 // a non-empty tile (they receive P2G halo contributions), plus tiles written
 // in the previous step (their nodes return to zero, as Reset_Nodaldata_to_Zero
 // leaves them).
-__global__ void k_touched(Params P, const int *count, int *touched, long long *touched_step, Ctl *ctl) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void touched_body(const Params &P, const int *count, int *touched,
+                                             long long *touched_step, Ctl *ctl, int t) {
     if (t >= P.ntiles) return;
     int tc[3];
     tile_coords(P, t, tc);
@@ -264,9 +272,12 @@ __global__ void k_touched(Params P, const int *count, int *touched, long long *t
     }
     if (now) touched_step[t] = cur;
 }
+__global__ void k_touched(Params P, const int *count, int *touched, long long *touched_step, Ctl *ctl) {
+    touched_body(P, count, touched, touched_step, ctl, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
-__global__ void k_scatter(long long n, const uint32_t *key, int tshift3, const int *start, int *fill, int32_t *bucket) {
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void scatter_body(long long n, const uint32_t *key, int tshift3, const int *start,
+                                             int *fill, int32_t *bucket, long long i) {
     int t = -1;
     if (i < n) {
         uint32_t k = key[i];
@@ -293,6 +304,9 @@ __global__ void k_scatter(long long n, const uint32_t *key, int tshift3, const i
         bucket[start[t] + base + rank] = (int32_t)i;
     }
 }
+__global__ void k_scatter(long long n, const uint32_t *key, int tshift3, const int *start, int *fill, int32_t *bucket) {
+    scatter_body(n, key, tshift3, start, fill, bucket, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+}
 
 // Per-tile stable ordering: particles of one tile sorted by (cell, storage
 // index), which equals a stable sort of the whole array by key.
@@ -302,71 +316,78 @@ __global__ void k_scatter(long long n, const uint32_t *key, int tshift3, const i
 // occupancy sets the sort's speed: 0.223 ms against 0.257 ms at 12288 and
 // 0.237 / 0.228 / 0.224 ms at 8192 / 6144 / 4608.
 constexpr int kSortCap = 5120;
-__global__ void __launch_bounds__(kThreads) k_tile_sort(const int *active, const int *start, const int *count,
-                                                        const uint32_t *key, const int32_t *bucket, int32_t *scratch,
-                                                        int32_t *perm, int *cell_start, int ncell, Ctl *ctl) {
-    extern __shared__ int sm[];
+// One non-empty tile w of the active list, sorted by the whole block; sm
+// holds 3 ncell + kSortCap ints.
+__device__ __forceinline__ void tile_sort_item(int *sm, const int *active, const int *start, const int *count,
+                                               const uint32_t *key, const int32_t *bucket, int32_t *scratch,
+                                               int32_t *perm, int *cell_start, int ncell, Ctl *ctl, int w) {
     int *cnt = sm, *cst = sm + ncell, *fil = sm + 2 * ncell, *ent_s = sm + 3 * ncell;
     __shared__ int sh[34];
     __shared__ int smax;
     const uint32_t cm = (uint32_t)ncell - 1u;
-    const int nitems = ctl->n_active_tiles;
-    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
-        const int t = active[w];
-        const int s0 = start[t], n = count[t];
-        int32_t *ent = (n <= kSortCap) ? ent_s : scratch + s0;
-        for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
-            cnt[c] = 0;
-            fil[c] = 0;
-        }
-        if (threadIdx.x == 0) smax = 0;
-        __syncthreads();
-        for (int e = threadIdx.x; e < n; e += blockDim.x) atomicAdd(&cnt[key[bucket[s0 + e]] & cm], 1);
-        __syncthreads();
-        // exclusive scan of the per-cell counts
-        int carry = 0;
-        for (int base = 0; base < ncell; base += blockDim.x) {
-            int c = base + threadIdx.x;
-            int v = c < ncell ? cnt[c] : 0;
-            int tot;
-            int ex = block_exclusive_scan(v, &tot, sh);
-            if (c < ncell) {
-                cst[c] = carry + ex;
-                if (v > 0) atomicMax(&smax, v);
-            }
-            carry += tot;
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            int i = bucket[s0 + e];
-            int c = key[i] & cm;
-            ent[cst[c] + atomicAdd(&fil[c], 1)] = i;
-        }
-        __syncthreads();
-        for (int q = threadIdx.x; q < n; q += blockDim.x) {
-            int i = ent[q];
-            int c = key[i] & cm;
-            int b = cst[c], e = b + cnt[c];
-            int rank = 0;
-            for (int r = b; r < e; ++r) rank += (ent[r] < i);
-            perm[s0 + b + rank] = i;
-        }
-        // cell ranges of this tile (relative to the tile start), for the
-        // per-cell P2G
-        int *cs = cell_start + (long long)w * (ncell + 1);
-        for (int c = threadIdx.x; c < ncell; c += blockDim.x) cs[c] = cst[c];
-        if (threadIdx.x == 0) {
-            cs[ncell] = n;
-            atomicMax(&ctl->maxppc, smax);
-        }
-        __syncthreads();
+    const int t = active[w];
+    const int s0 = start[t], n = count[t];
+    int32_t *ent = (n <= kSortCap) ? ent_s : scratch + s0;
+    for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
+        cnt[c] = 0;
+        fil[c] = 0;
     }
+    if (threadIdx.x == 0) smax = 0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < n; e += blockDim.x) atomicAdd(&cnt[key[bucket[s0 + e]] & cm], 1);
+    __syncthreads();
+    // exclusive scan of the per-cell counts
+    int carry = 0;
+    for (int base = 0; base < ncell; base += blockDim.x) {
+        int c = base + threadIdx.x;
+        int v = c < ncell ? cnt[c] : 0;
+        int tot;
+        int ex = block_exclusive_scan(v, &tot, sh);
+        if (c < ncell) {
+            cst[c] = carry + ex;
+            if (v > 0) atomicMax(&smax, v);
+        }
+        carry += tot;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        int i = bucket[s0 + e];
+        int c = key[i] & cm;
+        ent[cst[c] + atomicAdd(&fil[c], 1)] = i;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        int i = ent[q];
+        int c = key[i] & cm;
+        int b = cst[c], e = b + cnt[c];
+        int rank = 0;
+        for (int r = b; r < e; ++r) rank += (ent[r] < i);
+        perm[s0 + b + rank] = i;
+    }
+    // cell ranges of this tile (relative to the tile start), for the
+    // per-cell P2G
+    int *cs = cell_start + (long long)w * (ncell + 1);
+    for (int c = threadIdx.x; c < ncell; c += blockDim.x) cs[c] = cst[c];
+    if (threadIdx.x == 0) {
+        cs[ncell] = n;
+        atomicMax(&ctl->maxppc, smax);
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kThreads) k_tile_sort(const int *active, const int *start, const int *count,
+                                                        const uint32_t *key, const int32_t *bucket, int32_t *scratch,
+                                                        int32_t *perm, int *cell_start, int ncell, Ctl *ctl) {
+    extern __shared__ int sm[];
+    const int nitems = ctl->n_active_tiles;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x)
+        tile_sort_item(sm, active, start, count, key, bucket, scratch, perm, cell_start, ncell, ctl, w);
 }
 
 // ---------------------------------------------------------------- bookkeeping
 // Start of step: dt from the last particle reduction (Calculate_time_step,
 // mpm_particle_timestep.cpp:38-111), current bounds, accumulators reset.
-__global__ void k_dt_finalize(Params P, Ctl *ctl, int reset) {
+__device__ __forceinline__ void dt_finalize_body(const Params &P, Ctl *ctl, int reset) {
     double dtmin = bitsd(ctl->dtmin_bits);
     double dt;
     if (P.fixed_dt)
@@ -385,12 +406,13 @@ __global__ void k_dt_finalize(Params P, Ctl *ctl, int reset) {
         ctl->n_touched_tiles = 0;
     }
 }
+__global__ void k_dt_finalize(Params P, Ctl *ctl, int reset) { dt_finalize_body(P, ctl, reset); }
 
 // Fixed-point scales: a channel's node sum is bounded by
 // (particles per cell) x (stencil cells) x (largest per-particle term);
 // the scale 2^e keeps twice that bound below 2^bits (see fx_add_r).
-__global__ void k_scales(Ctl *ctl, int stencil_cells, int bits, const unsigned long long *bounds) {
-    int c = threadIdx.x;
+__device__ __forceinline__ void scales_body(Ctl *ctl, int stencil_cells, int bits, const unsigned long long *bounds,
+                                            int c) {
     if (c == 0) ctl->next_p2g = 0;  // the P2G launch that follows takes tiles from 0
     if (c >= CH_ALL) return;
     double b = bitsd(bounds[c]);
@@ -404,6 +426,9 @@ __global__ void k_scales(Ctl *ctl, int stencil_cells, int bits, const unsigned l
     }
     ctl->scale[c] = sc;
     ctl->inv_scale[c] = 1.0 / sc;
+}
+__global__ void k_scales(Ctl *ctl, int stencil_cells, int bits, const unsigned long long *bounds) {
+    scales_body(ctl, stencil_cells, bits, bounds, threadIdx.x);
 }
 
 __global__ void k_time_advance(Ctl *ctl) {
@@ -567,20 +592,18 @@ __device__ __forceinline__ long long to_fixed<double>(double v, double sc) {
 // low word's returning add yields the carry into the high word, and the
 // value is hi * 2^32 + lo.
 constexpr int kFxBits32 = 55, kFxBits64 = 61;
+// Branch-free: adding zero words changes no sum, and the straight-line
+// code keeps a warp's lanes together.
 template <class R>
 __device__ __forceinline__ void fx_add_r(unsigned *lo, int *hi, int idx, R v, R sc) {
     const long long q = to_fixed<R>(v, sc);
-    if (!q) return;
     if (sizeof(R) == 4) {
         atomicAdd(&lo[idx], (unsigned)(q & 0xFFFFFFll));
-        const int h = (int)(q >> 24);
-        if (h) atomicAdd(&hi[idx], h);
+        atomicAdd(&hi[idx], (int)(q >> 24));
     } else {
         const unsigned l = (unsigned)(unsigned long long)q;
-        int h = (int)(q >> 32);
         const unsigned old = atomicAdd(&lo[idx], l);
-        h += (old + l < old) ? 1 : 0;
-        if (h) atomicAdd(&hi[idx], h);
+        atomicAdd(&hi[idx], (int)(q >> 32) + ((old + l < old) ? 1 : 0));
     }
 }
 template <class R>
@@ -1136,6 +1159,117 @@ __device__ __forceinline__ FactRow<R, 1> fact_row(const FactZ<R> &z, R wy, R dwy
     return r;
 }
 
+// Interior weights of all W slots from the particle's offset f in its cell
+// (cubic, slot s at z = f + 1 - s) or bin (quadratic, u = offset from the
+// bin's node, slot s at u + 1 - s): the fixed pieces of the type-3 splines,
+// the same coefficients as the tables.  FP32 evaluates two slots per packed
+// FMA.
+template <class R, int ORD>
+__device__ __forceinline__ void interior_weights(R f, R dxinv, AxisW<R, P2GStc<ORD>::W> &a) {
+    if constexpr (ORD == 3 && sizeof(R) == 4) {
+        const float o6 = (float)kOneBySix, t3 = (float)kTwoByThree, f3 = (float)kFourByThree;
+        const float2 dd = make_float2(dxinv, dxinv);
+        // slots (0, 1) at z = (f + 1, f), slots (2, 3) at z = (f - 1, f - 2)
+        const float2 za = make_float2(f + 1.f, f), zb = make_float2(f - 1.f, f - 2.f);
+        const float2 za2 = __fmul2_rn(za, za), zb2 = __fmul2_rn(zb, zb);
+        const float2 za3 = __fmul2_rn(za2, za), zb3 = __fmul2_rn(zb2, zb);
+        const float2 wa = __ffma2_rn(make_float2(-o6, 0.5f), za3,
+                                     __ffma2_rn(make_float2(1.f, -1.f), za2,
+                                                __ffma2_rn(make_float2(-2.f, 0.f), za, make_float2(f3, t3))));
+        const float2 wb = __ffma2_rn(make_float2(-0.5f, o6), zb3,
+                                     __ffma2_rn(make_float2(-1.f, 1.f), zb2,
+                                                __ffma2_rn(make_float2(0.f, 2.f), zb, make_float2(t3, f3))));
+        const float2 da = __fmul2_rn(__ffma2_rn(make_float2(-0.5f, 1.5f), za2,
+                                                __ffma2_rn(make_float2(2.f, -2.f), za, make_float2(-2.f, 0.f))),
+                                     dd);
+        const float2 db = __fmul2_rn(__ffma2_rn(make_float2(-1.5f, 0.5f), zb2,
+                                                __ffma2_rn(make_float2(-2.f, 2.f), zb, make_float2(0.f, 2.f))),
+                                     dd);
+        a.w[0] = wa.x;
+        a.w[1] = wa.y;
+        a.w[2] = wb.x;
+        a.w[3] = wb.y;
+        a.dw[0] = da.x;
+        a.dw[1] = da.y;
+        a.dw[2] = db.x;
+        a.dw[3] = db.y;
+    } else if constexpr (ORD == 3) {
+        const R o6 = (R)kOneBySix, t3 = (R)kTwoByThree, f3 = (R)kFourByThree;
+        R z = f + R(1), z2 = z * z;
+        a.w[0] = fma(-o6, z2 * z, fma(R(1), z2, fma(R(-2), z, f3)));
+        a.dw[0] = fma(R(-0.5), z2, fma(R(2), z, R(-2))) * dxinv;
+        z = f;
+        z2 = z * z;
+        a.w[1] = fma(R(0.5), z2 * z, fma(R(-1), z2, fma(R(0), z, t3)));
+        a.dw[1] = fma(R(1.5), z2, fma(R(-2), z, R(0))) * dxinv;
+        z = f - R(1);
+        z2 = z * z;
+        a.w[2] = fma(R(-0.5), z2 * z, fma(R(-1), z2, fma(R(0), z, t3)));
+        a.dw[2] = fma(R(-1.5), z2, fma(R(-2), z, R(0))) * dxinv;
+        z = f - R(2);
+        z2 = z * z;
+        a.w[3] = fma(o6, z2 * z, fma(R(1), z2, fma(R(2), z, f3)));
+        a.dw[3] = fma(R(0.5), z2, fma(R(2), z, R(2))) * dxinv;
+    } else {
+        // quadratic on the bin's nodes n0 - 1, n0, n0 + 1 (pieces
+        // [0.5, 1.5], [-0.5, 0.5], [-1.5, -0.5])
+        R z = f + R(1);
+        a.w[0] = fma(R(0.5), z * z, fma(R(-1.5), z, R(1.125)));
+        a.dw[0] = (z - R(1.5)) * dxinv;
+        z = f;
+        a.w[1] = fma(R(-1), z * z, fma(R(0), z, R(0.75)));
+        a.dw[1] = (R(-2) * z) * dxinv;
+        z = f - R(1);
+        a.w[2] = fma(R(0.5), z * z, fma(R(1.5), z, R(1.125)));
+        a.dw[2] = (z + R(1.5)) * dxinv;
+    }
+}
+
+// Weight and derivative of one slot (the task's z-slice): the interior piece
+// of that slot alone, or the boundary-aware tables.  s is warp-uniform (the
+// task mapping gives a warp one slice), so the switch does not diverge.
+template <class R, int ORD>
+__device__ __forceinline__ void slot_weight(const SplineTables &tab, const Params &P, int d, double x, int i,
+                                            bool interior, R f, int s, R &w, R &dw) {
+    const R dxinv = (R)P.dxi[d];
+    if (interior) {
+        if constexpr (ORD == 3) {
+            const R o6 = (R)kOneBySix, t3 = (R)kTwoByThree, f3 = (R)kFourByThree;
+            const R z = f + R(1 - s), z2 = z * z;
+            switch (s) {
+                case 0: w = fma(-o6, z2 * z, fma(R(1), z2, fma(R(-2), z, f3))); dw = fma(R(-0.5), z2, fma(R(2), z, R(-2))); break;
+                case 1: w = fma(R(0.5), z2 * z, fma(R(-1), z2, fma(R(0), z, t3))); dw = fma(R(1.5), z2, fma(R(-2), z, R(0))); break;
+                case 2: w = fma(R(-0.5), z2 * z, fma(R(-1), z2, fma(R(0), z, t3))); dw = fma(R(-1.5), z2, fma(R(-2), z, R(0))); break;
+                default: w = fma(o6, z2 * z, fma(R(1), z2, fma(R(2), z, f3))); dw = fma(R(0.5), z2, fma(R(2), z, R(2))); break;
+            }
+        } else {
+            const R z = f + R(1 - s);
+            switch (s) {
+                case 0: w = fma(R(0.5), z * z, fma(R(-1.5), z, R(1.125))); dw = z - R(1.5); break;
+                case 1: w = fma(R(-1), z * z, fma(R(0), z, R(0.75))); dw = R(-2) * z; break;
+                default: w = fma(R(0.5), z * z, fma(R(1.5), z, R(1.125))); dw = z + R(1.5); break;
+            }
+        }
+        dw *= dxinv;
+    } else {
+        AxisW<R, P2GStc<ORD>::W> a;
+        p2g_axis_weights<R, ORD>(tab, P, d, x, i, false, a);
+        w = pick<P2GStc<ORD>::W>(a.w, s);
+        dw = pick<P2GStc<ORD>::W>(a.dw, s);
+    }
+}
+
+// Weights of all slots of one axis: interior pieces from the offset f, the
+// tables elsewhere.
+template <class R, int ORD>
+__device__ __forceinline__ void fact_axis_weights(const SplineTables &tab, const Params &P, int d, double x, int i,
+                                                  bool interior, R f, AxisW<R, P2GStc<ORD>::W> &a) {
+    if (interior)
+        interior_weights<R, ORD>(f, (R)P.dxi[d], a);
+    else
+        p2g_axis_weights<R, ORD>(tab, P, d, x, i, false, a);
+}
+
 template <class R, int ORD, int ROWS>
 __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned *acc_lo, int *acc_hi, const Params &P,
                                               const Parts<R> &A, const int *active, const int *start,
@@ -1150,38 +1284,49 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
     tile_coords(P, t, tc);
     const int s0 = start[t];
     const int *cs = cell_start + (long long)w * (T3 + 1);
+    // task u: warp u / 32 takes one (z-slice, row group) of 32 consecutive
+    // cells, so the slice is warp-uniform; the LANES warps of a group of 32
+    // cells are consecutive and run together (the cells' particles stay in L1)
     const int ntask = LANES * T3, step = (int)blockDim.x;
     for (int u = threadIdx.x; u < ntask; u += step) {
-        const int c = u / LANES, sub = u - c * LANES;
+        const int wi = u >> 5, lane = u & 31;
+        const int grp = wi / LANES, sub = wi - grp * LANES;
+        const int c = grp * 32 + lane;
         const int sz = sub / NPASS, rg = sub - sz * NPASS;
-        const int cnext = (u + step) / LANES;
         const int ka = cs[c], kb = cs[c + 1];
-        if (EXG_P2G_PREFETCH && sub == 0 && cnext < T3) {
+        if (EXG_P2G_PREFETCH && sub == 0) {
             // L2 prefetch of the first particle of the cell this thread takes next
-            const int kn = cs[cnext];
-            if (kn < cs[cnext + 1]) {
-                const int pn = perm[s0 + kn];
-                auto pf = [](const void *q) { asm volatile("prefetch.global.L2 [%0];" ::"l"(q)); };
+            const int un = u + step, wn = un >> 5;
+            const int cnext = (wn / LANES) * 32 + (un & 31);
+            if (un < ntask && wn % LANES == 0) {
+                const int kn = cs[cnext];
+                if (kn < cs[cnext + 1]) {
+                    const int pn = perm[s0 + kn];
+                    auto pf = [](const void *q) { asm volatile("prefetch.global.L2 [%0];" ::"l"(q)); };
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    pf(A.x[d] + pn);
-                    pf(A.v[d] + pn);
+                    for (int d = 0; d < 3; ++d) {
+                        pf(A.x[d] + pn);
+                        pf(A.v[d] + pn);
+                    }
+#pragma unroll
+                    for (int c6 = 0; c6 < 6; ++c6) pf(A.sig[c6] + pn);
+                    pf(A.mass + pn);
+                    pf(A.vol + pn);
+                    pf(A.phase + pn);
                 }
-#pragma unroll
-                for (int c6 = 0; c6 < 6; ++c6) pf(A.sig[c6] + pn);
-                pf(A.mass + pn);
-                pf(A.vol + pn);
-                pf(A.phase + pn);
             }
         }
         if (ka == kb) continue;
         const int lx = c % T, ly = (c / T) % T, lz = c / (T * T);
         const int iv[3] = {tc[0] * T + lx, tc[1] * T + ly, tc[2] * T + lz};
         bool inter[3];
+        double xo[3];  // the cell's (cubic) or bin node's (quadratic) coordinate
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
+        for (int d = 0; d < 3; ++d) {
             inter[d] = P.periodic[d] ||
                        (ORD == 2 ? (iv[d] >= 3 && iv[d] <= P.nc[d] - 3) : (iv[d] >= 3 && iv[d] <= P.nc[d] - 4));
+            xo[d] = P.plo[d] + iv[d] * P.dx[d];
+        }
         FactAcc<R> acc[ROWS][W];
 #pragma unroll
         for (int r = 0; r < ROWS; ++r)
@@ -1192,14 +1337,20 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
             const int p = perm[s0 + k];
             if (A.phase[p] != 0) continue;
             const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
-            AxisW<R, W> az;
-            p2g_axis_weights<R, ORD>(*tab, P, 2, dual_x(P, 2, x[2]), iv[2], inter[2], az);
-            const R wz = pick<W>(az.w, sz), dwz = pick<W>(az.dw, sz);
+            double xw[3];
+            R f[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                xw[d] = dual_x(P, d, x[d]);
+                f[d] = (R)((xw[d] - xo[d]) * P.dxi[d]);
+            }
+            R wz, dwz;
+            slot_weight<R, ORD>(*tab, P, 2, xw[2], iv[2], inter[2], f[2], sz, wz, dwz);
             if (wz == R(0) && dwz == R(0)) continue;
             any = true;
             AxisW<R, W> ax, ay;
-            p2g_axis_weights<R, ORD>(*tab, P, 0, dual_x(P, 0, x[0]), iv[0], inter[0], ax);
-            p2g_axis_weights<R, ORD>(*tab, P, 1, dual_x(P, 1, x[1]), iv[1], inter[1], ay);
+            fact_axis_weights<R, ORD>(*tab, P, 0, xw[0], iv[0], inter[0], f[0], ax);
+            fact_axis_weights<R, ORD>(*tab, P, 1, xw[1], iv[1], inter[1], f[1], ay);
             const R m = A.mass[p], vol = A.vol[p];
             const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
                               x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] &&
@@ -1678,9 +1829,37 @@ __device__ __forceinline__ void g2p_finish(const Params &P, bool upd_vel, bool u
             v[d] = a * v[d] + a * dpic[d] + (R(1) - a) * vpic[d];
         }
     }
-    if (upd_sr) {
-        // get_deformation_gradient_tensor (interpolants.H:1732-1787) on
-        // F = I + E: E' = E + (L dt) + (L dt) E.
+    if (upd_sr && sizeof(R) == 8) {
+        // FP64 state holds F itself: get_deformation_gradient_tensor
+        // (interpolants.H:1732-1787), F <- (I + L dt) F, in the reference's
+        // operation order with every product and sum rounded on its own (no
+        // fused multiply-add), so F and J = det F follow the reference's
+        // rounding step by step
+        double nrm = 0.0;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) nrm = __dadd_rn(nrm, __dmul_rn((double)gv[a][b], (double)gv[a][b]));
+        if (!(nrm >= 1.0e10)) {
+            double L[3][3], Fo[3][3];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    const double gd = __dmul_rn((double)gv[a][b], dt);
+                    L[a][b] = (a == b) ? __dadd_rn(1.0, gd) : gd;
+                    Fo[a][b] = (double)E[a * 3 + b];
+                }
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    double acc = __dmul_rn(L[a][0], Fo[0][b]);
+                    acc = __dadd_rn(acc, __dmul_rn(L[a][1], Fo[1][b]));
+                    acc = __dadd_rn(acc, __dmul_rn(L[a][2], Fo[2][b]));
+                    E[a * 3 + b] = (R)acc;
+                }
+        }
+        int ind = 0;
+        for (int d1 = 0; d1 < 3; ++d1)
+            for (int d2 = d1; d2 < 3; ++d2) sr[ind++] = R(0.5) * (gv[d1][d2] + gv[d2][d1]);
+    } else if (upd_sr) {
+        // FP32 state holds E = F - I: the same update on F = I + E reads
+        // E' = E + (L dt) + (L dt) E, which keeps small strains resolved
         R nrm = R(0);
         for (int a = 0; a < 3; ++a)
             for (int b = 0; b < 3; ++b) nrm += gv[a][b] * gv[a][b];
@@ -1941,7 +2120,11 @@ __device__ __forceinline__ void g2p_particle_smem(const SplineTables &tab, const
         for (int d = 0; d < 3; ++d) {
             const int n0 = dual_bin(P, d, x[d]);
             const bool in = P.periodic[d] || (n0 >= 3 && n0 <= P.nc[d] - 3);
-            dual_axis_weights<R>(tab, P, d, dual_x(P, d, x[d]), n0, in, a[d]);
+            const double xw = dual_x(P, d, x[d]);
+            if (in)
+                interior_weights<R, 2>((R)((xw - (P.plo[d] + n0 * P.dx[d])) * P.dxi[d]), (R)P.dxi[d], a[d]);
+            else
+                dual_axis_weights<R>(tab, P, d, xw, n0, false, a[d]);
             base[d] = n0 - 1;
         }
         g2p_window<R, 3>(na, base, a[0].w, a[0].dw, a[1].w, a[1].dw, a[2].w, a[2].dw, upd_vel, upd_sr, vpic, dpic,
@@ -1958,7 +2141,10 @@ __device__ __forceinline__ void g2p_particle_smem(const SplineTables &tab, const
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             const bool in = P.periodic[d] || (iv[d] >= 3 && iv[d] <= P.nc[d] - 4);
-            cell_axis_weights<R, 3>(tab, P, d, x[d], iv[d], in, a[d]);
+            if (in)
+                interior_weights<R, 3>((R)((x[d] - (P.plo[d] + iv[d] * P.dx[d])) * P.dxi[d]), (R)P.dxi[d], a[d]);
+            else
+                axis_weights<R, 4, -1>(tab, P, d, x[d], iv[d], a[d]);
             base[d] = iv[d] - 1;
         }
         g2p_window<R, 4>(na, base, a[0].w, a[0].dw, a[1].w, a[1].dw, a[2].w, a[2].dw, upd_vel, upd_sr, vpic, dpic,
@@ -2088,10 +2274,12 @@ __device__ __forceinline__ void volume_stress(const Params &P, const Material &m
     double e[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) e[q] = (double)E[q];
-    // J = det F in FP64: from F = I + E with FP64 state; with FP32 state the
-    // caller's J, which follows F multiplicatively in FP64 (det(I + L dt)
-    // per F update), since det of the FP32 F would carry its rounding
-    const double det = (sizeof(R) == 8) ? det_IpE(e) : J;
+    // J = det F in FP64: with FP64 state E holds F and det F is formed in
+    // the reference's order (updateVolume, mpm_particle_timestep.cpp:160-163)
+    // without fused multiply-adds; with FP32 state (E = F - I) the caller's
+    // J, which follows F multiplicatively in FP64 (det(I + L dt) per F
+    // update), since det of the FP32 F would carry its rounding
+    const double det = (sizeof(R) == 8) ? det_ref(e) : J;
     if (do_volume) {
         const double V = (double)vol0 * det;
         J = det;
@@ -2129,13 +2317,18 @@ __device__ __forceinline__ void volume_stress(const Params &P, const Material &m
             pres = (R)pj;
             newtonian<R>(sr, sig, (R)mt.mu, (R)pj);
         } else {
-            // neo-Hookean (constitutive_models.H:161-250), FP64 from E = F - I:
-            // b - I = E + E^T + E E^T, J = max(det F, 1e-12)
+            // neo-Hookean (constitutive_models.H:161-250), FP64, J = max(det F,
+            // 1e-12): b - I from F itself (FP64 state, b = F F^T as the
+            // reference forms it) or from E = F - I (FP32 state: b - I =
+            // E + E^T + E E^T keeps small strains resolved)
             const double mu = mt.E / (2.0 * (1.0 + mt.nu));
             const double lambda = mt.E * mt.nu / ((1.0 + mt.nu) * (1.0 - 2.0 * mt.nu));
             const double Jc = fmax(det, 1.e-12);
             const double vol = lambda * log(Jc) / Jc, muJ = mu / Jc;
             auto bm = [&](int i, int j) {
+                if (sizeof(R) == 8)
+                    return (e[3 * i] * e[3 * j] + e[3 * i + 1] * e[3 * j + 1] + e[3 * i + 2] * e[3 * j + 2]) -
+                           (i == j ? 1.0 : 0.0);
                 return e[3 * i + j] + e[3 * j + i] +
                        (e[3 * i] * e[3 * j] + e[3 * i + 1] * e[3 * j + 1] + e[3 * i + 2] * e[3 * j + 2]);
             };
@@ -3048,7 +3241,7 @@ __global__ void k_batch_plan(BatchCtl *b, Ctl *const *ctls) {
     const int ns = b->nscenes;
     if (threadIdx.x == 0) {
         ca = ct = 0;
-        b->next_p2g = b->next_nodes = b->next_g2p = 0;
+        b->next_p2g = b->next_nodes = b->next_g2p = b->next_sort = 0;
     }
     __syncthreads();
     for (int base = 0; base < ns; base += blockDim.x) {
@@ -3073,6 +3266,115 @@ __global__ void k_batch_plan(BatchCtl *b, Ctl *const *ctls) {
         b->pre_active[ns] = ca;
         b->pre_touched[ns] = ct;
     }
+}
+
+#if defined(EXG_R_FP64)
+// ---- batched sort and bookkeeping: one launch of each kernel for all
+// scenes, running the single-scene bodies, so a batched scene is sorted
+// exactly as when stepped alone.  Per-particle kernels map each block to one
+// scene (BatchCtl::pre_blocks), so no warp mixes scenes; per-tile kernels map
+// threads through BatchCtl::pre_tiles.
+
+// Step start: the step's P2G bounds (those of the last G2P), dt and the
+// accumulator reset (k_dt_finalize) of scene i < nscenes by thread i; zeroed
+// tile counts of every scene.
+__global__ void k_bb_start(const SortDesc *__restrict__ d, const BatchCtl *__restrict__ b) {
+    const int ns = b->nscenes, tot = b->pre_tiles[ns];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ns) {
+        const SortDesc &x = d[i];
+        for (int c = 0; c < CH_ALL; ++c) x.bounds_cur[c] = x.ctl->bound_bits[c];
+        dt_finalize_body(x.P, x.ctl, 1);
+    }
+    if (i < tot) {
+        const int s = scene_of(b->pre_tiles, ns, i);
+        const int t = i - b->pre_tiles[s];
+        d[s].tile_count[t] = 0;
+        d[s].tile_fill[t] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(kBatchThreads) k_bb_keys(const SortDesc *__restrict__ d,
+                                                            const BatchCtl *__restrict__ b) {
+    const int s = scene_of(b->pre_blocks, b->nscenes, blockIdx.x);
+    const SortDesc &x = d[s];
+    const long long i = (long long)(blockIdx.x - b->pre_blocks[s]) * blockDim.x + threadIdx.x;
+    keys_body(x.P, x.x[0], x.x[1], x.x[2], x.np, x.key, x.tile_count, x.ctl, 1, i);
+}
+
+__global__ void k_bb_tile_scan(const SortDesc *__restrict__ d) {
+    const SortDesc &x = d[blockIdx.x];
+    tile_scan_block((int)x.P.ntiles, x.tile_count, x.tile_start, x.active, x.slot, x.ctl);
+}
+
+__global__ void __launch_bounds__(kBatchThreads) k_bb_scatter(const SortDesc *__restrict__ d,
+                                                               const BatchCtl *__restrict__ b) {
+    const int s = scene_of(b->pre_blocks, b->nscenes, blockIdx.x);
+    const SortDesc &x = d[s];
+    const long long i = (long long)(blockIdx.x - b->pre_blocks[s]) * blockDim.x + threadIdx.x;
+    scatter_body(x.np, x.key, 3 * x.P.tshift, x.tile_start, x.tile_fill, x.bucket, i);
+}
+
+// Persistent blocks over the concatenated active-tile lists (the tile order
+// of k_batch_plan's prefix sums), taken from a device counter.
+__global__ void __launch_bounds__(kThreads) k_bb_tile_sort(const SortDesc *__restrict__ d, BatchCtl *b, int ncell) {
+    extern __shared__ int sm[];
+    __shared__ int s_item, s_scene;
+    const int ns = b->nscenes, total = b->pre_active[ns];
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int i = atomicAdd(&b->next_sort, 1);
+            s_item = i;
+            s_scene = i < total ? scene_of(b->pre_active, ns, i) : -1;
+        }
+        __syncthreads();
+        const int i = s_item, s = s_scene;
+        if (i >= total) break;
+        const SortDesc &x = d[s];
+        tile_sort_item(sm, x.active, x.tile_start, x.tile_count, x.key, x.bucket, x.bucket + x.cap, x.perm,
+                       x.cell_start, ncell, x.ctl, i - b->pre_active[s]);
+    }
+}
+
+__global__ void k_bb_touched(const SortDesc *__restrict__ d, const BatchCtl *__restrict__ b) {
+    const int ns = b->nscenes, i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= b->pre_tiles[ns]) return;
+    const int s = scene_of(b->pre_tiles, ns, i);
+    const SortDesc &x = d[s];
+    touched_body(x.P, x.tile_count, x.touched, x.touched_step, x.ctl, i - b->pre_tiles[s]);
+}
+
+// One block per scene, one thread per fixed-point channel.
+__global__ void k_bb_scales(const SortDesc *__restrict__ d, int stencil_cells, int bits) {
+    const SortDesc &x = d[blockIdx.x];
+    scales_body(x.ctl, stencil_cells, bits, x.bounds_cur, threadIdx.x);
+}
+
+#endif  // EXG_R_FP64
+
+__global__ void k_bb_time_advance(const SortDesc *__restrict__ d, int ns) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ns) return;
+    Ctl *ctl = d[s].ctl;
+    ctl->time += ctl->dt;
+    ctl->steps += 1;
+}
+
+// Particles outside the domain of every scene after the batched G2P (see
+// k_copy_lost).
+template <class R>
+__global__ void __launch_bounds__(kBatchThreads) k_bb_copy_lost(const SceneDesc<R> *__restrict__ dr,
+                                                                 const SortDesc *__restrict__ d,
+                                                                 const BatchCtl *__restrict__ b, int temp) {
+    const int s = scene_of(b->pre_blocks, b->nscenes, blockIdx.x);
+    const SortDesc &x = d[s];
+    Ctl *ctl = x.ctl;
+    if (ctl->lost == 0) return;
+    const long long i = (long long)(blockIdx.x - b->pre_blocks[s]) * blockDim.x + threadIdx.x;
+    if (i >= x.np || x.key[i] != 0xFFFFFFFFu) return;
+    const long long j = ctl->n_sorted + (long long)atomicAdd(&ctl->lost_fill, 1ull);
+    Parts<R> Bo = dr[s].Bo;
+    copy_particle<R>(dr[s].A, i, Bo, j, temp != 0);
 }
 
 template <class R, int ORD, bool THERM>
@@ -3642,6 +3944,54 @@ static bool batch_descriptors_t(Batch &b) {
             EXG_CUDA_OK(cudaMemcpy(b.desc[par], h.data(), h.size(), cudaMemcpyHostToDevice));
             b.desc_host[par] = std::move(h);
         }
+        // the batched sort's view of the same scenes
+        std::vector<SortDesc> sd(n);
+        for (size_t s = 0; s < n; ++s) {
+            Ctx &c = *b.scenes[s];
+            SortDesc &x = sd[s];
+            std::memset(&x, 0, sizeof(x));
+            x.P = c.P;
+            const Parts<R> &A = (par == b.parity) ? c.A<R>() : c.Bp<R>();
+            for (int k = 0; k < 3; ++k) x.x[k] = A.x[k];
+            x.np = c.np;
+            x.cap = (int)c.cap;
+            x.key = c.sb.key;
+            x.tile_count = c.sb.tile_count;
+            x.tile_fill = c.sb.tile_fill;
+            x.tile_start = c.sb.tile_start;
+            x.active = c.sb.active;
+            x.slot = c.sb.slot;
+            x.touched = c.sb.touched;
+            x.cell_start = c.sb.cell_start;
+            x.touched_step = c.sb.touched_step;
+            x.bucket = c.sb.bucket;
+            x.perm = c.sb.perm;
+            x.ctl = c.ctl;
+            x.bounds_cur = c.bounds_cur;
+        }
+        const unsigned char *sraw = reinterpret_cast<const unsigned char *>(sd.data());
+        std::vector<unsigned char> sh(sraw, sraw + n * sizeof(SortDesc));
+        if (sh != b.sdesc_host[par]) {
+            changed = true;
+            if (!b.sdesc[par]) EXG_CUDA_OK(cudaMalloc(&b.sdesc[par], sh.size()));
+            EXG_CUDA_OK(cudaMemcpy(b.sdesc[par], sh.data(), sh.size(), cudaMemcpyHostToDevice));
+            b.sdesc_host[par] = std::move(sh);
+        }
+    }
+    // block and tile prefix sums of the batched per-particle and per-tile
+    // kernels (particle counts change only with an upload)
+    std::vector<int> pre_blocks(n + 1, 0), pre_tiles(n + 1, 0);
+    for (size_t s = 0; s < n; ++s) {
+        const Ctx &c = *b.scenes[s];
+        pre_blocks[s + 1] = pre_blocks[s] + (int)((c.np + kBatchThreads - 1) / kBatchThreads);
+        pre_tiles[s + 1] = pre_tiles[s] + (int)c.P.ntiles;
+    }
+    if (changed || pre_blocks[n] != b.total_blocks || pre_tiles[n] != b.total_tiles) {
+        EXG_CUDA_OK(cudaMemcpy(b.bctl->pre_blocks, pre_blocks.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+        EXG_CUDA_OK(cudaMemcpy(b.bctl->pre_tiles, pre_tiles.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+        b.total_blocks = pre_blocks[n];
+        b.total_tiles = pre_tiles[n];
+        changed = true;
     }
     b.desc_bytes = sizeof(SceneDesc<R>);
     return changed;
@@ -3664,32 +4014,37 @@ static void batch_g2p_t(Batch &b, const SceneDesc<R> *d, int B3) {
 }
 
 template <class R, int ORD>
-static void batch_core_t(Batch &b) {
+static void batch_p2g_t(Batch &b) {
     Ctx &c0 = *b.scenes[0];
     const SceneDesc<R> *d = reinterpret_cast<const SceneDesc<R> *>(b.desc[b.parity]);
     const int B3 = c0.P.B * c0.P.B * c0.P.B;
-    const int flags = PF_MASS | PF_VEL | PF_FORCE;
-    {
-        constexpr int NCH = CH_MOM_END;
-        const size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * NCH * B3;
-        auto kern = k_p2g_batch<R, ORD, false>;
-        constexpr int nthr = P2GCfg<R, ORD, false>::THREADS;
-        EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        static int grid = 0;
-        static size_t gsm = 0;
-        if (!grid || gsm != sm) {
-            grid = persistent_grid(kern, sm, nthr);
-            gsm = sm;
-        }
-        kern<<<grid, nthr, sm, b.stream>>>(d, b.bctl, B3);
-        EXG_CUDA_OK(cudaGetLastError());
+    constexpr int NCH = CH_MOM_END;
+    const size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * NCH * B3;
+    auto kern = k_p2g_batch<R, ORD, false>;
+    constexpr int nthr = P2GCfg<R, ORD, false>::THREADS;
+    EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    static int grid = 0;
+    static size_t gsm = 0;
+    if (!grid || gsm != sm) {
+        grid = persistent_grid(kern, sm, nthr);
+        gsm = sm;
     }
-    {
-        static int grid = 0;
-        if (!grid) grid = persistent_grid(k_nodes_batch<R, false>, 0);
-        k_nodes_batch<R, false><<<grid, kThreads, 0, b.stream>>>(d, b.bctl, NM_FUSED, flags);
-        EXG_CUDA_OK(cudaGetLastError());
-    }
+    kern<<<grid, nthr, sm, b.stream>>>(d, b.bctl, B3);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+template <class R>
+static void batch_nodes_t(Batch &b) {
+    const SceneDesc<R> *d = reinterpret_cast<const SceneDesc<R> *>(b.desc[b.parity]);
+    static int grid = 0;
+    if (!grid) grid = persistent_grid(k_nodes_batch<R, false>, 0);
+    k_nodes_batch<R, false><<<grid, kThreads, 0, b.stream>>>(d, b.bctl, NM_FUSED, PF_MASS | PF_VEL | PF_FORCE);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+template <class R, int ORD>
+static void batch_g2p_o(Batch &b) {
+    Ctx &c0 = *b.scenes[0];
+    const SceneDesc<R> *d = reinterpret_cast<const SceneDesc<R> *>(b.desc[b.parity]);
+    const int B3 = c0.P.B * c0.P.B * c0.P.B;
     bool lean = true;
     for (Ctx *s : b.scenes) lean = lean && g2p_lean(*s);
     if (lean)
@@ -3697,18 +4052,66 @@ static void batch_core_t(Batch &b) {
     else
         batch_g2p_t<R, ORD, false>(b, d, B3);
 }
-void EXG_SFX(launch_batch_core)(Batch &b) {
+void EXG_SFX(launch_batch_p2g)(Batch &b) {
     using R = EXG_R;
     switch (b.scenes[0]->P.uniform_order) {
-        case 1: batch_core_t<R, 1>(b); break;
-        case 2: batch_core_t<R, 2>(b); break;
-        case 3: batch_core_t<R, 3>(b); break;
-        default: batch_core_t<R, 0>(b); break;
+        case 1: batch_p2g_t<R, 1>(b); break;
+        case 2: batch_p2g_t<R, 2>(b); break;
+        case 3: batch_p2g_t<R, 3>(b); break;
+        default: batch_p2g_t<R, 0>(b); break;
     }
 }
+void EXG_SFX(launch_batch_nodes)(Batch &b) { batch_nodes_t<EXG_R>(b); }
+void EXG_SFX(launch_batch_g2p)(Batch &b) {
+    using R = EXG_R;
+    switch (b.scenes[0]->P.uniform_order) {
+        case 1: batch_g2p_o<R, 1>(b); break;
+        case 2: batch_g2p_o<R, 2>(b); break;
+        case 3: batch_g2p_o<R, 3>(b); break;
+        default: batch_g2p_o<R, 0>(b); break;
+    }
+}
+void EXG_SFX(launch_batch_core)(Batch &b) {
+    EXG_SFX(launch_batch_p2g)(b);
+    EXG_SFX(launch_batch_nodes)(b);
+    EXG_SFX(launch_batch_g2p)(b);
+}
+void EXG_SFX(launch_batch_finish)(Batch &b) {
+    using R = EXG_R;
+    const SceneDesc<R> *dr = reinterpret_cast<const SceneDesc<R> *>(b.desc[b.parity]);
+    if (b.total_blocks > 0)
+        k_bb_copy_lost<R><<<b.total_blocks, kBatchThreads, 0, b.stream>>>(dr, b.sdesc[b.parity], b.bctl,
+                                                                          b.scenes[0]->specs.use_temp);
+    const int ns = (int)b.scenes.size();
+    k_bb_time_advance<<<nblocks(ns), kThreads, 0, b.stream>>>(b.sdesc[b.parity], ns);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
 #if defined(EXG_R_FP64)
 void launch_batch_plan(Batch &b) {
     k_batch_plan<<<1, kThreads, 0, b.stream>>>(b.bctl, b.ctls);
+    EXG_CUDA_OK(cudaGetLastError());
+}
+
+void launch_batch_sort(Batch &b) {
+    const SortDesc *d = b.sdesc[b.parity];
+    const int ns = (int)b.scenes.size();
+    const Ctx &c0 = *b.scenes[0];
+    k_bb_start<<<nblocks(std::max(b.total_tiles, ns)), kThreads, 0, b.stream>>>(d, b.bctl);
+    if (b.total_blocks > 0) k_bb_keys<<<b.total_blocks, kBatchThreads, 0, b.stream>>>(d, b.bctl);
+    k_bb_tile_scan<<<ns, 1024, 0, b.stream>>>(d);
+    if (b.total_blocks > 0) k_bb_scatter<<<b.total_blocks, kBatchThreads, 0, b.stream>>>(d, b.bctl);
+    // active-tile prefix sums for the batched tile sort
+    k_batch_plan<<<1, kThreads, 0, b.stream>>>(b.bctl, b.ctls);
+    const int ncell = c0.P.T * c0.P.T * c0.P.T;
+    const size_t sm = sizeof(int) * (3 * ncell + kSortCap);
+    EXG_CUDA_OK(cudaFuncSetAttribute(k_bb_tile_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    static int sgrid = 0;
+    if (!sgrid) sgrid = persistent_grid(k_bb_tile_sort, sm);
+    k_bb_tile_sort<<<sgrid, kThreads, sm, b.stream>>>(d, b.bctl, ncell);
+    k_bb_touched<<<nblocks(b.total_tiles), kThreads, 0, b.stream>>>(d, b.bctl);
+    const int W = (c0.P.uniform_order == 1) ? 2 : (c0.P.dual ? 3 : 4);
+    k_bb_scales<<<ns, 32, 0, b.stream>>>(d, W * W * W, c0.precision == EXG_PREC_FP64 ? kFxBits64 : kFxBits32);
     EXG_CUDA_OK(cudaGetLastError());
 }
 #endif

@@ -149,7 +149,8 @@ EXPORTED = [
     "exg_get_stream", "exg_p2g_momentum_noalloc", "exg_batch_create", "exg_batch_destroy", "exg_batch_scene",
     "exg_batch_num_scenes", "exg_batch_step", "exg_batch_last_error", "exg_particles_alloc_pinned",
     "exg_particles_free_pinned", "exg_levelset_shape", "exg_levelset_build_device", "exg_init_levelsets",
-    "exg_get_levelset", "exg_autotune", "exg_set_variants", "exg_get_variants",
+    "exg_get_levelset", "exg_autotune", "exg_set_variants", "exg_get_variants", "exg_batch_set_stage_timing",
+    "exg_batch_last_step_timing",
 ]
 
 _lib = None
@@ -227,6 +228,8 @@ def lib() -> C.CDLL:
         "exg_batch_step": (i, [vp, i]),
         "exg_batch_last_error": (C.c_char_p, [vp]),
         "exg_autotune": (i, [vp]),
+        "exg_batch_set_stage_timing": (i, [vp, i]),
+        "exg_batch_last_step_timing": (i, [vp, pd]),
         "exg_set_variants": (i, [vp, i, i]),
         "exg_get_variants": (i, [vp, C.POINTER(i), C.POINTER(i), pd, pd]),
     }
@@ -272,6 +275,22 @@ class Particles:
             except Exception:
                 pass
             self._soa = None
+
+    def view(self, n: int) -> "Particles":
+        """A set of n particles laid out (component-major) at the start of
+        this page-locked set's memory: a staging area for smaller sets.  It
+        shares the memory and frees nothing; keep this set alive while it is
+        used."""
+        if self._soa is None or not 0 < n <= self.n:
+            raise ValueError("view needs a pinned set of at least n particles")
+        v = Particles.__new__(Particles)
+        v._soa = None
+        v._parent = self
+        s = self._soa
+        v.pos = np.ctypeslib.as_array(s.pos, shape=(3 * n,)).reshape(3, n)
+        v.rdata = np.ctypeslib.as_array(s.rdata, shape=(EXG_NREAL * n,)).reshape(EXG_NREAL, n)
+        v.idata = np.ctypeslib.as_array(s.idata, shape=(EXG_NINT * n,)).reshape(EXG_NINT, n)
+        return v
 
     def pinned_copy(self) -> "Particles":
         p = Particles(self.n, pinned=True)
@@ -631,6 +650,19 @@ class Batch:
         rc = self.L.exg_batch_step(self.h, nsteps)
         if rc:
             raise ExgError(rc, "exg_batch_step", self.L.exg_batch_last_error(self.h).decode(errors="replace"))
+
+    def stage_timing(self, on: bool):
+        rc = self.L.exg_batch_set_stage_timing(self.h, int(on))
+        if rc:
+            raise ExgError(rc, "exg_batch_set_stage_timing")
+
+    def last_step_timing(self):
+        """Mean ms per timed step: [sort + bookkeeping, p2g, nodal, g2p, steps]."""
+        out = (C.c_double * 5)()
+        rc = self.L.exg_batch_last_step_timing(self.h, out)
+        if rc:
+            raise ExgError(rc, "exg_batch_last_step_timing")
+        return list(out)
 
     def close(self):
         if self.h:

@@ -334,6 +334,13 @@ int exg_batch_num_scenes(const exg_batch *batch);
 /* nsteps explicit steps of every scene; each scene keeps its own dt and time. */
 int exg_batch_step(exg_batch *batch, int nsteps);
 const char *exg_batch_last_error(const exg_batch *batch);
+/* Per-stage device timing of batch steps, as exg_set_stage_timing for a
+ * context: while enabled, exg_batch_step runs without graph replay and
+ * records CUDA events between its stages; exg_batch_last_step_timing
+ * returns the mean ms per step since it was enabled: [sort and bookkeeping,
+ * p2g, nodal, g2p, steps timed]. */
+int exg_batch_set_stage_timing(exg_batch *batch, int on);
+int exg_batch_last_step_timing(exg_batch *batch, double *ms5);
 
 /* Deterministic device reductions of Do_All_Diagnostics (utilities.cpp:551-615). */
 int exg_diagnostics(exg_ctx *ctx, exg_diag *out);

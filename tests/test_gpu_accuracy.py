@@ -7,10 +7,13 @@ FP64 bound.  The GPU's nodal sums are exact fixed-point sums, the oracle's
 are sequential FP64 sums: the two differ by rounding (~1e-16) every step,
 and a workload amplifies such differences at its own rate (reflections at
 walls and obstacles are discontinuous in position).  The test measures that
-rate directly: the oracle against itself with every initial position,
-velocity component and diagonal entry of F moved by one ulp (an ulp of J
-moves the Tait pressure p = K((1/J)^gamma - 1) by gamma K ulp, ~3e-9 Pa for
-water: the fluid's pressure and stress are that sensitive to rounding).  The FP64 GPU path must stay within
+rate directly (tests/golden/self_divergence.json, made on the CPU by
+tests/golden/make_self_divergence.py): the oracle against itself with every
+initial position, velocity component and diagonal entry of F moved by one
+ulp (two seeds), and with its P2G summing in another order (one thread
+against many); an ulp of J moves the Tait pressure p = K((1/J)^gamma - 1) by
+gamma K ulp, ~3e-9 Pa for water, so the fluid's pressure and stress are that
+sensitive to rounding.  The FP64 GPU path must stay within
 max(1e-10, 10 x that self-divergence) in every field; on the workloads whose
 self-divergence stays below 1e-11 (the elastic spheres, the dam break) that
 is the 1e-10 of the parity tests.  Measured self-divergence after 1000 steps
@@ -25,6 +28,7 @@ flow against slip walls grows rounding by ~1e5 over 1000 steps, so its mixed
 bound is the measured 5e-2."""
 import json
 import os
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -79,23 +83,19 @@ def oracle_1000(s, p, phi):
     return o.download()
 
 
+def self_divergence(name):
+    f = Path(__file__).resolve().parent / "golden" / "self_divergence.json"
+    return json.loads(f.read_text())[name]["max"]
+
+
 @pytest.mark.parametrize("name", ["spheres", "dam_break", "twisted_column", "heated_block"])
 def test_thousand_steps_against_oracle(name):
     s, p, phi = workload(name)
     r = oracle_1000(s, p, phi)
-    # the workload's own amplification of rounding: every initial position
-    # and velocity component one ulp away (up or down, seeded)
-    q = p.copy()
-    rng = np.random.default_rng(1)
-
-    def ulp(a):
-        return np.where(rng.random(a.shape) < 0.5, np.nextafter(a, -np.inf), np.nextafter(a, np.inf))
-
-    q.pos[:] = ulp(q.pos)
-    q.rdata[nt.R_VEL:nt.R_VEL + 3] = ulp(q.rdata[nt.R_VEL:nt.R_VEL + 3])
-    for a in (0, 4, 8):  # F's diagonal: one ulp of J (the Tait pressure's sensitivity)
-        q.rdata[nt.R_DEFGRAD + a] = ulp(q.rdata[nt.R_DEFGRAD + a])
-    self_div = l2_errors(oracle_1000(s, q, phi), r, bool(s.use_temp))
+    # the workload's own amplification of rounding, measured on the CPU by
+    # tests/golden/make_self_divergence.py (ulp perturbations, the oracle's
+    # own summation order)
+    self_div = self_divergence(name)
     res = {}
     for prec, tag in [(nt.PREC_FP64, "fp64"), (nt.PREC_MIXED, "mixed")]:
         s2 = s.copy()
