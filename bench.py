@@ -315,9 +315,9 @@ def run_ours(args, rank, world):
     dev = torch.cuda.current_device()
     head, _ = measure(args, args.config, rank, world, dev, with_e2e=True, with_accuracy=(rank == 0))
     # kernels per fused step: dt_finalize, keys, tile_scan, touched, scatter,
-    # tile_sort, scales, p2g_cell, nodes, g2p_fused, copy_lost,
+    # tile_sort, scales, p2g_fact, nodes, g2p_fused, copy_lost,
     # time_advance (USL); MUSL adds reset_accum, state_reduce, scales,
-    # p2g_cell, nodes and a second g2p_fused
+    # p2g_fact, nodes and a second g2p_fused
     launches = args.steps * (12 if not head["musl"] else 18)
     prec_dtype = "f32+f64" if args.precision == "mixed" else "f64"
     line = {

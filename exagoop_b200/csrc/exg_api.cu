@@ -12,6 +12,7 @@
 #include <stdexcept>
 #include <thread>
 #include <tuple>
+#include <cudaTypedefs.h>
 #include "exg_internal.h"
 #include "exg_levelset.h"
 
@@ -490,6 +491,14 @@ int status_from_ctl(Ctx &c) {
         c.err = "fixed-point range overflow";
         return EXG_ERR_OVERFLOW;
     }
+    if (st & ST_TIMEOUT) {
+        c.err = "a node-block transfer of the fused G2P did not complete within its wait limit";
+        return EXG_ERR_TIMEOUT;
+    }
+    if (st & ST_ALIGN) {
+        c.err = "internal: the fused G2P's node-block buffer was not 128-byte aligned for TMA";
+        return EXG_ERR_CUDA;
+    }
     return EXG_OK;
 }
 
@@ -562,6 +571,44 @@ void swap_parts(Ctx &c) {
     c.orient ^= 1;
 }
 
+// Interleaved node records and the tensor map the fused G2P stages its node
+// blocks with (one 4-D box: record words x B x B x B).  Skipped on grids
+// with a periodic axis (the box cannot wrap) or when EXG_NO_TMA is set; the
+// G2P then stages with plain loads.
+void setup_node_records(Ctx &c) {
+    std::memset(&c.tmap, 0, sizeof(c.tmap));
+    c.tma = false;
+    if (c.P.periodic[0] || c.P.periodic[1] || c.P.periodic[2] || std::getenv("EXG_NO_TMA")) return;
+    const bool f64 = fp64(c);
+    const size_t esz = f64 ? 8 : 4, ns = f64 ? rec_words<double>() : rec_words<float>();
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
+        q != cudaDriverEntryPointSuccess)
+        return;
+    auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    EXG_CUDA_OK(cudaMalloc(&c.rec, esz * ns * c.P.nnodes));
+    EXG_CUDA_OK(cudaMemset(c.rec, 0, esz * ns * c.P.nnodes));
+    const cuuint64_t dims[4] = {ns, (cuuint64_t)c.P.nn[0], (cuuint64_t)c.P.nn[1], (cuuint64_t)c.P.nn[2]};
+    const cuuint64_t strides[3] = {esz * ns, esz * ns * c.P.nn[0], esz * ns * c.P.nn[0] * c.P.nn[1]};
+    const cuuint32_t box[4] = {(cuuint32_t)ns, (cuuint32_t)c.P.B, (cuuint32_t)c.P.B, (cuuint32_t)c.P.B};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = encode(&c.tmap, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                              c.rec, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        cudaFree(c.rec);
+        c.rec = nullptr;
+        return;
+    }
+    c.tma = true;
+    if (f64)
+        reinterpret_cast<Nodes<double> *>(c.nodes)->rec = reinterpret_cast<double *>(c.rec);
+    else
+        reinterpret_cast<Nodes<float> *>(c.nodes)->rec = reinterpret_cast<float *>(c.rec);
+}
+
 void drop_graphs(Ctx &c) {
     for (int k = 0; k < 2; ++k) {
         if (c.gexec[k]) cudaGraphExecDestroy(c.gexec[k]);
@@ -613,6 +660,7 @@ int exg_ctx_create(const exg_specs *specs, int device, exg_ctx **out) {
             c.nodes = N;
         }
         for (void *p : c.node_allocs) EXG_CUDA_OK(cudaMemset(p, 0, esz * c.P.nnodes));
+        setup_node_records(c);
         c.ctl = dalloc<Ctl>(1);
         EXG_CUDA_OK(cudaMemset(c.ctl, 0, sizeof(Ctl)));
         EXG_CUDA_OK(cudaMallocHost(&c.ctl_host, sizeof(Ctl)));
@@ -669,6 +717,8 @@ int exg_ctx_destroy(exg_ctx *ctx) {
     free_list(c.allocs_a);
     free_list(c.allocs_b);
     free_list(c.node_allocs);
+    if (c.rec) cudaFree(c.rec);
+    c.rec = nullptr;
     if (c.precision == EXG_PREC_FP64) {
         delete reinterpret_cast<Parts<double> *>(c.pa);
         delete reinterpret_cast<Parts<double> *>(c.pb);

@@ -29,6 +29,7 @@ enum : unsigned {
     ST_BC = 8u,
     ST_TIMEOUT = 16u,
     ST_BUCKET = 32u,
+    ST_ALIGN = 64u,  // a shared-memory staging buffer was not aligned for TMA (plain loads used)
 };
 
 // Fixed-point P2G channels.  Momentum: mass, p(3), f(3).  Thermal: m cp,
@@ -172,7 +173,15 @@ struct Material {
 template <class R>
 struct Nodes {
     R *c[EXG_N_NCOMP];
+    // interleaved copy of the fields the fused G2P reads, written by the
+    // nodal kernel of a fused step: per node v(3), dv(3) (FP32 padded to 8
+    // words, FP64 6), so one 4-D TMA box fetches a tile's whole node block in
+    // the layout the G2P uses; null when the G2P stages nodes itself
+    // (periodic axes)
+    R *rec;
 };
+template <class R>
+constexpr int rec_words() { return sizeof(R) == 4 ? 8 : 6; }
 
 // ------------------------------------------------------------------ math
 template <class R>

@@ -1,6 +1,7 @@
 // exg_internal.h -- host-side context of the B200 MPM step and the kernel
 // launchers shared by the translation units of libexg.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 #include <string>
@@ -211,6 +212,11 @@ struct Ctx {
     // by the autotuner (exg_autotune) or set by exg_set_variants
     int p2g_var = 0, g2p_var = 0;
     bool tuned = false;
+    // TMA staging of the fused G2P's node blocks: the tensor map over the
+    // nodal records (Nodes::rec), when the grid has no periodic axis
+    bool tma = false;
+    CUtensorMap tmap;
+    void *rec = nullptr;
     double tune_ms[2][4] = {};   // measured ms of each variant: [p2g/g2p][variant]
 
     template <class R>

@@ -316,6 +316,52 @@ __global__ void k_scatter(long long n, const uint32_t *key, int tshift3, const i
 // occupancy sets the sort's speed: 0.223 ms against 0.257 ms at 12288 and
 // 0.237 / 0.228 / 0.224 ms at 8192 / 6144 / 4608.
 constexpr int kSortCap = 5120;
+// A cell of up to kRankLinear particles ranks each entry by counting the
+// smaller storage indices of its cell (cnt^2 compares, cheapest for the few
+// particles of an ordinary cell); a more crowded cell (a pile-up at a wall
+// or a contact) is sorted by the whole block instead, in cnt log^2 cnt.
+constexpr int kRankLinear = 32;
+
+// Sorts a[0..L) ascending in place with a bitonic network over the next
+// power of two P >= L, the whole block taking part.  Each merge first
+// compares mirrored positions of a run, then halves, so every comparator
+// (i, j) has i < j and puts the smaller value at i; the missing entries
+// L..P-1 act as +infinity at the top and therefore never move: a comparator
+// with j >= L is skipped.
+__device__ void block_bitonic_sort(int32_t *a, int L) {
+    int P = 1;
+    while (P < L) P <<= 1;
+    for (int k = 2; k <= P; k <<= 1) {
+        const int hk = k >> 1;
+        for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
+            const int blk = t / hk, off = t - blk * hk;
+            const int i = blk * k + off, j = blk * k + k - 1 - off;
+            if (j < L) {
+                const int32_t x = a[i], y = a[j];
+                if (y < x) {
+                    a[i] = y;
+                    a[j] = x;
+                }
+            }
+        }
+        __syncthreads();
+        for (int h = hk >> 1; h >= 1; h >>= 1) {
+            for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                const int blk = t / h, off = t - blk * h;
+                const int i = blk * 2 * h + off, j = i + h;
+                if (j < L) {
+                    const int32_t x = a[i], y = a[j];
+                    if (y < x) {
+                        a[i] = y;
+                        a[j] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // One non-empty tile w of the active list, sorted by the whole block; sm
 // holds 3 ncell + kSortCap ints.
 __device__ __forceinline__ void tile_sort_item(int *sm, const int *active, const int *start, const int *count,
@@ -356,10 +402,20 @@ __device__ __forceinline__ void tile_sort_item(int *sm, const int *active, const
         ent[cst[c] + atomicAdd(&fil[c], 1)] = i;
     }
     __syncthreads();
+    if (smax > kRankLinear) {
+        // crowded cells (block-uniform: counts and smax are shared), one
+        // after another, each sorted by storage index in place
+        for (int c = 0; c < ncell; ++c)
+            if (cnt[c] > kRankLinear) block_bitonic_sort(ent + cst[c], cnt[c]);
+    }
     for (int q = threadIdx.x; q < n; q += blockDim.x) {
         int i = ent[q];
         int c = key[i] & cm;
         int b = cst[c], e = b + cnt[c];
+        if (e - b > kRankLinear) {
+            perm[s0 + q] = i;  // its cell is sorted already
+            continue;
+        }
         int rank = 0;
         for (int r = b; r < e; ++r) rank += (ent[r] < i);
         perm[s0 + b + rank] = i;
@@ -835,19 +891,20 @@ constexpr int kCellThreads = 128;
 // threads, or half a slice at 512; FP64 holds one or two rows.
 constexpr int kP2GVariants = 3;
 static_assert(kP2GVariants == EXG_NUM_VARIANTS, "the launchers dispatch EXG_NUM_VARIANTS P2G variants");
-// rows per pass, threads per block, minimum blocks per SM
-//   FP32 cubic:     (4, 256, 1)  (2, 512, 1)  (2, 256, 2)
-//   FP32 quadratic: (3, 512, 1)  (3, 256, 2)  (1, 256, 2)
-//   FP64 cubic:     (1, 512, 1)  (2, 256, 1)  (1, 256, 1)
-//   FP64 quadratic: (1, 512, 1)  (3, 256, 1)  (1, 256, 1)
+// rows per pass, threads per block, minimum blocks per SM, lane map (0: a
+// warp takes one z-slice of 32 cells, 1: a cell's slices in adjacent lanes)
+//   FP32 cubic:     (4, 256, 1, 0)  (4, 256, 1, 1)  (2, 512, 1, 0)
+//   FP32 quadratic: (3, 512, 1, 0)  (3, 512, 1, 1)  (3, 256, 2, 0)
+//   FP64 cubic:     (1, 512, 1, 1)  (2, 256, 1, 1)  (1, 512, 1, 0)
+//   FP64 quadratic: (1, 512, 1, 1)  (3, 256, 1, 1)  (1, 512, 1, 0)
 template <class R, int ORD, int V>
 struct P2GVar {
     static constexpr int K = (sizeof(R) == 4 ? 0 : 2) + (ORD == 3 ? 0 : 1);
-    static constexpr int TAB[4][3][3] = {{{4, 256, 1}, {2, 512, 1}, {2, 256, 2}},
-                                         {{3, 512, 1}, {3, 256, 2}, {1, 256, 2}},
-                                         {{1, 512, 1}, {2, 256, 1}, {1, 256, 1}},
-                                         {{1, 512, 1}, {3, 256, 1}, {1, 256, 1}}};
-    static constexpr int ROWS = TAB[K][V][0], THREADS = TAB[K][V][1], MINB = TAB[K][V][2];
+    static constexpr int TAB[4][3][4] = {{{4, 256, 1, 0}, {4, 256, 1, 1}, {2, 512, 1, 0}},
+                                         {{3, 512, 1, 0}, {3, 512, 1, 1}, {3, 256, 2, 0}},
+                                         {{1, 512, 1, 1}, {2, 256, 1, 1}, {1, 512, 1, 0}},
+                                         {{1, 512, 1, 1}, {3, 256, 1, 1}, {1, 512, 1, 0}}};
+    static constexpr int ROWS = TAB[K][V][0], THREADS = TAB[K][V][1], MINB = TAB[K][V][2], MAP = TAB[K][V][3];
 };
 
 template <class R, int ORD, bool THERM>
@@ -865,6 +922,7 @@ struct P2GCfg {
     static constexpr int THREADS = FACT ? P2GVar<R, (FACT ? ORD : 2), 0>::THREADS
                                         : ((ORD == 2) ? EXG_P2G2_THREADS : kCellThreads);
     static constexpr int MINB = FACT ? P2GVar<R, (FACT ? ORD : 2), 0>::MINB : ((ORD == 2) ? EXG_P2G2_MINB : 1);
+    static constexpr int MAP = FACT ? P2GVar<R, (FACT ? ORD : 2), 0>::MAP : 0;
 };
 
 // One tile of the per-cell P2G into its fixed-point node block (zeroed by
@@ -1270,7 +1328,7 @@ __device__ __forceinline__ void fact_axis_weights(const SplineTables &tab, const
         p2g_axis_weights<R, ORD>(tab, P, d, x, i, false, a);
 }
 
-template <class R, int ORD, int ROWS>
+template <class R, int ORD, int ROWS, int MAP>
 __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned *acc_lo, int *acc_hi, const Params &P,
                                               const Parts<R> &A, const int *active, const int *start,
                                               const int *cell_start, const int32_t *perm, long long *staging,
@@ -1284,21 +1342,34 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
     tile_coords(P, t, tc);
     const int s0 = start[t];
     const int *cs = cell_start + (long long)w * (T3 + 1);
-    // task u: warp u / 32 takes one (z-slice, row group) of 32 consecutive
-    // cells, so the slice is warp-uniform; the LANES warps of a group of 32
-    // cells are consecutive and run together (the cells' particles stay in L1)
+    // task u -> (cell, z-slice, row group).  MAP 0: warp u / 32 takes one
+    // (z-slice, row group) of 32 consecutive cells, so the slice is
+    // warp-uniform (one z weight evaluated, no divergence); the LANES warps of
+    // a group of 32 cells are consecutive and run together (the cells'
+    // particles stay in L1).  MAP 1: a cell's LANES tasks sit in adjacent
+    // lanes, which read each particle with one load.
     const int ntask = LANES * T3, step = (int)blockDim.x;
+    auto task = [&](int uu, int &cc, int &ss) {
+        if (MAP == 0) {
+            const int wi = uu >> 5, g = wi / LANES;
+            ss = wi - g * LANES;
+            cc = g * 32 + (uu & 31);
+        } else {
+            cc = uu / LANES;
+            ss = uu - cc * LANES;
+        }
+    };
     for (int u = threadIdx.x; u < ntask; u += step) {
-        const int wi = u >> 5, lane = u & 31;
-        const int grp = wi / LANES, sub = wi - grp * LANES;
-        const int c = grp * 32 + lane;
+        int c, sub;
+        task(u, c, sub);
         const int sz = sub / NPASS, rg = sub - sz * NPASS;
         const int ka = cs[c], kb = cs[c + 1];
         if (EXG_P2G_PREFETCH && sub == 0) {
             // L2 prefetch of the first particle of the cell this thread takes next
-            const int un = u + step, wn = un >> 5;
-            const int cnext = (wn / LANES) * 32 + (un & 31);
-            if (un < ntask && wn % LANES == 0) {
+            const int un = u + step;
+            int cnext = 0, sn = 1;
+            if (un < ntask) task(un, cnext, sn);
+            if (un < ntask && sn == 0) {
                 const int kn = cs[cnext];
                 if (kn < cs[cnext + 1]) {
                     const int pn = perm[s0 + kn];
@@ -1345,7 +1416,14 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
                 f[d] = (R)((xw[d] - xo[d]) * P.dxi[d]);
             }
             R wz, dwz;
-            slot_weight<R, ORD>(*tab, P, 2, xw[2], iv[2], inter[2], f[2], sz, wz, dwz);
+            if (MAP == 0) {
+                slot_weight<R, ORD>(*tab, P, 2, xw[2], iv[2], inter[2], f[2], sz, wz, dwz);
+            } else {
+                AxisW<R, W> az;
+                fact_axis_weights<R, ORD>(*tab, P, 2, xw[2], iv[2], inter[2], f[2], az);
+                wz = pick<W>(az.w, sz);
+                dwz = pick<W>(az.dw, sz);
+            }
             if (wz == R(0) && dwz == R(0)) continue;
             any = true;
             AxisW<R, W> ax, ay;
@@ -1433,8 +1511,9 @@ __global__ void __launch_bounds__(P2GVar<R, ORD, V>::THREADS, P2GVar<R, ORD, V>:
         __syncthreads();
         const int w = s_item;
         if (w >= nitems) break;
-        p2g_tile_fact<R, ORD, P2GVar<R, ORD, V>::ROWS>(tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm,
-                                                        staging, sc, grav, w);
+        p2g_tile_fact<R, ORD, P2GVar<R, ORD, V>::ROWS, P2GVar<R, ORD, V>::MAP>(tab, acc_lo, acc_hi, P, A, active,
+                                                                                start, cell_start, perm, staging,
+                                                                                sc, grav, w);
     }
 }
 
@@ -1557,6 +1636,22 @@ __device__ void node_bcs(const Params &P, const NodeBCArgs &bc, int i, int j, in
             if (applybc<double>(rin, rout, bd.wall_mu, nd, bd.mom_bc) < 0) status |= ST_BC;
             for (int d = 0; d < 3; ++d) v[d] = rout[d] + bd.wall_vel[d];
         }
+    }
+}
+
+// One node's record for the fused G2P: v and dv rounded to R as the dense
+// arrays hold them, in the layout of the G2P's shared-memory node block.
+template <class R>
+__device__ __forceinline__ void write_rec(R *rec, long long ni, const double v[3], const double dv[3]) {
+    if constexpr (sizeof(R) == 4) {
+        float *q = rec + ni * 8;
+        *reinterpret_cast<float4 *>(q) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)dv[0]);
+        *reinterpret_cast<float4 *>(q + 4) = make_float4((float)dv[1], (float)dv[2], 0.f, 0.f);
+    } else {
+        double *q = rec + ni * 6;
+        *reinterpret_cast<double2 *>(q) = make_double2(v[0], v[1]);
+        *reinterpret_cast<double2 *>(q + 2) = make_double2(v[2], dv[0]);
+        *reinterpret_cast<double2 *>(q + 4) = make_double2(dv[1], dv[2]);
     }
 }
 
@@ -1691,6 +1786,7 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
                 Nd.c[EXG_N_FRC + d][ni] = (R)f[d];
                 Nd.c[EXG_N_DVEL + d][ni] = (R)dv[d];
             }
+            if (Nd.rec) write_rec<R>(Nd.rec, ni, v, dv);
             if (THERM && (flags & PF_TEMP)) {
                 // P2G_Temperature(1,1,1), backup_current_temperature and
                 // Nodal_Time_Update_Temperature (main.cpp:100-102) on a node
@@ -1719,10 +1815,15 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
             if (m > 0.0)
                 for (int d = 0; d < 3; ++d) v[d] = (m >= P.mass_tol) ? p[d] / m : 0.0;
             node_bcs(P, bc, nid[0], nid[1], nid[2], m, v, status);
+            double dv[3];
             for (int d = 0; d < 3; ++d) {
                 Nd.c[EXG_N_VEL + d][ni] = (R)v[d];
-                if (m > 0.0) Nd.c[EXG_N_DVEL + d][ni] = (R)(v[d] - (double)Nd.c[EXG_N_DVEL + d][ni]);
+                const R dold = Nd.c[EXG_N_DVEL + d][ni];
+                const R dnew = (m > 0.0) ? (R)(v[d] - (double)dold) : dold;
+                if (m > 0.0) Nd.c[EXG_N_DVEL + d][ni] = dnew;
+                dv[d] = (double)dnew;
             }
+            if (Nd.rec) write_rec<R>(Nd.rec, ni, v, dv);
             if (THERM && (flags & PF_SRC)) {
                 // P2G_Temperature(1,0,1) of MUSL (main.cpp:133): the reset
                 // zeroes m cp and m cp T, only the source is deposited
@@ -2392,7 +2493,8 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
                                          const Parts<R> &Bo, const Nodes<R> &Nd, const NodeBCArgs &bc,
                                          const Material *mats, const int *active, const int *start, const int *count,
                                          const int32_t *perm, int mode, int w, double dt, double asr, bool upd_vel,
-                                         float (&run_b)[CH_ALL], double &run_speed, bool &red, unsigned &status) {
+                                         float (&run_b)[CH_ALL], double &run_speed, bool &red, unsigned &status,
+                                         bool staged = false) {
     const int B = P.B, B3 = B * B * B;
     const int t = active[w];
     int tc[3];
@@ -2402,16 +2504,19 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
     na.B = B;
     na.B3 = B3;
     for (int d = 0; d < 3; ++d) na.org[d] = tc[d] * P.T - P.hlo;
-    for (int idx = threadIdx.x; idx < B3; idx += blockDim.x) {
-        const int bx = idx % B, by = (idx / B) % B, bz = idx / (B * B);
-        const long long ni = node_index(P, na.org[0] + bx, na.org[1] + by, na.org[2] + bz);
-        R *q = nb + idx * SmemNodes<R>::NS;
-        for (int c = 0; c < 3; ++c) {
-            q[c] = ni >= 0 ? Nd.c[EXG_N_VEL + c][ni] : R(0);
-            q[3 + c] = ni >= 0 ? Nd.c[EXG_N_DVEL + c][ni] : R(0);
+    if (!staged) {
+        // the node block by plain loads (the caller did not stage it by TMA)
+        for (int idx = threadIdx.x; idx < B3; idx += blockDim.x) {
+            const int bx = idx % B, by = (idx / B) % B, bz = idx / (B * B);
+            const long long ni = node_index(P, na.org[0] + bx, na.org[1] + by, na.org[2] + bz);
+            R *q = nb + idx * SmemNodes<R>::NS;
+            for (int c = 0; c < 3; ++c) {
+                q[c] = ni >= 0 ? Nd.c[EXG_N_VEL + c][ni] : R(0);
+                q[3 + c] = ni >= 0 ? Nd.c[EXG_N_DVEL + c][ni] : R(0);
+            }
         }
+        __syncthreads();
     }
-    __syncthreads();
     const int s0 = start[t], n = count[t];
     // a velocity update overwrites v' of every phase-0 particle: the stored
     // v' is read only for rigid particles and for G2P without it
@@ -2564,17 +2669,69 @@ struct G2PVar {
     static constexpr int MINB = (V == 0) ? EXG_G2P_MINB : (V == 1 ? (sizeof(R) == 4 ? 4 : 1) : 1);
 };
 
+// ---- TMA staging of the G2P node block (cp.async.bulk.tensor + mbarrier)
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Arms the barrier's current phase for `bytes` of transfer (one arrival).
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// One 4-D tensor box (node-record words, x, y, z) into shared memory,
+// completing on the barrier.  Coordinates outside the tensor read zeros.
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            unsigned long long *bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for a barrier phase: gives up after kTmaWaitLimit polls (each
+// poll may itself suspend the warp for a while), so a transfer that never
+// completes ends the kernel with ST_TIMEOUT instead of hanging it.
+constexpr long long kTmaWaitLimit = 1ll << 24;
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+    for (long long it = 0; it < kTmaWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 template <class R, int ORD, bool LEAN, int V = 0>
 __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
                                                         const Material *mats, const int *active, const int *start,
-                                                        const int *count, const int32_t *perm, Ctl *ctl, int mode) {
-    extern __shared__ __align__(16) unsigned char smraw[];
+                                                        const int *count, const int32_t *perm, Ctl *ctl, int mode,
+                                                        const __grid_constant__ CUtensorMap tmap, int use_tma) {
+    extern __shared__ __align__(128) unsigned char smraw[];
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
-    R *nb = reinterpret_cast<R *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
+    const size_t tab_bytes = (sizeof(SplineTables) + 127) & ~size_t(127);
+    // The dynamic shared memory follows the kernel's static shared variables
+    // and is only 16-byte aligned, while a TMA tensor copy writes to a
+    // 128-byte aligned shared address: the node blocks start at the next
+    // 128-byte boundary after the tables (the launch adds 128 bytes for it).
+    const unsigned nb_sa = smem_addr(smraw + tab_bytes);
+    R *nb = reinterpret_cast<R *>(smraw + tab_bytes + ((128u - (nb_sa & 127u)) & 127u));
     load_tables(tab);
     const double dt = ctl->dt, time = ctl->time;
     const double asr = (time < P.applied_sr_time) ? P.applied_sr : 0.0;
     unsigned status = 0;
+    if (use_tma && (smem_addr(nb) & 127u) != 0u) {
+        // never taken with the padding above; checked before any copy is issued
+        status |= ST_ALIGN;
+        use_tma = 0;
+    }
     const bool upd_vel = (mode != GM_STRAIN);
     // running per-thread maxima of the P2G bounds (float is enough for a
     // power-of-two scale with a factor-2 margin; rounded up on conversion)
@@ -2584,15 +2741,77 @@ __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g
     double run_speed = 0.0;  // largest CFL wave speed of the thread's particles
     bool red = false;
     const int nitems = ctl->n_active_tiles;
-    __shared__ int s_item;
-    for (;;) {
-        // tiles are taken in turn from a device counter (reset by k_nodes)
-        if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_g2p, 1);
+    if (!use_tma) {
+        __shared__ int s_item;
+        for (;;) {
+            // tiles are taken in turn from a device counter (reset by k_nodes)
+            if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_g2p, 1);
+            __syncthreads();
+            const int w = s_item;
+            if (w >= nitems) break;
+            g2p_tile<R, ORD, LEAN>(tab, nb, P, A, Bo, Nd, bc, mats, active, start, count, perm, mode, w, dt, asr,
+                                   upd_vel, run_b, run_speed, red, status);
+        }
+    } else {
+        // The node block of each tile comes by one TMA box from the nodal
+        // kernel's interleaved records.  FP32: two buffers, the next tile's
+        // block loads while this tile's particles are updated; FP64 (larger
+        // blocks): one buffer, loaded between tiles.
+        constexpr int NBUF = sizeof(R) == 4 ? 2 : 1;
+        const int B = P.B;
+        const size_t buf_words = (((size_t)B * B * B * SmemNodes<R>::NS * sizeof(R) + 127) & ~size_t(127)) / sizeof(R);
+        const unsigned box_bytes = (unsigned)((size_t)B * B * B * SmemNodes<R>::NS * sizeof(R));
+        __shared__ __align__(8) unsigned long long mbar[2];
+        __shared__ int s_items[2];
+        auto issue = [&](int item, int b) {
+            int tc[3];
+            tile_coords(P, active[item], tc);
+            mbar_expect_tx(&mbar[b], box_bytes);
+            tma_load_4d(nb + b * buf_words, &tmap, 0, tc[0] * P.T - P.hlo, tc[1] * P.T - P.hlo, tc[2] * P.T - P.hlo,
+                        &mbar[b]);
+        };
+        if (threadIdx.x == 0) {
+            mbar_init(&mbar[0], 1);
+            mbar_init(&mbar[1], 1);
+            mbar_init_fence();
+            const int i = atomicAdd(&ctl->next_g2p, 1);
+            s_items[0] = i;
+            if (i < nitems) issue(i, 0);
+        }
         __syncthreads();
-        const int w = s_item;
-        if (w >= nitems) break;
-        g2p_tile<R, ORD, LEAN>(tab, nb, P, A, Bo, Nd, bc, mats, active, start, count, perm, mode, w, dt, asr, upd_vel, run_b,
-                         run_speed, red, status);
+        unsigned ph[2] = {0u, 0u};
+        int cur = 0;
+        for (;;) {
+            const int w = s_items[cur];
+            if (w >= nitems) break;
+            if (NBUF == 2 && threadIdx.x == 0) {
+                // the other buffer's last tile is done (the block synchronised)
+                const int i = atomicAdd(&ctl->next_g2p, 1);
+                s_items[cur ^ 1] = i;
+                if (i < nitems) issue(i, cur ^ 1);
+            }
+            const bool ok = mbar_wait(&mbar[cur], ph[cur]);
+            ph[cur] ^= 1u;
+            if (__syncthreads_or(!ok)) {
+                // a transfer did not complete: flag it, and before leaving
+                // wait (bounded) for the other buffer's transfer in flight
+                status |= ST_TIMEOUT;
+                if (NBUF == 2 && s_items[cur ^ 1] < nitems) mbar_wait(&mbar[cur ^ 1], ph[cur ^ 1]);
+                break;
+            }
+            g2p_tile<R, ORD, LEAN>(tab, nb + cur * buf_words, P, A, Bo, Nd, bc, mats, active, start, count, perm,
+                                   mode, w, dt, asr, upd_vel, run_b, run_speed, red, status, true);
+            if (NBUF == 2) {
+                cur ^= 1;
+            } else {
+                if (threadIdx.x == 0) {
+                    const int i = atomicAdd(&ctl->next_g2p, 1);
+                    s_items[0] = i;
+                    if (i < nitems) issue(i, 0);
+                }
+                __syncthreads();
+            }
+        }
     }
     if (mode != GM_VEL) {
         double rb[CH_ALL];
@@ -3412,9 +3631,9 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
             for (int d = 0; d < 3; ++d) grav[d] = (R)sd.P.gravity[d];
         }
         if constexpr (P2GCfg<R, ORD, THERM>::FACT)
-            p2g_tile_fact<R, ORD, P2GCfg<R, ORD, THERM>::ROWS>(tab, acc_lo, acc_hi, sd.P, sd.A, sd.active, sd.start,
-                                                                sd.cell_start, sd.perm, sd.staging, sc, grav,
-                                                                i - b->pre_active[s]);
+            p2g_tile_fact<R, ORD, P2GCfg<R, ORD, THERM>::ROWS, P2GCfg<R, ORD, THERM>::MAP>(
+                tab, acc_lo, acc_hi, sd.P, sd.A, sd.active, sd.start, sd.cell_start, sd.perm, sd.staging, sc, grav,
+                i - b->pre_active[s]);
         else
             p2g_tile<R, ORD, THERM>(tab, acc_lo, acc_hi, sd.P, sd.A, sd.active, sd.start, sd.cell_start, sd.perm,
                                     sd.staging, sc, grav, i - b->pre_active[s]);
@@ -3724,7 +3943,12 @@ void EXG_SFX(launch_nodes)(Ctx &c, int mode, int flags, bool all_tiles) {
 template <class R, int ORD, bool LEAN, int V = 0>
 static void g2p_lt(Ctx &c, int mode) {
     const int B3 = c.P.B * c.P.B * c.P.B;
-    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(R) * SmemNodes<R>::NS * B3;
+    // tables, then one node block (two with TMA staging in FP32), each
+    // 128-byte aligned
+    const size_t tabb = (sizeof(SplineTables) + 127) & ~size_t(127);
+    const size_t buf = (sizeof(R) * SmemNodes<R>::NS * B3 + 127) & ~size_t(127);
+    const int nbuf = (c.tma && sizeof(R) == 4) ? 2 : 1;
+    size_t sm = tabb + nbuf * buf + 128;  // + room to align the node blocks to 128 bytes
     auto kern = k_g2p_fused<R, ORD, LEAN, V>;
     constexpr int nthr = G2PVar<R, V>::THREADS;
     EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -3735,7 +3959,8 @@ static void g2p_lt(Ctx &c, int mode) {
         gsm = sm;
     }
     kern<<<grid, nthr, sm, c.stream>>>(c.P, c.A<R>(), c.Bp<R>(), c.N<R>(), make_bc(c), c.mat_dev, c.sb.active,
-                                       c.sb.tile_start, c.sb.tile_count, c.sb.perm, c.ctl, mode);
+                                       c.sb.tile_start, c.sb.tile_count, c.sb.perm, c.ctl, mode, c.tmap,
+                                       c.tma ? 1 : 0);
     EXG_CUDA_OK(cudaGetLastError());
 }
 template <class R, int ORD>

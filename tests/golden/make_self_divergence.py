@@ -11,7 +11,10 @@ Probes, each against the oracle run on all host threads:
               of F one ulp up or down (two seeds);
   order       the oracle on one thread (its P2G sums nodes in particle
               order; on many threads OpenMP atomics interleave the threads'
-              contributions, as the reference's GPU atomics do).
+              contributions, as the reference's GPU atomics do);
+  noise       after every step, every position, velocity and stress
+              component one ulp up or down (a two-ulp spread, as two
+              correct implementations round each step's results apart).
 The workloads and sizes are those of tests/test_gpu_accuracy.py.  CPU only;
 run from the repository root (it takes a few minutes):
 
@@ -47,6 +50,27 @@ def run(s, p, phi, threads):
     return o.download()
 
 
+def run_noisy(s, p, phi, threads, seed):
+    o = orc.Oracle(s, threads=threads)
+    o.upload(p)
+    if phi is not None:
+        o.set_levelset(0, phi)
+    o.init_internal_forces()
+    rng = np.random.default_rng(seed)
+
+    def ulp(a):
+        return np.where(rng.random(a.shape) < 0.5, np.nextafter(a, -np.inf), np.nextafter(a, np.inf))
+
+    for _ in range(1000):
+        assert o.step(1) == 0
+        q = o.download()
+        q.pos[:] = ulp(q.pos)
+        q.rdata[nt.R_VEL:nt.R_VEL + 3] = ulp(q.rdata[nt.R_VEL:nt.R_VEL + 3])
+        q.rdata[nt.R_STRESS:nt.R_STRESS + 6] = ulp(q.rdata[nt.R_STRESS:nt.R_STRESS + 6])
+        o.upload(q)
+    return o.download()
+
+
 def perturbed(p, seed):
     q = p.copy()
     rng = np.random.default_rng(seed)
@@ -72,6 +96,7 @@ def main():
             "ulp1": acc.l2_errors(run(s, perturbed(p, 1), phi, threads), base, th),
             "ulp2": acc.l2_errors(run(s, perturbed(p, 2), phi, threads), base, th),
             "order": acc.l2_errors(run(s, p, phi, 1), base, th),
+            "noise": acc.l2_errors(run_noisy(s, p, phi, threads, 3), base, th),
         }
         fields = probes["ulp1"].keys()
         out[name] = {"max": {f: max(pr[f] for pr in probes.values()) for f in fields}, "probes": probes,

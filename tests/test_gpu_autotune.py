@@ -1,5 +1,5 @@
 """The launch-variant autotuner (exg_autotune, exg_set_variants,
-exg_get_variants).  Every P2G variant (rows per pass x threads per block)
+exg_get_variants), and the fused G2P's two ways of staging node blocks.  Every P2G variant (rows per pass x threads per block)
 and every fused-G2P variant (threads per block x blocks per SM) must give
 bit-identical particles after fused steps: the P2G sums each node over a
 cell's particles in storage order with the same expression whatever the
@@ -94,3 +94,16 @@ def test_set_variants_rejects_out_of_range():
     with pytest.raises(nt.ExgError):
         ctx.set_variants(0, -2)
     ctx.close()
+
+
+@pytest.mark.parametrize("name", ["spheres_cubic", "dam_break_quadratic"])
+@pytest.mark.parametrize("precision", [nt.PREC_MIXED, nt.PREC_FP64])
+def test_tma_and_plain_node_staging_agree(name, precision, monkeypatch):
+    # the fused G2P stages each tile's node block by one TMA box from the
+    # nodal records, or (EXG_NO_TMA, and on periodic grids) by plain loads:
+    # the same values in the same layout, so the steps agree bit for bit
+    s, p = small(name, precision)
+    ref, _ = run(s, p, 8, 0, 0)
+    monkeypatch.setenv("EXG_NO_TMA", "1")
+    got, _ = run(s, p, 8, 0, 0)
+    assert same(got, ref)

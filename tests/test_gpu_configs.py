@@ -119,8 +119,9 @@ def diag_close(a, b, tol):
 
 def check_diag(gd, od, g=None, r=None):
     """Diagnostics parity in two parts: each side's reductions equal the
-    reference's formulas evaluated on that side's own particles (1e-12;
-    the GPU reduces in a fixed two-pass order, the oracle sequentially),
+    reference's formulas evaluated on that side's own particles (the GPU
+    reduces in a fixed two-pass tree, within 1e-12; the oracle sequentially,
+    within n eps),
     and the two sides' particles agree field by field (the parity checks).
     Directly against each other the aggregates agree within 1e-9 (sums of
     fields that agree to 1e-10 of their max norm, some cancelling), the
@@ -128,7 +129,9 @@ def check_diag(gd, od, g=None, r=None):
     if g is not None:
         diag_close(gd, diag_from_particles(g), 1e-12)
     if r is not None:
-        diag_close(od, diag_from_particles(r), 1e-12)
+        # the oracle sums sequentially, as a single-threaded reduction does:
+        # its rounding grows with the particle count (n eps)
+        diag_close(od, diag_from_particles(r), max(1e-12, 2.2e-16 * r.n))
     assert gd["mass"] == pytest.approx(od["mass"], rel=1e-12)
     assert gd["np"] == od["np"]
     for k in ("tke", "tse", "mwa_velmag"):

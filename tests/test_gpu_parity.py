@@ -79,6 +79,25 @@ def test_sort_bitexact_clustered():
     assert np.array_equal(keys, okeys) and np.array_equal(perm, operm)
 
 
+@pytest.mark.parametrize("pile", [33, 40, 300, 3000])
+def test_sort_bitexact_crowded_cells(pile):
+    # cells above the linear-rank limit (32) are sorted by the whole block:
+    # several crowded cells in one tile, sizes just above the limit, not a
+    # power of two, and one tile past the shared-memory capacity (5120)
+    s, p = random_scene(12, npart=24000)
+    rng = np.random.default_rng(pile)
+    lo = np.array([s.plo[d] for d in range(3)])
+    dx = np.array([(s.phi[d] - s.plo[d]) / s.ncells[d] for d in range(3)])
+    for k in range(6):
+        c = lo + (np.array([3, 4 + (k % 2), 3 + k // 2]) + 0.5) * dx
+        idx = rng.choice(p.n, size=pile, replace=False)
+        p.pos[:, idx] = c[:, None] + (rng.random((3, pile)) - 0.5) * 0.9 * dx[:, None]
+    ctx, o = pair(s, p)
+    keys, perm = ctx.sort_keys()
+    okeys, operm = o.sort_keys(ctx.tile())
+    assert np.array_equal(keys, okeys) and np.array_equal(perm, operm)
+
+
 @pytest.mark.parametrize("order", [1, 2, 3])
 def test_p2g_momentum(order):
     s, p = random_scene(20 + order, order=order)

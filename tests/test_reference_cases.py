@@ -111,9 +111,15 @@ def test_reference_case_against_oracle(name):
     o.init_internal_forces()
     assert o.step(n) == 0
     r = o.download()
-    for f, k in [(nt.R_VEL, 3), (nt.R_STRESS, 6), (nt.R_DEFGRAD, 9), (nt.R_DENSITY, 1)]:
+    # stresses are compared against the stress of a 1e-5 strain of the
+    # stiffest modulus: the elastic block translates rigidly, so its stress
+    # is rounding noise (~1e-16 of the modulus) that two correct codes need
+    # not share; 1e-10 of that floor is 1e-15 of the modulus
+    stiff = max(r.rdata[nt.R_E].max(), r.rdata[nt.R_BULK].max())
+    for f, k, floor in [(nt.R_VEL, 3, 0.0), (nt.R_STRESS, 6, 1e-5 * stiff), (nt.R_DEFGRAD, 9, 0.0),
+                        (nt.R_DENSITY, 1, 0.0)]:
         b = r.rdata[f:f + k]
-        assert np.abs(g.rdata[f:f + k] - b).max() <= 1e-10 * max(np.abs(b).max(), 1e-300), f
+        assert np.abs(g.rdata[f:f + k] - b).max() <= 1e-10 * max(np.abs(b).max(), floor, 1e-300), f
     assert np.abs(g.pos - r.pos).max() < 1e-12
 
 
