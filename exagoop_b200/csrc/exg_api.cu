@@ -678,12 +678,14 @@ int exg_ctx_create(const exg_specs *specs, int device, exg_ctx **out) {
         c.sb.touched = dalloc<int>(nt);
         c.sb.touched_step = dalloc<long long>(nt);
         c.sb.cell_start = dalloc<int>((size_t)nt * (c.P.T * c.P.T * c.P.T + 1));
+        c.sb.item_start = dalloc<int>(nt + 1);
         EXG_CUDA_OK(cudaMemset(c.sb.touched_step, 0xff, sizeof(long long) * nt));  // -1: never
         EXG_CUDA_OK(cudaMemset(c.sb.slot, 0xff, sizeof(int) * nt));
         c.nch = specs->use_temp ? CH_ALL : CH_MOM_END;
         const long long B3 = (long long)c.P.B * c.P.B * c.P.B;
         c.staging_cap = (size_t)nt;
-        c.staging = dalloc<long long>((size_t)nt * c.nch * B3);
+        c.staging = dalloc<long long>((size_t)nt * (c.precision == EXG_PREC_FP64 ? stg_stride<double>(c.nch * B3)
+                                                                                 : stg_stride<float>(c.nch * B3)));
         if (specs->use_temp) {
             // thermal wall pass: one entry per node of each non-periodic face
             c.n_tface = 0;
@@ -736,7 +738,8 @@ int exg_ctx_destroy(exg_ctx *ctx) {
     cudaFree(c.tface);
     cudaFree(c.ttmp);
     void *bufs[] = {c.sb.key, c.sb.perm, c.sb.bucket, c.sb.tile_count, c.sb.tile_fill, c.sb.tile_start,
-                    c.sb.active, c.sb.slot, c.sb.touched, c.sb.touched_step, c.sb.cell_start, c.staging, c.ctl,
+                    c.sb.active, c.sb.slot, c.sb.touched, c.sb.touched_step, c.sb.cell_start, c.sb.item_start,
+                    c.staging, c.ctl,
                     c.bounds_cur, c.bounds2, c.dtmin2, c.mat_dev, c.diag_dev, c.stage};
     for (void *p : bufs) cudaFree(p);
     if (c.ctl_host) cudaFreeHost(c.ctl_host);
@@ -956,6 +959,7 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
                 upload_parts<float>(c, p, mat);
             set_tref(c, p);
             c.parts_sorted = false;
+            c.reordered = false;
             c.reduce_stale = true;
             sync(c);
             return EXG_OK;
@@ -1001,6 +1005,7 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
         c.sb.perm = dalloc<int32_t>(n);
         c.sb.bucket = dalloc<int32_t>(2 * n);
         c.parts_sorted = false;
+        c.reordered = false;
         c.reduce_stale = true;
         sync(c);
     });
@@ -1416,8 +1421,11 @@ void autotune_impl(Ctx &c) {
 }
 
 // The choice for this context: the process cache when it holds one for this
-// kind of context, otherwise a tuning run.  Graphs captured with other
-// variants are dropped.
+// kind of context, otherwise a tuning run, but only on particles in the
+// order a fused step leaves them (right after an upload they are in the
+// caller's order, whose scattered loads would rank the variants wrongly; the
+// first step then runs with the current variants, which give the same
+// results).  Graphs captured with other variants are dropped.
 void ensure_tuned(Ctx &c) {
     if (c.tuned) return;
     const int p0 = c.p2g_var, g0 = c.g2p_var;
@@ -1433,7 +1441,7 @@ void ensure_tuned(Ctx &c) {
     }
     if (hit)
         c.tuned = true;
-    else
+    else if (c.reordered)
         autotune_impl(c);
     if (c.p2g_var != p0 || c.g2p_var != g0) drop_graphs(c);
 }
@@ -1483,11 +1491,13 @@ int exg_step(exg_ctx *ctx, int nsteps) {
     Ctx &c = ctx->c;
     if (c.np == 0) return fail(ctx, EXG_ERR_NOT_READY, "no particles");
     EXG_TRY(ctx, {
-        if (c.specs.autotune && nsteps > 0) ensure_tuned(c);
+        const bool tune = c.specs.autotune && nsteps > 0;
+        if (tune) ensure_tuned(c);
         if (c.reduce_stale) do_reduce(c);
         const bool host_dep = has_udf(c) || (c.specs.use_temp && has_udf_temp(c));
         const bool use_graph = !host_dep && !c.timing && std::getenv("EXG_NO_GRAPH") == nullptr;
         for (int s = 0; s < nsteps; ++s) {
+            if (tune && !c.tuned && c.reordered) ensure_tuned(c);
             if (host_dep) {
                 // UDF wall tables depend on the step's start time: tabulate on
                 // the host before the step's kernels.
@@ -1504,6 +1514,7 @@ int exg_step(exg_ctx *ctx, int nsteps) {
                         enqueue_step(c);
                         c.warm[c.orient] = true;
                         swap_parts(c);
+                        c.reordered = true;
                         continue;
                     }
                     cudaGraph_t graph = nullptr;
@@ -1515,9 +1526,11 @@ int exg_step(exg_ctx *ctx, int nsteps) {
                 }
                 EXG_CUDA_OK(cudaGraphLaunch(g, c.stream));
                 swap_parts(c);
+                c.reordered = true;
             } else {
                 enqueue_step(c);
                 swap_parts(c);
+                c.reordered = true;
                 if (c.timing) {
                     sync(c);
                     float ms[4];

@@ -57,8 +57,23 @@ struct Ctl {
     long long n_sorted;                // particles inside the domain after the sort
     unsigned long long lost_fill;      // next slot for out-of-domain particles in the re-ordered storage
     int next_p2g;                      // dynamic tile counter of the P2G kernel (reset by k_scales)
-    int next_g2p;                      // dynamic tile counter of the fused G2P (reset by k_nodes)
+    int next_g2p;                      // dynamic item counter of the fused G2P (reset by k_nodes)
+    int n_g2p_items;                   // work items of the fused G2P (chunks of kG2PChunk particles of a tile)
+    int pad2;
 };
+// Particles of one work item of the fused G2P: a tile of more particles
+// (a pile-up) is split into several items, so that no item is much longer
+// than an ordinary tile.  Each item stages its tile's node block again, so
+// ordinary tiles (8 particles per cell of an 8^3 tile) stay whole: items of
+// 1024 made the 9 M-particle sphere step's G2P 5 % slower (FP64, whose node
+// block arrives single-buffered, 15 %).
+constexpr int kG2PChunk = 4096;
+
+// Per-tile stride of the P2G staging array, in 64-bit words, for nv
+// fixed-point values: FP32 state one 64-bit integer per value; FP64 state
+// the 64-bit low words, then the 32-bit high words (96-bit values).
+template <class R>
+EXG_HD constexpr long long stg_stride(long long nv) { return sizeof(R) == 4 ? nv : nv + (nv + 1) / 2; }
 
 // Control block of a batch of independent scenes advanced by one launch per
 // kernel: prefix sums of the scenes' tile counts and the batch's dynamic
@@ -136,7 +151,7 @@ struct SortDesc {
     long long np;
     int cap;  // sort scratch (tiles above the shared-memory cap) starts at bucket + cap
     uint32_t *key;
-    int *tile_count, *tile_fill, *tile_start, *active, *slot, *touched, *cell_start;
+    int *tile_count, *tile_fill, *tile_start, *active, *slot, *touched, *cell_start, *item_start;
     long long *touched_step;
     int32_t *bucket, *perm;
     Ctl *ctl;

@@ -61,6 +61,7 @@ struct SortBufs {
     int *touched = nullptr;      // [ntiles] tiles whose nodes the nodal kernel writes
     long long *touched_step = nullptr;  // [ntiles] last step the tile was touched
     int *cell_start = nullptr;   // [ntiles][T^3 + 1] per-cell particle ranges of each non-empty tile
+    int *item_start = nullptr;   // [ntiles + 1] first fused-G2P work item of each active tile
 };
 
 struct Ctx;
@@ -212,6 +213,9 @@ struct Ctx {
     // by the autotuner (exg_autotune) or set by exg_set_variants
     int p2g_var = 0, g2p_var = 0;
     bool tuned = false;
+    // the particles are in the order a fused step leaves them (tile-major,
+    // as every later step sees them): set by exg_step, cleared by uploads
+    bool reordered = false;
     // TMA staging of the fused G2P's node blocks: the tensor map over the
     // nodal records (Nodes::rec), when the grid has no periodic axis
     bool tma = false;

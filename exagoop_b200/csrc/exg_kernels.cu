@@ -197,28 +197,33 @@ __global__ void k_keys(Params P, double *x0, double *x1, double *x2, long long n
 }
 
 // Exclusive scan of tile counts (one block): tile starts, the ascending
-// list of non-empty tiles and each tile's slot in it.
+// list of non-empty tiles, each tile's slot in it, and the first fused-G2P
+// work item of each active tile (ceil(count / kG2PChunk) items a tile).
 __device__ __forceinline__ void tile_scan_block(int ntiles, const int *count, int *start, int *active, int *slot,
-                                                Ctl *ctl) {
+                                                int *item_start, Ctl *ctl) {
     __shared__ int sh[34];
-    __shared__ int carry, acarry;
+    __shared__ int carry, acarry, icarry;
     if (threadIdx.x == 0) {
         carry = 0;
         acarry = 0;
+        icarry = 0;
     }
     __syncthreads();
     for (int base = 0; base < ntiles; base += blockDim.x) {
         int i = base + threadIdx.x;
         int c = i < ntiles ? count[i] : 0;
         int a = c > 0;
-        int tc, ta;
+        int it = (c + kG2PChunk - 1) / kG2PChunk;
+        int tc, ta, ti;
         int ec = block_exclusive_scan(c, &tc, sh);
         int ea = block_exclusive_scan(a, &ta, sh);
+        int ei = block_exclusive_scan(it, &ti, sh);
         if (i < ntiles) {
             start[i] = carry + ec;
             if (a) {
                 active[acarry + ea] = i;
                 slot[i] = acarry + ea;
+                item_start[acarry + ea] = icarry + ei;
             } else {
                 slot[i] = -1;
             }
@@ -227,16 +232,20 @@ __device__ __forceinline__ void tile_scan_block(int ntiles, const int *count, in
         if (threadIdx.x == 0) {
             carry += tc;
             acarry += ta;
+            icarry += ti;
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
         ctl->n_active_tiles = acarry;
         ctl->n_sorted = carry;
+        ctl->n_g2p_items = icarry;
+        item_start[acarry] = icarry;
     }
 }
-__global__ void k_tile_scan(int ntiles, const int *count, int *start, int *active, int *slot, Ctl *ctl) {
-    tile_scan_block(ntiles, count, start, active, slot, ctl);
+__global__ void k_tile_scan(int ntiles, const int *count, int *start, int *active, int *slot, int *item_start,
+                            Ctl *ctl) {
+    tile_scan_block(ntiles, count, start, active, slot, item_start, ctl);
 }
 
 // Tiles whose owned nodes the nodal kernel writes this step: tiles next to
@@ -477,8 +486,10 @@ __device__ __forceinline__ void scales_body(Ctl *ctl, int stencil_cells, int bit
     if (S > 0.0 && S < 1e300) {
         int ex;
         frexp(S, &ex);  // S < 2^ex
-        // 2^e stays inside FP32's range; a channel this small contributes 0
-        sc = ldexp(1.0, max(-100, min(100, bits - ex)));
+        // 2^e stays inside the state's range (FP32: |e| <= 100); a channel
+        // this small contributes 0
+        const int lim = bits > 64 ? 900 : 100;
+        sc = ldexp(1.0, max(-lim, min(lim, bits - ex)));
     }
     ctl->scale[c] = sc;
     ctl->inv_scale[c] = 1.0 / sc;
@@ -639,34 +650,102 @@ __device__ __forceinline__ long long to_fixed<double>(double v, double sc) {
     return __double2ll_rn(v * sc);
 }
 
-// A node's fixed-point sum is kept in two 32-bit shared-memory words.
-// FP32 state (scale bound 2^55, kFxBits32): without carries, lo collects the
-// low 24 bits of each addend (at most 64 addends per node and tile, so
-// lo < 2^30) and hi the arithmetic upper part, which fits 32 bits; the value
-// is hi * 2^24 + lo and both adds are fire-and-forget reductions.  FP64
-// state (bound 2^61, kFxBits64, the full precision the FP64 path needs): the
-// low word's returning add yields the carry into the high word, and the
-// value is hi * 2^32 + lo.
-constexpr int kFxBits32 = 55, kFxBits64 = 61;
+// A node's fixed-point sum in shared memory.
+// FP32 state (scale bound 2^55, kFxBits32): two 32-bit words; without
+// carries, lo collects the low 24 bits of each addend (at most 64 addends
+// per node and tile, so lo < 2^30) and hi the arithmetic upper part, which
+// fits 32 bits; the value is hi * 2^24 + lo and both adds are
+// fire-and-forget reductions.
+// FP64 state (bound 2^93, kFxBits64): a 64-bit low word and a 32-bit high
+// word, value hi * 2^64 + lo; the low word's returning add yields the carry.
+// The 93 bits keep the FP64 mantissa of a node whose sum is 2^-40 of the
+// channel's bound: a node reached only by the edge of a few particles'
+// supports has a mass that small, and its velocity p / m, which the
+// velocity gradient weights by the slowly vanishing dN, needs relative, not
+// absolute, precision.
+constexpr int kFxBits32 = 55, kFxBits64 = 93;
+// 32-bit words of the low part of one fixed-point value (shared memory)
+template <class R>
+__host__ __device__ constexpr int fx_lo_words() { return sizeof(R) == 4 ? 1 : 2; }
+
+// The FP64 addend x = v * sc (|x| < 2^93) as hi * 2^64 + lo.  Below 2^63 in
+// magnitude it is the rounded 64-bit integer, sign-extended; above, x is an
+// integer already and hi = floor(x / 2^64) and lo = x - hi 2^64 are exact.
+// Both are formed and one is selected (no divergence).
+__device__ __forceinline__ void fx_split64(double x, unsigned long long &lo, int &hi) {
+    const long long q = __double2ll_rn(x);
+    const double h = floor(x * 0x1p-64);
+    const double r = fma(-h, 0x1p64, x);
+    const bool small = fabs(x) < 0x1p63;
+    lo = small ? (unsigned long long)q : __double2ull_rn(r);
+    hi = small ? (q < 0 ? -1 : 0) : (int)h;
+}
+
 // Branch-free: adding zero words changes no sum, and the straight-line
 // code keeps a warp's lanes together.
 template <class R>
 __device__ __forceinline__ void fx_add_r(unsigned *lo, int *hi, int idx, R v, R sc) {
-    const long long q = to_fixed<R>(v, sc);
     if (sizeof(R) == 4) {
+        const long long q = to_fixed<R>(v, sc);
         atomicAdd(&lo[idx], (unsigned)(q & 0xFFFFFFll));
         atomicAdd(&hi[idx], (int)(q >> 24));
     } else {
-        const unsigned l = (unsigned)(unsigned long long)q;
-        const unsigned old = atomicAdd(&lo[idx], l);
-        atomicAdd(&hi[idx], (int)(q >> 32) + ((old + l < old) ? 1 : 0));
+        unsigned long long l;
+        int h;
+        fx_split64((double)v * (double)sc, l, h);
+        unsigned long long *lo64 = reinterpret_cast<unsigned long long *>(lo);
+        const unsigned long long old = atomicAdd(&lo64[idx], l);
+        atomicAdd(&hi[idx], h + ((old + l < old) ? 1 : 0));
     }
 }
+// Zeroes the tile's fixed-point block (n values) in shared memory.
 template <class R>
-__device__ __forceinline__ long long fx_value(unsigned lo, int hi) {
-    if (sizeof(R) == 4) return (long long)hi * (1ll << 24) + (long long)lo;
-    return (long long)((((unsigned long long)(unsigned)hi) << 32) + (unsigned long long)lo);
+__device__ __forceinline__ void fx_zero(unsigned *lo, int *hi, int n) {
+    for (int i = threadIdx.x; i < n * fx_lo_words<R>(); i += blockDim.x) lo[i] = 0u;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) hi[i] = 0;
 }
+// Writes the tile's fixed-point block (n values) to its staging slot: FP32
+// one 64-bit integer per value; FP64 the 64-bit low words, then the 32-bit
+// high words.
+template <class R>
+__device__ __forceinline__ void fx_store(const unsigned *lo, const int *hi, int n, long long *dst) {
+    if (sizeof(R) == 4) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = (long long)hi[i] * (1ll << 24) + (long long)lo[i];
+    } else {
+        const unsigned long long *lo64 = reinterpret_cast<const unsigned long long *>(lo);
+        int *dh = reinterpret_cast<int *>(dst + n);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            dst[i] = (long long)lo64[i];
+            dh[i] = hi[i];
+        }
+    }
+}
+// A node's sum over its partial blocks: FP32 a 64-bit integer; FP64 a 128-bit
+// two's-complement pair (hi carries the low words' overflow).
+template <class R>
+struct FxSum {
+    long long v = 0;
+    __device__ __forceinline__ void add(const long long *blk, long long nv, long long i) { v += blk[i]; }
+    __device__ __forceinline__ double value() const { return (double)v; }
+};
+template <>
+struct FxSum<double> {
+    unsigned long long lo = 0;
+    long long hi = 0;
+    __device__ __forceinline__ void add(const long long *blk, long long nv, long long i) {
+        const unsigned long long l = (unsigned long long)blk[i];
+        const int h = reinterpret_cast<const int *>(blk + nv)[i];
+        const unsigned long long o = lo;
+        lo = o + l;
+        hi += (long long)h + (lo < o ? 1 : 0);
+    }
+    // exact below 2^63 in magnitude; above, (double)lo rounds by at most 2^10
+    // against a value of at least 2^63, then the sum rounds once
+    __device__ __forceinline__ double value() const {
+        if ((hi == 0 && (long long)lo >= 0) || (hi == -1 && (long long)lo < 0)) return (double)(long long)lo;
+        return (double)hi * 0x1p64 + (double)lo;
+    }
+};
 
 // Per-axis weights of a cell whose stencil nodes are all interior (shape
 // type 3): the polynomial piece of each stencil offset is fixed (linear,
@@ -1067,9 +1146,7 @@ __device__ __forceinline__ void p2g_tile(const SplineTables *tab, unsigned *acc_
         }
     }
     __syncthreads();
-    long long *dst = staging + (long long)w * NCH * B3;
-    for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x)
-        dst[i] = fx_value<R>(acc_lo[i], acc_hi[i]);
+    fx_store<R>(acc_lo, acc_hi, NCH * B3, staging + (long long)w * stg_stride<R>((long long)NCH * B3));
     __syncthreads();
 }
 
@@ -1083,7 +1160,7 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
     const int B3 = P.B * P.B * P.B;
     unsigned *acc_lo = reinterpret_cast<unsigned *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
-    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3);
+    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3 * fx_lo_words<R>());
     load_tables(tab);
     R sc[NCH];
 #pragma unroll
@@ -1097,10 +1174,7 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
         // tiles are taken in turn from a device counter: blocks that drew
         // light tiles take more of them
         if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_p2g, 1);
-        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) {
-            acc_lo[i] = 0u;
-            acc_hi[i] = 0;
-        }
+        fx_zero<R>(acc_lo, acc_hi, NCH * B3);
         __syncthreads();
         const int w = s_item;
         if (w >= nitems) break;
@@ -1328,6 +1402,122 @@ __device__ __forceinline__ void fact_axis_weights(const SplineTables &tab, const
         p2g_axis_weights<R, ORD>(tab, P, d, x, i, false, a);
 }
 
+// The particles ka..kb-1 of one cell (bin) into a task's accumulators: for
+// each particle the z weight of the task's slice first (a zero slice weight
+// and derivative skip it), then the x and y weights, the particle's
+// z-factored terms, and per y row of the task a packed FMA per node and
+// channel pair.  Returns whether any particle contributed.
+template <class R, int ORD, int ROWS, int MAP>
+__device__ __forceinline__ bool fact_deposit_cell(const SplineTables *tab, const Params &P, const Parts<R> &A,
+                                                  const int32_t *perm, int s0, int ka, int kb, const int iv[3],
+                                                  const bool inter[3], const double xo[3], int sz, int rg,
+                                                  const R *grav, FactAcc<R> (&acc)[ROWS][P2GStc<ORD>::W]) {
+    constexpr int W = P2GStc<ORD>::W;
+    constexpr int NPASS = W / ROWS;
+    bool any = false;
+    for (int k = ka; k < kb; ++k) {
+        const int p = perm[s0 + k];
+        if (A.phase[p] != 0) continue;
+        const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+        double xw[3];
+        R f[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            xw[d] = dual_x(P, d, x[d]);
+            f[d] = (R)((xw[d] - xo[d]) * P.dxi[d]);
+        }
+        R wz, dwz;
+        if (MAP == 0) {
+            slot_weight<R, ORD>(*tab, P, 2, xw[2], iv[2], inter[2], f[2], sz, wz, dwz);
+        } else {
+            AxisW<R, W> az;
+            fact_axis_weights<R, ORD>(*tab, P, 2, xw[2], iv[2], inter[2], f[2], az);
+            wz = pick<W>(az.w, sz);
+            dwz = pick<W>(az.dw, sz);
+        }
+        if (wz == R(0) && dwz == R(0)) continue;
+        any = true;
+        AxisW<R, W> ax, ay;
+        fact_axis_weights<R, ORD>(*tab, P, 0, xw[0], iv[0], inter[0], f[0], ax);
+        fact_axis_weights<R, ORD>(*tab, P, 1, xw[1], iv[1], inter[1], f[1], ay);
+        const R m = A.mass[p], vol = A.vol[p];
+        const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] && x[1] > P.slab_lo[1] &&
+                          x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] && x[2] < P.slab_hi[2];
+        R sg[6];
+#pragma unroll
+        for (int c6 = 0; c6 < 6; ++c6) sg[c6] = -vol * A.sig[c6][p];
+        // rows of the symmetric stress in packed XX XY XZ YY YZ ZZ order
+        const R s0r[3] = {sg[0], sg[1], sg[2]}, s1r[3] = {sg[1], sg[3], sg[4]}, s2r[3] = {sg[2], sg[4], sg[5]};
+        FactZ<R> z;
+        z.m = m * wz;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const R bd = fma(m, grav[d], slab ? (R)P.extforce[d] : R(0));
+            const R sd0 = d == 0 ? s0r[0] : (d == 1 ? s1r[0] : s2r[0]);
+            const R sd1 = d == 0 ? s0r[1] : (d == 1 ? s1r[1] : s2r[1]);
+            const R sd2 = d == 0 ? s0r[2] : (d == 1 ? s1r[2] : s2r[2]);
+            z.p[d] = (m * A.v[d][p]) * wz;
+            z.a[d] = fma(sd2, dwz, bd * wz);
+            z.b[d] = sd1 * wz;
+            z.c[d] = sd0 * wz;
+        }
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r) {
+            const int sy = rg * ROWS + r;
+            const R wy = NPASS == 1 ? ay.w[r] : pick<W>(ay.w, sy);
+            const R dwy = NPASS == 1 ? ay.dw[r] : pick<W>(ay.dw, sy);
+            const FactRow<R, 1> row = fact_row<R>(z, wy, dwy);
+#pragma unroll
+            for (int sx = 0; sx < W; ++sx) {
+                if constexpr (sizeof(R) == 4)
+                    acc[r][sx].add(row, make_float2(ax.w[sx], ax.w[sx]), make_float2(ax.dw[sx], ax.dw[sx]));
+                else
+                    acc[r][sx].add(row, ax.w[sx], ax.dw[sx]);
+            }
+        }
+    }
+    return any;
+}
+
+// L2 prefetch of the first particle of cell c, if it has one.
+template <class R>
+__device__ __forceinline__ void prefetch_cell_head(const Parts<R> &A, const int32_t *perm, int s0, const int *cs,
+                                                   int c) {
+    const int kn = cs[c];
+    if (kn < cs[c + 1]) {
+        const int pn = perm[s0 + kn];
+        auto pf = [](const void *q) { asm volatile("prefetch.global.L2 [%0];" ::"l"(q)); };
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            pf(A.x[d] + pn);
+            pf(A.v[d] + pn);
+        }
+#pragma unroll
+        for (int c6 = 0; c6 < 6; ++c6) pf(A.sig[c6] + pn);
+        pf(A.mass + pn);
+        pf(A.vol + pn);
+        pf(A.phase + pn);
+    }
+}
+
+template <class R, int ORD>
+__device__ __forceinline__ void cell_frame(const Params &P, const int tc[3], int lx, int ly, int lz, int iv[3],
+                                           bool inter[3], double xo[3]) {
+    const int T = P.T;
+    iv[0] = tc[0] * T + lx;
+    iv[1] = tc[1] * T + ly;
+    iv[2] = tc[2] * T + lz;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        inter[d] = P.periodic[d] ||
+                   (ORD == 2 ? (iv[d] >= 3 && iv[d] <= P.nc[d] - 3) : (iv[d] >= 3 && iv[d] <= P.nc[d] - 4));
+        xo[d] = P.plo[d] + iv[d] * P.dx[d];  // the cell's (cubic) or bin node's (quadratic) coordinate
+    }
+}
+
+// One tile of the factorized P2G, one task per (cell, z-slice, row group):
+// the task's ROWS x W node block accumulates the cell's particles in
+// registers and is added to the tile's fixed-point block after the cell.
 template <class R, int ORD, int ROWS, int MAP>
 __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned *acc_lo, int *acc_hi, const Params &P,
                                               const Parts<R> &A, const int *active, const int *start,
@@ -1369,104 +1559,21 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
             const int un = u + step;
             int cnext = 0, sn = 1;
             if (un < ntask) task(un, cnext, sn);
-            if (un < ntask && sn == 0) {
-                const int kn = cs[cnext];
-                if (kn < cs[cnext + 1]) {
-                    const int pn = perm[s0 + kn];
-                    auto pf = [](const void *q) { asm volatile("prefetch.global.L2 [%0];" ::"l"(q)); };
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        pf(A.x[d] + pn);
-                        pf(A.v[d] + pn);
-                    }
-#pragma unroll
-                    for (int c6 = 0; c6 < 6; ++c6) pf(A.sig[c6] + pn);
-                    pf(A.mass + pn);
-                    pf(A.vol + pn);
-                    pf(A.phase + pn);
-                }
-            }
+            if (un < ntask && sn == 0) prefetch_cell_head(A, perm, s0, cs, cnext);
         }
         if (ka == kb) continue;
         const int lx = c % T, ly = (c / T) % T, lz = c / (T * T);
-        const int iv[3] = {tc[0] * T + lx, tc[1] * T + ly, tc[2] * T + lz};
+        int iv[3];
         bool inter[3];
-        double xo[3];  // the cell's (cubic) or bin node's (quadratic) coordinate
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            inter[d] = P.periodic[d] ||
-                       (ORD == 2 ? (iv[d] >= 3 && iv[d] <= P.nc[d] - 3) : (iv[d] >= 3 && iv[d] <= P.nc[d] - 4));
-            xo[d] = P.plo[d] + iv[d] * P.dx[d];
-        }
+        double xo[3];
+        cell_frame<R, ORD>(P, tc, lx, ly, lz, iv, inter, xo);
         FactAcc<R> acc[ROWS][W];
 #pragma unroll
         for (int r = 0; r < ROWS; ++r)
 #pragma unroll
             for (int sx = 0; sx < W; ++sx) acc[r][sx].zero();
-        bool any = false;
-        for (int k = ka; k < kb; ++k) {
-            const int p = perm[s0 + k];
-            if (A.phase[p] != 0) continue;
-            const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
-            double xw[3];
-            R f[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                xw[d] = dual_x(P, d, x[d]);
-                f[d] = (R)((xw[d] - xo[d]) * P.dxi[d]);
-            }
-            R wz, dwz;
-            if (MAP == 0) {
-                slot_weight<R, ORD>(*tab, P, 2, xw[2], iv[2], inter[2], f[2], sz, wz, dwz);
-            } else {
-                AxisW<R, W> az;
-                fact_axis_weights<R, ORD>(*tab, P, 2, xw[2], iv[2], inter[2], f[2], az);
-                wz = pick<W>(az.w, sz);
-                dwz = pick<W>(az.dw, sz);
-            }
-            if (wz == R(0) && dwz == R(0)) continue;
-            any = true;
-            AxisW<R, W> ax, ay;
-            fact_axis_weights<R, ORD>(*tab, P, 0, xw[0], iv[0], inter[0], f[0], ax);
-            fact_axis_weights<R, ORD>(*tab, P, 1, xw[1], iv[1], inter[1], f[1], ay);
-            const R m = A.mass[p], vol = A.vol[p];
-            const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
-                              x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] &&
-                              x[2] < P.slab_hi[2];
-            R sg[6];
-#pragma unroll
-            for (int c6 = 0; c6 < 6; ++c6) sg[c6] = -vol * A.sig[c6][p];
-            // rows of the symmetric stress in packed XX XY XZ YY YZ ZZ order
-            const R s0r[3] = {sg[0], sg[1], sg[2]}, s1r[3] = {sg[1], sg[3], sg[4]}, s2r[3] = {sg[2], sg[4], sg[5]};
-            FactZ<R> z;
-            z.m = m * wz;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const R bd = fma(m, grav[d], slab ? (R)P.extforce[d] : R(0));
-                const R sd0 = d == 0 ? s0r[0] : (d == 1 ? s1r[0] : s2r[0]);
-                const R sd1 = d == 0 ? s0r[1] : (d == 1 ? s1r[1] : s2r[1]);
-                const R sd2 = d == 0 ? s0r[2] : (d == 1 ? s1r[2] : s2r[2]);
-                z.p[d] = (m * A.v[d][p]) * wz;
-                z.a[d] = fma(sd2, dwz, bd * wz);
-                z.b[d] = sd1 * wz;
-                z.c[d] = sd0 * wz;
-            }
-#pragma unroll
-            for (int r = 0; r < ROWS; ++r) {
-                const int sy = rg * ROWS + r;
-                const R wy = NPASS == 1 ? ay.w[r] : pick<W>(ay.w, sy);
-                const R dwy = NPASS == 1 ? ay.dw[r] : pick<W>(ay.dw, sy);
-                const FactRow<R, 1> row = fact_row<R>(z, wy, dwy);
-#pragma unroll
-                for (int sx = 0; sx < W; ++sx) {
-                    if constexpr (sizeof(R) == 4)
-                        acc[r][sx].add(row, make_float2(ax.w[sx], ax.w[sx]), make_float2(ax.dw[sx], ax.dw[sx]));
-                    else
-                        acc[r][sx].add(row, ax.w[sx], ax.dw[sx]);
-                }
-            }
-        }
-        if (!any) continue;
+        if (!fact_deposit_cell<R, ORD, ROWS, MAP>(tab, P, A, perm, s0, ka, kb, iv, inter, xo, sz, rg, grav, acc))
+            continue;
 #pragma unroll
         for (int r = 0; r < ROWS; ++r)
 #pragma unroll
@@ -1477,9 +1584,132 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
             }
     }
     __syncthreads();
-    long long *dst = staging + (long long)w * NCH * B3;
-    for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) dst[i] = fx_value<R>(acc_lo[i], acc_hi[i]);
+    fx_store<R>(acc_lo, acc_hi, NCH * B3, staging + (long long)w * stg_stride<R>((long long)NCH * B3));
     __syncthreads();
+}
+
+// Segments a row of a tile is cut into for p2g_tile_xrun (1: whole rows;
+// half rows measured no faster: the block's closing barrier waits for the
+// slowest segment either way).
+constexpr int kXRunParts = 1;
+
+// One tile of the factorized P2G, one task per (segment of T / kXRunParts
+// cells along x, z-slice, row group): the task walks its segment's cells in
+// x order with a window of W node columns in registers.  Once cell cx is
+// done, no later cell of the segment reaches node column cx, so that column
+// alone goes to the tile's fixed-point block and the window moves by one
+// column; the last W - 1 columns go after the segment.  Per cell one column
+// of ROWS x 7 values is converted and added instead of W columns.
+template <class R, int ORD, int ROWS, int MAP>
+__device__ __forceinline__ void p2g_tile_xrun(const SplineTables *tab, unsigned *acc_lo, int *acc_hi, const Params &P,
+                                              const Parts<R> &A, const int *active, const int *start,
+                                              const int *cell_start, const int32_t *perm, long long *staging,
+                                              const R *sc, const R *grav, int w) {
+    constexpr int W = P2GStc<ORD>::W;
+    static_assert(W % ROWS == 0, "rows per pass must divide the stencil width");
+    constexpr int NPASS = W / ROWS, LANES = W * NPASS, NCH = CH_MOM_END;
+    const int B = P.B, B3 = B * B * B, T = P.T, T2 = T * T, T3 = T2 * T;
+    const int SL = T / kXRunParts, NSEG = T2 * kXRunParts;  // cells per segment, segments per tile
+    const int t = active[w];
+    int tc[3];
+    tile_coords(P, t, tc);
+    const int s0 = start[t];
+    const int *cs = cell_start + (long long)w * (T3 + 1);
+    // task u -> (segment, z-slice, row group); MAP 0: a warp takes one
+    // (z-slice, row group) of 32 segments (warp-uniform slice), MAP 1: a
+    // segment's LANES tasks in adjacent lanes
+    const int groups = (NSEG + 31) >> 5;
+    const int ntask = MAP == 0 ? groups * 32 * LANES : NSEG * LANES, step = (int)blockDim.x;
+    for (int u = threadIdx.x; u < ntask; u += step) {
+        int seg, sub;
+        if (MAP == 0) {
+            const int wi = u >> 5, g = wi / LANES;
+            sub = wi - g * LANES;
+            seg = g * 32 + (u & 31);
+        } else {
+            seg = u / LANES;
+            sub = u - seg * LANES;
+        }
+        if (seg >= NSEG) continue;
+        const int sz = sub / NPASS, rg = sub - sz * NPASS;
+        const int row = seg / kXRunParts, x0 = (seg - row * kXRunParts) * SL;
+        const int ly = row % T, lz = row / T;
+        const int c0 = row * T + x0;  // first cell of the segment (x fastest)
+        FactAcc<R> acc[ROWS][W];
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+            for (int sx = 0; sx < W; ++sx) acc[r][sx].zero();
+        unsigned dirty = 0;  // bit j: window column j holds contributions
+        const int ybase = (lz + sz) * B + ly + rg * ROWS;
+        auto flush = [&](int j, int col) {
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r) {
+                const int idx = (ybase + r) * B + col;
+#pragma unroll
+                for (int ch = 0; ch < NCH; ++ch) {
+                    R v;
+                    switch (j) {  // j is a compile-time constant at every call
+                        case 0: v = acc[r][0].get(ch); break;
+                        case 1: v = acc[r][1 % W].get(ch); break;
+                        case 2: v = acc[r][2 % W].get(ch); break;
+                        default: v = acc[r][W - 1].get(ch); break;
+                    }
+                    fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, v, sc[ch]);
+                }
+            }
+        };
+        for (int k = 0; k < SL; ++k) {
+            const int cx = x0 + k, c = c0 + k;
+            const int ka = cs[c], kb = cs[c + 1];
+            if (EXG_P2G_PREFETCH && k + 1 < SL && sub == 0) prefetch_cell_head(A, perm, s0, cs, c + 1);
+            if (ka < kb) {
+                int iv[3];
+                bool inter[3];
+                double xo[3];
+                cell_frame<R, ORD>(P, tc, cx, ly, lz, iv, inter, xo);
+                if (fact_deposit_cell<R, ORD, ROWS, MAP>(tab, P, A, perm, s0, ka, kb, iv, inter, xo, sz, rg, grav,
+                                                         acc))
+                    dirty |= (1u << W) - 1u;
+            }
+            if (dirty & 1u) flush(0, cx);
+            // the window moves one column along x
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r) {
+#pragma unroll
+                for (int j = 0; j + 1 < W; ++j) acc[r][j] = acc[r][j + 1];
+                acc[r][W - 1].zero();
+            }
+            dirty >>= 1;
+        }
+#pragma unroll
+        for (int j = 0; j + 1 < W; ++j)
+            if (dirty & (1u << j)) flush(j, x0 + SL + j);
+    }
+    __syncthreads();
+    fx_store<R>(acc_lo, acc_hi, NCH * B3, staging + (long long)w * stg_stride<R>((long long)NCH * B3));
+    __syncthreads();
+}
+
+// FP64 cubic tasks walk rows of cells (p2g_tile_xrun): its fixed-point
+// adds are returning 64-bit atomics, and the walk converts and adds a third
+// as many values (FP64 P2G 3.46 -> 2.97 ms on the 9 M-particle spheres).
+// FP32 cubic and all quadratic tasks take one cell (bin) each
+// (p2g_tile_fact): the FP32 adds are cheap, and the per-cell walk keeps
+// more tasks per thread to even out uneven cells (1.66 against 1.69 ms).
+// Every launch variant of one precision and order uses the same walk, so
+// the register sums and hence the results are the same for all of them.
+template <class R, int ORD, int ROWS, int MAP>
+__device__ __forceinline__ void p2g_tile_factorized(const SplineTables *tab, unsigned *acc_lo, int *acc_hi,
+                                                    const Params &P, const Parts<R> &A, const int *active,
+                                                    const int *start, const int *cell_start, const int32_t *perm,
+                                                    long long *staging, const R *sc, const R *grav, int w) {
+    if constexpr (ORD == 3 && sizeof(R) == 8)
+        p2g_tile_xrun<R, ORD, ROWS, MAP>(tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm, staging, sc,
+                                         grav, w);
+    else
+        p2g_tile_fact<R, ORD, ROWS, MAP>(tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm, staging, sc,
+                                         grav, w);
 }
 
 template <class R, int ORD, int V>
@@ -1492,7 +1722,7 @@ __global__ void __launch_bounds__(P2GVar<R, ORD, V>::THREADS, P2GVar<R, ORD, V>:
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
     const int B3 = P.B * P.B * P.B;
     unsigned *acc_lo = reinterpret_cast<unsigned *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
-    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3);
+    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3 * fx_lo_words<R>());
     load_tables(tab);
     R sc[NCH];
 #pragma unroll
@@ -1504,14 +1734,11 @@ __global__ void __launch_bounds__(P2GVar<R, ORD, V>::THREADS, P2GVar<R, ORD, V>:
     for (;;) {
         // tiles are taken in turn from a device counter
         if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_p2g, 1);
-        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) {
-            acc_lo[i] = 0u;
-            acc_hi[i] = 0;
-        }
+        fx_zero<R>(acc_lo, acc_hi, NCH * B3);
         __syncthreads();
         const int w = s_item;
         if (w >= nitems) break;
-        p2g_tile_fact<R, ORD, P2GVar<R, ORD, V>::ROWS, P2GVar<R, ORD, V>::MAP>(tab, acc_lo, acc_hi, P, A, active,
+        p2g_tile_factorized<R, ORD, P2GVar<R, ORD, V>::ROWS, P2GVar<R, ORD, V>::MAP>(tab, acc_lo, acc_hi, P, A, active,
                                                                                 start, cell_start, perm, staging,
                                                                                 sc, grav, w);
     }
@@ -1679,9 +1906,9 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
             ok = ok && nid[d] < nown;
         }
         if (!ok) continue;
-        long long accv[NCH];
+        FxSum<R> accv[NCH];
 #pragma unroll
-        for (int c = 0; c < NCH; ++c) accv[c] = 0;
+        for (int c = 0; c < NCH; ++c) accv[c] = FxSum<R>();
         // Source tiles per axis: the node's own tile, plus the lower
         // neighbour when the node lies in its high halo (l < hhi) or the
         // upper neighbour when it lies in its low halo (l >= T - hlo); both
@@ -1722,16 +1949,18 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
                     const int lz = a ? l2[2] : l1[2], ly = b2 ? l2[1] : l1[1], lx = c2 ? l2[0] : l1[0];
                     const int sl = slot[(sz * P.ntile[1] + sy) * P.ntile[0] + sx];
                     if (sl < 0) continue;
-                    const long long base = (long long)sl * NCH * B3 + ((long long)lz * B + ly) * B + lx;
+                    const long long nv = (long long)NCH * B3;
+                    const long long *blk = staging + (long long)sl * stg_stride<R>(nv);
+                    const long long off = ((long long)lz * B + ly) * B + lx;
 #pragma unroll
-                    for (int c = 0; c < NCH; ++c) accv[c] += staging[base + (long long)c * B3];
+                    for (int c = 0; c < NCH; ++c) accv[c].add(blk, nv, off + (long long)c * B3);
                 }
         const long long ni = ((long long)nid[2] * P.nn[1] + nid[1]) * P.nn[0] + nid[0];
-        double m = (double)accv[CH_M] * isc[CH_M];
+        double m = accv[CH_M].value() * isc[CH_M];
         double p[3], f[3];
         for (int d = 0; d < 3; ++d) {
-            p[d] = (double)accv[CH_P + d] * isc[CH_P + d];
-            f[d] = (double)accv[CH_F + d] * isc[CH_F + d];
+            p[d] = accv[CH_P + d].value() * isc[CH_P + d];
+            f[d] = accv[CH_F + d].value() * isc[CH_F + d];
         }
         if (mode == NM_MERGE) {
             // P2G_Momentum: zero + deposit + normalise (mpm_particle_grid_ops.cpp:368-627)
@@ -1752,13 +1981,13 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
                 // zeroed, m k only when temperatures are deposited, and T is
                 // normalised where m cp > 0 (mpm_particle_grid_ops.cpp:680-884)
                 const bool fT = flags & PF_TEMP;
-                const double mc = fT ? (double)accv[CH_MC] * isc[CH_MC] : 0.0;
-                const double mct = fT ? (double)accv[CH_MCT] * isc[CH_MCT] : 0.0;
+                const double mc = fT ? accv[CH_MC].value() * isc[CH_MC] : 0.0;
+                const double mct = fT ? accv[CH_MCT].value() * isc[CH_MCT] : 0.0;
                 Nd.c[EXG_N_MASS_SPHEAT][ni] = (R)mc;
                 Nd.c[EXG_N_MASS_SPHEAT_TEMP][ni] = (R)mct;
-                Nd.c[EXG_N_SOURCE_TEMP][ni] = (R)((flags & PF_SRC) ? (double)accv[CH_SRC] * isc[CH_SRC] : 0.0);
+                Nd.c[EXG_N_SOURCE_TEMP][ni] = (R)((flags & PF_SRC) ? accv[CH_SRC].value() * isc[CH_SRC] : 0.0);
                 if (fT) {
-                    Nd.c[EXG_N_MASS_COND][ni] = (R)((double)accv[CH_MK] * isc[CH_MK]);
+                    Nd.c[EXG_N_MASS_COND][ni] = (R)(accv[CH_MK].value() * isc[CH_MK]);
                     if (mc > 0.0) Nd.c[EXG_N_TEMPERATURE][ni] = (R)((mc >= P.mass_tol) ? mct / mc : -P.Tref);
                 }
             }
@@ -1791,8 +2020,8 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
                 // P2G_Temperature(1,1,1), backup_current_temperature and
                 // Nodal_Time_Update_Temperature (main.cpp:100-102) on a node
                 // that Reset_Nodaldata_to_Zero left at 0
-                const double mc = (double)accv[CH_MC] * isc[CH_MC], mct = (double)accv[CH_MCT] * isc[CH_MCT];
-                const double src = (double)accv[CH_SRC] * isc[CH_SRC];
+                const double mc = accv[CH_MC].value() * isc[CH_MC], mct = accv[CH_MCT].value() * isc[CH_MCT];
+                const double src = accv[CH_SRC].value() * isc[CH_SRC];
                 // temperatures relative to Tref (0 K is -Tref); DELTA holds 0
                 // where m cp = 0, as the reset leaves it
                 double Tn = -P.Tref;
@@ -1804,7 +2033,7 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
                     Tn = -P.Tref;
                 Nd.c[EXG_N_MASS_SPHEAT][ni] = (R)mc;
                 Nd.c[EXG_N_MASS_SPHEAT_TEMP][ni] = (R)mct;
-                Nd.c[EXG_N_MASS_COND][ni] = (R)((double)accv[CH_MK] * isc[CH_MK]);
+                Nd.c[EXG_N_MASS_COND][ni] = (R)(accv[CH_MK].value() * isc[CH_MK]);
                 Nd.c[EXG_N_SOURCE_TEMP][ni] = (R)src;
                 Nd.c[EXG_N_TEMPERATURE][ni] = (R)Tn;
                 Nd.c[EXG_N_DELTA_TEMPERATURE][ni] = (R)Told;
@@ -1829,7 +2058,7 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
                 // zeroes m cp and m cp T, only the source is deposited
                 Nd.c[EXG_N_MASS_SPHEAT][ni] = R(0);
                 Nd.c[EXG_N_MASS_SPHEAT_TEMP][ni] = R(0);
-                Nd.c[EXG_N_SOURCE_TEMP][ni] = (R)((double)accv[CH_SRC] * isc[CH_SRC]);
+                Nd.c[EXG_N_SOURCE_TEMP][ni] = (R)(accv[CH_SRC].value() * isc[CH_SRC]);
             }
         }
     }
@@ -2494,7 +2723,7 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
                                          const Material *mats, const int *active, const int *start, const int *count,
                                          const int32_t *perm, int mode, int w, double dt, double asr, bool upd_vel,
                                          float (&run_b)[CH_ALL], double &run_speed, bool &red, unsigned &status,
-                                         bool staged = false) {
+                                         bool staged = false, int kbeg = 0, int kend = 1 << 30) {
     const int B = P.B, B3 = B * B * B;
     const int t = active[w];
     int tc[3];
@@ -2521,7 +2750,9 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
     // a velocity update overwrites v' of every phase-0 particle: the stored
     // v' is read only for rigid particles and for G2P without it
     const bool vel_only = mode == GM_VEL, fresh_vp = vel_only || upd_vel;
-    for (int k = s0 + threadIdx.x; k < s0 + n; k += blockDim.x) {
+    // the particles kbeg .. kend - 1 of the tile (one work item)
+    const int k_end = s0 + min(n, kend);
+    for (int k = s0 + kbeg + threadIdx.x; k < k_end; k += blockDim.x) {
         if (EXG_G2P_PREFETCH && k + EXG_G2P_PREFETCH * (int)blockDim.x < s0 + n)
             prefetch_particle<R>(A, k + EXG_G2P_PREFETCH * blockDim.x, !fresh_vp);
         const int p = perm[k];
@@ -2662,11 +2893,13 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
 constexpr int kG2PVariants = 3;
 static_assert(kG2PVariants == EXG_NUM_VARIANTS, "the launchers dispatch EXG_NUM_VARIANTS G2P variants");
 // threads per block, minimum blocks per SM:
-//   FP32: (256, 2)  (128, 4)  (384, 1);   FP64: (256, 2)  (256, 1)  (384, 1)
+//   FP32: (256, 2)  (192, 2)  (384, 1);   FP64: (256, 2)  (256, 1)  (384, 1)
+// (192, 2) keeps 12 warps per SM, as (384, 1), with 170 registers a thread
+// and two blocks whose barriers and node-block waits overlap.
 template <class R, int V>
 struct G2PVar {
-    static constexpr int THREADS = (V == 0) ? EXG_G2P_THREADS : (V == 1 ? (sizeof(R) == 4 ? 128 : 256) : 384);
-    static constexpr int MINB = (V == 0) ? EXG_G2P_MINB : (V == 1 ? (sizeof(R) == 4 ? 4 : 1) : 1);
+    static constexpr int THREADS = (V == 0) ? EXG_G2P_THREADS : (V == 1 ? (sizeof(R) == 4 ? 192 : 256) : 384);
+    static constexpr int MINB = (V == 0) ? EXG_G2P_MINB : (V == 1 ? (sizeof(R) == 4 ? 2 : 1) : 1);
 };
 
 // ---- TMA staging of the G2P node block (cp.async.bulk.tensor + mbarrier)
@@ -2709,10 +2942,26 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
     return false;
 }
 
+// The active tile of fused-G2P work item `item`: the last w with
+// item_start[w] <= item (every active tile has at least one item, so the
+// starts increase strictly).
+__device__ __forceinline__ int item_tile(const int *item_start, int nact, int item) {
+    int lo = 0, hi = nact - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (item_start[mid] <= item)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
 template <class R, int ORD, bool LEAN, int V = 0>
 __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g2p_fused(Params P, Parts<R> A, Parts<R> Bo, Nodes<R> Nd, NodeBCArgs bc,
                                                         const Material *mats, const int *active, const int *start,
-                                                        const int *count, const int32_t *perm, Ctl *ctl, int mode,
+                                                        const int *count, const int32_t *perm,
+                                                        const int *item_start, Ctl *ctl, int mode,
                                                         const __grid_constant__ CUtensorMap tmap, int use_tma) {
     extern __shared__ __align__(128) unsigned char smraw[];
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
@@ -2740,17 +2989,22 @@ __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g
     for (int c = 0; c < CH_ALL; ++c) run_b[c] = 0.0f;
     double run_speed = 0.0;  // largest CFL wave speed of the thread's particles
     bool red = false;
-    const int nitems = ctl->n_active_tiles;
+    // work items (chunks of kG2PChunk particles of a tile) are taken in turn
+    // from a device counter (reset by k_nodes)
+    const int nitems = ctl->n_g2p_items, nact = ctl->n_active_tiles;
     if (!use_tma) {
-        __shared__ int s_item;
+        __shared__ int s_item, s_w;
         for (;;) {
-            // tiles are taken in turn from a device counter (reset by k_nodes)
-            if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_g2p, 1);
+            if (threadIdx.x == 0) {
+                s_item = atomicAdd(&ctl->next_g2p, 1);
+                if (s_item < nitems) s_w = item_tile(item_start, nact, s_item);
+            }
             __syncthreads();
-            const int w = s_item;
-            if (w >= nitems) break;
+            const int it = s_item;
+            if (it >= nitems) break;
+            const int w = s_w, kb = (it - item_start[w]) * kG2PChunk;
             g2p_tile<R, ORD, LEAN>(tab, nb, P, A, Bo, Nd, bc, mats, active, start, count, perm, mode, w, dt, asr,
-                                   upd_vel, run_b, run_speed, red, status);
+                                   upd_vel, run_b, run_speed, red, status, false, kb, kb + kG2PChunk);
         }
     } else {
         // The node block of each tile comes by one TMA box from the nodal
@@ -2762,10 +3016,12 @@ __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g
         const size_t buf_words = (((size_t)B * B * B * SmemNodes<R>::NS * sizeof(R) + 127) & ~size_t(127)) / sizeof(R);
         const unsigned box_bytes = (unsigned)((size_t)B * B * B * SmemNodes<R>::NS * sizeof(R));
         __shared__ __align__(8) unsigned long long mbar[2];
-        __shared__ int s_items[2];
+        __shared__ int s_items[2], s_ws[2];
         auto issue = [&](int item, int b) {
+            const int w = item_tile(item_start, nact, item);
+            s_ws[b] = w;
             int tc[3];
-            tile_coords(P, active[item], tc);
+            tile_coords(P, active[w], tc);
             mbar_expect_tx(&mbar[b], box_bytes);
             tma_load_4d(nb + b * buf_words, &tmap, 0, tc[0] * P.T - P.hlo, tc[1] * P.T - P.hlo, tc[2] * P.T - P.hlo,
                         &mbar[b]);
@@ -2782,8 +3038,9 @@ __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g
         unsigned ph[2] = {0u, 0u};
         int cur = 0;
         for (;;) {
-            const int w = s_items[cur];
-            if (w >= nitems) break;
+            const int it = s_items[cur];
+            if (it >= nitems) break;
+            const int w = s_ws[cur], kb = (it - item_start[w]) * kG2PChunk;
             if (NBUF == 2 && threadIdx.x == 0) {
                 // the other buffer's last tile is done (the block synchronised)
                 const int i = atomicAdd(&ctl->next_g2p, 1);
@@ -2800,7 +3057,8 @@ __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g
                 break;
             }
             g2p_tile<R, ORD, LEAN>(tab, nb + cur * buf_words, P, A, Bo, Nd, bc, mats, active, start, count, perm,
-                                   mode, w, dt, asr, upd_vel, run_b, run_speed, red, status, true);
+                                   mode, w, dt, asr, upd_vel, run_b, run_speed, red, status, true, kb,
+                                   kb + kG2PChunk);
             if (NBUF == 2) {
                 cur ^= 1;
             } else {
@@ -3523,7 +3781,7 @@ __global__ void __launch_bounds__(kBatchThreads) k_bb_keys(const SortDesc *__res
 
 __global__ void k_bb_tile_scan(const SortDesc *__restrict__ d) {
     const SortDesc &x = d[blockIdx.x];
-    tile_scan_block((int)x.P.ntiles, x.tile_count, x.tile_start, x.active, x.slot, x.ctl);
+    tile_scan_block((int)x.P.ntiles, x.tile_count, x.tile_start, x.active, x.slot, x.item_start, x.ctl);
 }
 
 __global__ void __launch_bounds__(kBatchThreads) k_bb_scatter(const SortDesc *__restrict__ d,
@@ -3604,7 +3862,7 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
     extern __shared__ __align__(16) unsigned char smraw[];
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
     unsigned *acc_lo = reinterpret_cast<unsigned *>(smraw + ((sizeof(SplineTables) + 15) & ~15));
-    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3);
+    int *acc_hi = reinterpret_cast<int *>(acc_lo + NCH * B3 * fx_lo_words<R>());
     load_tables(tab);
     const int ns = b->nscenes, total = b->pre_active[ns];
     int cur = -1;
@@ -3615,10 +3873,7 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
             s_item = i;
             s_scene = i < total ? scene_of(b->pre_active, ns, i) : -1;
         }
-        for (int i = threadIdx.x; i < NCH * B3; i += blockDim.x) {
-            acc_lo[i] = 0u;
-            acc_hi[i] = 0;
-        }
+        fx_zero<R>(acc_lo, acc_hi, NCH * B3);
         __syncthreads();
         const int i = s_item, s = s_scene;
         if (i >= total) break;
@@ -3631,7 +3886,7 @@ __global__ void __launch_bounds__(P2GCfg<R, ORD, THERM>::THREADS, P2GCfg<R, ORD,
             for (int d = 0; d < 3; ++d) grav[d] = (R)sd.P.gravity[d];
         }
         if constexpr (P2GCfg<R, ORD, THERM>::FACT)
-            p2g_tile_fact<R, ORD, P2GCfg<R, ORD, THERM>::ROWS, P2GCfg<R, ORD, THERM>::MAP>(
+            p2g_tile_factorized<R, ORD, P2GCfg<R, ORD, THERM>::ROWS, P2GCfg<R, ORD, THERM>::MAP>(
                 tab, acc_lo, acc_hi, sd.P, sd.A, sd.active, sd.start, sd.cell_start, sd.perm, sd.staging, sc, grav,
                 i - b->pre_active[s]);
         else
@@ -3797,7 +4052,7 @@ void launch_keys(Ctx &c) {
 
 void launch_sort_rest(Ctx &c, bool touched_list) {
     k_tile_scan<<<1, 1024, 0, c.stream>>>((int)c.P.ntiles, c.sb.tile_count, c.sb.tile_start, c.sb.active, c.sb.slot,
-                                          c.ctl);
+                                          c.sb.item_start, c.ctl);
     if (c.np > 0)
         k_scatter<<<nblocks(c.np), kThreads, 0, c.stream>>>(c.np, c.sb.key, 3 * c.P.tshift, c.sb.tile_start,
                                                             c.sb.tile_fill, c.sb.bucket);
@@ -3856,7 +4111,7 @@ template <class R, int ORD, bool TH>
 static void p2g_cell_t(Ctx &c, int flags) {
     const int NCH = TH ? CH_ALL : CH_MOM_END;
     const int B3 = c.P.B * c.P.B * c.P.B;
-    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * NCH * B3;
+    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned) * (fx_lo_words<R>() + 1) * NCH * B3;
     auto kern = k_p2g_cell<R, ORD, TH>;
     constexpr int nthr = P2GCfg<R, ORD, TH>::THREADS;
     EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -3878,7 +4133,7 @@ static void p2g_cell_t(Ctx &c, int flags) {
 template <class R, int ORD, int V>
 static void p2g_fact_v(Ctx &c) {
     const int B3 = c.P.B * c.P.B * c.P.B;
-    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * CH_MOM_END * B3;
+    size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned) * (fx_lo_words<R>() + 1) * CH_MOM_END * B3;
     auto kern = k_p2g_fact<R, ORD, V>;
     constexpr int nthr = P2GVar<R, ORD, V>::THREADS;
     EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -3959,8 +4214,8 @@ static void g2p_lt(Ctx &c, int mode) {
         gsm = sm;
     }
     kern<<<grid, nthr, sm, c.stream>>>(c.P, c.A<R>(), c.Bp<R>(), c.N<R>(), make_bc(c), c.mat_dev, c.sb.active,
-                                       c.sb.tile_start, c.sb.tile_count, c.sb.perm, c.ctl, mode, c.tmap,
-                                       c.tma ? 1 : 0);
+                                       c.sb.tile_start, c.sb.tile_count, c.sb.perm, c.sb.item_start, c.ctl, mode,
+                                       c.tmap, c.tma ? 1 : 0);
     EXG_CUDA_OK(cudaGetLastError());
 }
 template <class R, int ORD>
@@ -4186,6 +4441,7 @@ static bool batch_descriptors_t(Batch &b) {
             x.tile_start = c.sb.tile_start;
             x.active = c.sb.active;
             x.slot = c.sb.slot;
+            x.item_start = c.sb.item_start;
             x.touched = c.sb.touched;
             x.cell_start = c.sb.cell_start;
             x.touched_step = c.sb.touched_step;
@@ -4244,7 +4500,7 @@ static void batch_p2g_t(Batch &b) {
     const SceneDesc<R> *d = reinterpret_cast<const SceneDesc<R> *>(b.desc[b.parity]);
     const int B3 = c0.P.B * c0.P.B * c0.P.B;
     constexpr int NCH = CH_MOM_END;
-    const size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned long long) * NCH * B3;
+    const size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned) * (fx_lo_words<R>() + 1) * NCH * B3;
     auto kern = k_p2g_batch<R, ORD, false>;
     constexpr int nthr = P2GCfg<R, ORD, false>::THREADS;
     EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));

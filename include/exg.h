@@ -163,7 +163,7 @@ typedef struct exg_specs {
     /* B200 execution keys (exg.* namespace, no counterpart in the reference) */
     int precision; /* EXG_PREC_FP64 or EXG_PREC_MIXED */
     int tile;      /* tile edge in cells: 0 = the default (8), else 4 or 8 */
-    int autotune;  /* 1 (default): the first exg_step times the launch variants (exg_autotune) */
+    int autotune;  /* 1 (default): exg_step times the launch variants (exg_autotune) after its first step */
 } exg_specs;
 
 typedef struct exg_diag {
@@ -371,7 +371,10 @@ int exg_get_stream(exg_ctx *ctx, void **stream);
  * launches each, on the context's stream, outside any graph) and keeps the
  * fastest; choices are cached per (device, precision, order, tile, G2P
  * kind, particle-count decade) so later contexts of the same kind reuse them
- * without timing.  With specs.autotune = 1 the first exg_step calls it.
+ * without timing.  With specs.autotune = 1, exg_step calls it once the
+ * particles are in the order a fused step leaves them (tile-major, as every
+ * later step sees them): after the first step following an upload, which
+ * runs with the current variants (a cached choice is applied at once).
  * It leaves the particle state and the step's control block as it found
  * them; nodal data is recomputed by the next step. */
 #define EXG_NUM_VARIANTS 3

@@ -14,7 +14,12 @@ Probes, each against the oracle run on all host threads:
               contributions, as the reference's GPU atomics do);
   noise       after every step, every position, velocity and stress
               component one ulp up or down (a two-ulp spread, as two
-              correct implementations round each step's results apart).
+              correct implementations round each step's results apart);
+              a fluid particle's pressure moves by K 2^-52 instead (the
+              Tait pressure K((1/J)^gamma - 1) is a difference of numbers
+              near 1, so two correct evaluations of the power differ by
+              an ulp of 1, which is K 2^-52 in p), equally on the three
+              diagonal stress components.
 The workloads and sizes are those of tests/test_gpu_accuracy.py.  CPU only;
 run from the repository root (it takes a few minutes):
 
@@ -67,6 +72,11 @@ def run_noisy(s, p, phi, threads, seed):
         q.pos[:] = ulp(q.pos)
         q.rdata[nt.R_VEL:nt.R_VEL + 3] = ulp(q.rdata[nt.R_VEL:nt.R_VEL + 3])
         q.rdata[nt.R_STRESS:nt.R_STRESS + 6] = ulp(q.rdata[nt.R_STRESS:nt.R_STRESS + 6])
+        fluid = q.idata[nt.I_MODEL] == 1
+        if fluid.any():
+            dp = np.where(rng.random(q.n) < 0.5, -1.0, 1.0) * q.rdata[nt.R_BULK] * 2.0 ** -52
+            for c in (0, 3, 5):
+                q.rdata[nt.R_STRESS + c] = np.where(fluid, q.rdata[nt.R_STRESS + c] - dp, q.rdata[nt.R_STRESS + c])
         o.upload(q)
     return o.download()
 

@@ -118,6 +118,32 @@ def test_p2g_momentum(order):
         assert e_v < TOL64 and e_p < TOL64, f"node velocity {c}: {e_v:.3e} {e_p:.3e}"
 
 
+@pytest.mark.parametrize("order", [2, 3])
+def test_p2g_light_node_velocities_fp64(order):
+    # nodes that only the edges of particles' supports reach carry tiny
+    # masses; their velocities p / m must keep relative precision (the FP64
+    # fixed point is 96 bits wide), because the G2P's velocity gradient
+    # weights them by dN, which vanishes more slowly than N
+    s, p = small_dam(order=order, seed=60 + order)
+    rng = np.random.default_rng(order)
+    p.rdata[nt.R_VEL:nt.R_VEL + 3] = rng.normal(0, 0.3, (3, p.n))
+    # a spray of single particles in the empty part of the box: nodes at
+    # the ends of their supports get masses many decades below the block's
+    spray = rng.choice(p.n, 400, replace=False)
+    for d, (lo, hi) in enumerate([(0.55, 0.95), (0.05, 0.45), (0.05, 0.45)]):
+        p.pos[d, spray] = rng.uniform(lo, hi, 400)
+    ctx, o = pair(s, p)
+    ctx.P2G_Momentum(1, 1, 1)
+    o.p2g_momentum(1, 1, 1)
+    m = o.nodes(nt.N_MASS)
+    light = (m > 1e-10 * m.max()) & (m < 1e-4 * m.max())
+    assert light.sum() >= 5  # nodes beyond the block's faces
+    for c in range(3):
+        vo, vg = o.nodes(nt.N_VEL + c), ctx.nodes(nt.N_VEL + c)
+        e = np.abs(vg - vo)[light].max() / np.abs(vo).max()
+        assert e < 1e-12, f"velocity {c} at light nodes: {e:.3e}"
+
+
 def test_p2g_mixed_orders():
     # ncells < 5 on one axis: quadratic falls back to linear there
     s, p = random_scene(31, n=(20, 4, 12), order=2)
