@@ -495,6 +495,10 @@ int status_from_ctl(Ctx &c) {
         c.err = "a node-block transfer of the fused G2P did not complete within its wait limit";
         return EXG_ERR_TIMEOUT;
     }
+    if (st & ST_BOUNDS) {
+        c.err = "internal: a work-item, particle or staging index failed its range check";
+        return EXG_ERR_CUDA;
+    }
     if (st & ST_ALIGN) {
         c.err = "internal: the fused G2P's node-block buffer was not 128-byte aligned for TMA";
         return EXG_ERR_CUDA;
@@ -932,6 +936,13 @@ int exg_particles_upload(exg_ctx *ctx, const exg_particle_soa *p) {
                     std::tie(m.E, m.nu, m.K, m.gamma, m.mu, m.model) = key;
                     m.ipow = (m.gamma >= 1.0 && m.gamma <= 16.0 && m.gamma == std::floor(m.gamma)) ? (int)m.gamma
                                                                                                        : 0;
+                    if (m.model == 1) {
+                        m.pmod = m.K;
+                    } else {
+                        const double lambda = m.E * m.nu / ((1 + m.nu) * (1 - 2.0 * m.nu));
+                        const double mu = m.E / (2.0 * (1 + m.nu));
+                        m.pmod = lambda + 2.0 * mu;
+                    }
                     it = idx.emplace(key, (int)c.mats.size()).first;
                     c.mats.push_back(m);
                 }

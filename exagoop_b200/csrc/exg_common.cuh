@@ -30,6 +30,7 @@ enum : unsigned {
     ST_TIMEOUT = 16u,
     ST_BUCKET = 32u,
     ST_ALIGN = 64u,  // a shared-memory staging buffer was not aligned for TMA (plain loads used)
+    ST_BOUNDS = 128u,  // an index failed its range check (the access was skipped)
 };
 
 // Fixed-point P2G channels.  Momentum: mass, p(3), f(3).  Thermal: m cp,
@@ -182,6 +183,11 @@ struct Material {
     double E, nu, K, gamma, mu;
     int model;
     int ipow;  // gamma when it is a whole number in 1..16 (the Tait power by multiplication), else 0
+    // modulus of the CFL sound speed sqrt(pmod / rho) (Calculate_time_step,
+    // mpm_particle_timestep.cpp:55-100): K for the fluid model, lambda + 2 mu
+    // otherwise, formed once per material on the host in the reference's
+    // expression order
+    double pmod;
 };
 
 // Dense nodal storage, reference component order, x fastest.

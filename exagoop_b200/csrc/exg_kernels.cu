@@ -526,21 +526,44 @@ __device__ __forceinline__ void particle_bounds(const Params &P, const Material 
     double sq = 0.0;
     for (int d = 0; d < 3; ++d) sq += fabs(q[d]) * 2.0 * P.dxi[d];
     b[CH_SRC] = fabs(vol) * sq + fabs(vol * Q);
-    // Calculate_time_step, mpm_particle_timestep.cpp:55-100
-    double Cs;
-    if (mt.model == 1)
-        Cs = sqrt(mt.K / rho);
-    else {
-        double lambda = mt.E * mt.nu / ((1 + mt.nu) * (1 - 2.0 * mt.nu));
-        double mu = mt.E / (2.0 * (1 + mt.nu));
-        Cs = sqrt((lambda + 2.0 * mu) / rho);
-    }
+    // Calculate_time_step, mpm_particle_timestep.cpp:55-100 (the modulus per
+    // material, Material::pmod)
+    const double Cs = sqrt(mt.pmod / rho);
     double vm = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
     // the particle's CFL step is dxmin / speed; a thread that handles many
     // particles keeps the largest speed and divides once: correctly rounded
     // division by a positive number is monotone, so the minimum step is the
     // same bits
     speed = Cs + vm;
+}
+
+// The same reductions in the mixed-precision G2P without temperature, in
+// FP32: the bounds only set power-of-two fixed-point scales with a factor-2
+// margin, so FP32 rounded upward bounds them as well; the CFL speed is the
+// FP32 sum of FP32 square roots (dt then carries a relative 1e-7 of FP32
+// rounding, as the FP32 velocities it follows).  Saves the FP64 divisions,
+// square roots and channel sums of particle_bounds.
+__device__ __forceinline__ void lean_bounds_f(const Params &P, const Material &mt, float m, const float v[3],
+                                              float vol, const float sig[6], float rho, float (&run_b)[CH_ALL],
+                                              double &run_speed) {
+    const float am = fabsf(m), av = fabsf(vol);
+    run_b[CH_M] = fmaxf(run_b[CH_M], am);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) run_b[CH_P + d] = fmaxf(run_b[CH_P + d], __fmul_ru(am, fabsf(v[d])));
+    const int rowi[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        float s = 0.f;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) s = __fadd_ru(s, __fmul_ru(fabsf(sig[rowi[d][j]]), __double2float_ru(2.0 * P.dxi[j])));
+        float b = __fmul_ru(am, __double2float_ru(fabs(P.gravity[d])));
+        if (P.external_loads) b = __fadd_ru(b, __double2float_ru(fabs(P.extforce[d])));
+        b = __fadd_ru(b, __fmul_ru(av, s));
+        run_b[CH_F + d] = fmaxf(run_b[CH_F + d], b);
+    }
+    const float cs = sqrtf(__double2float_rn(mt.pmod) / rho);
+    const float vm = sqrtf(fmaf(v[2], v[2], fmaf(v[1], v[1], v[0] * v[0])));
+    run_speed = fmax(run_speed, (double)(cs + vm));
 }
 
 __device__ __forceinline__ void block_reduce_push(unsigned long long *bounds, unsigned long long *dtmin,
@@ -971,19 +994,21 @@ constexpr int kCellThreads = 128;
 constexpr int kP2GVariants = 3;
 static_assert(kP2GVariants == EXG_NUM_VARIANTS, "the launchers dispatch EXG_NUM_VARIANTS P2G variants");
 // rows per pass, threads per block, minimum blocks per SM, lane map (0: a
-// warp takes one z-slice of 32 cells, 1: a cell's slices in adjacent lanes)
-//   FP32 cubic:     (4, 256, 1, 0)  (4, 256, 1, 1)  (2, 512, 1, 0)
+// warp takes one z-slice of 32 cells, 1: a cell's slices in adjacent
+// lanes), particle records staged in shared memory (p2g_tile_staged)
+//   FP32 cubic:     (4, 256, 1, 0)  (4, 256, 1, 1)  (4, 256, 1, 0, staged)
 //   FP32 quadratic: (3, 512, 1, 0)  (3, 512, 1, 1)  (3, 256, 2, 0)
 //   FP64 cubic:     (1, 512, 1, 1)  (2, 256, 1, 1)  (1, 512, 1, 0)
 //   FP64 quadratic: (1, 512, 1, 1)  (3, 256, 1, 1)  (1, 512, 1, 0)
 template <class R, int ORD, int V>
 struct P2GVar {
     static constexpr int K = (sizeof(R) == 4 ? 0 : 2) + (ORD == 3 ? 0 : 1);
-    static constexpr int TAB[4][3][4] = {{{4, 256, 1, 0}, {4, 256, 1, 1}, {2, 512, 1, 0}},
-                                         {{3, 512, 1, 0}, {3, 512, 1, 1}, {3, 256, 2, 0}},
-                                         {{1, 512, 1, 1}, {2, 256, 1, 1}, {1, 512, 1, 0}},
-                                         {{1, 512, 1, 1}, {3, 256, 1, 1}, {1, 512, 1, 0}}};
+    static constexpr int TAB[4][3][5] = {{{4, 256, 1, 0, 0}, {4, 256, 1, 1, 0}, {4, 256, 1, 0, 1}},
+                                         {{3, 512, 1, 0, 0}, {3, 512, 1, 1, 0}, {3, 256, 2, 0, 0}},
+                                         {{1, 512, 1, 1, 0}, {2, 256, 1, 1, 0}, {1, 512, 1, 0, 0}},
+                                         {{1, 512, 1, 1, 0}, {3, 256, 1, 1, 0}, {1, 512, 1, 0, 0}}};
     static constexpr int ROWS = TAB[K][V][0], THREADS = TAB[K][V][1], MINB = TAB[K][V][2], MAP = TAB[K][V][3];
+    static constexpr bool STAGED = TAB[K][V][4] != 0;
 };
 
 template <class R, int ORD, bool THERM>
@@ -1588,6 +1613,185 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
     __syncthreads();
 }
 
+// Staged variant of the per-cell factorized P2G (FP32 cubic, four tasks of
+// a cell, one per z-slice).  The direct walk has each of a cell's four tasks
+// load every particle and form its x, y and z weights and terms again.
+// Here the block first writes one record per particle to shared memory --
+// the same FP32 values the direct walk forms: m, m v, m g + f_ext, -V sigma
+// and the weights and derivatives of all four slots of x, y and z -- and
+// the tasks then read them.  Records of the k-th particle of the 32 cells
+// of a group sit at slot 32 k + lane, so the lanes of a warp (the cells of
+// the group) read consecutive words.  A round stages two groups (a group
+// is 32 consecutive cells of the tile; its four slices are four warps of
+// the 256-thread block); a group with a cell of more than kStageK particles
+// takes the direct walk for that round.  The values and the order of every
+// operation on them are the direct walk's, so the results are the same
+// bits.
+constexpr int kStageK = 12, kStageSlots = kStageK * 32, kStageFields = 37;
+enum { SF_M = 0, SF_MV = 1, SF_BD = 4, SF_SG = 7, SF_AXW = 13, SF_AXD = 17, SF_AYW = 21, SF_AYD = 25, SF_AZW = 29,
+       SF_AZD = 33 };
+constexpr size_t kStageBytes = sizeof(float) * 2 * kStageFields * kStageSlots;
+
+template <class R, int ORD, int ROWS>
+__device__ __forceinline__ void p2g_tile_staged(const SplineTables *tab, unsigned *acc_lo, int *acc_hi,
+                                                const Params &P, const Parts<R> &A, const int *active,
+                                                const int *start, const int *cell_start, const int32_t *perm,
+                                                long long *staging, const R *sc, const R *grav, int w, R *rec) {
+    constexpr int W = P2GStc<ORD>::W, NCH = CH_MOM_END;
+    static_assert(ROWS == W, "the staged walk holds whole slices");
+    const int B = P.B, B3 = B * B * B, T = P.T, T3 = T * T * T, ngroups = T3 >> 5;
+    const int t = active[w];
+    int tc[3];
+    tile_coords(P, t, tc);
+    const int s0 = start[t];
+    const int *cs = cell_start + (long long)w * (T3 + 1);
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gsub = wid / W, sz = wid - gsub * W;  // blockDim.x == 2 W 32: group of the pair, z-slice
+    __shared__ int s_over[2];
+    for (int g0 = 0; g0 < ngroups; g0 += 2) {
+        if (threadIdx.x < 2) s_over[threadIdx.x] = 0;
+        __syncthreads();
+        // records of the two groups
+        for (int sl = threadIdx.x; sl < 2 * kStageSlots; sl += blockDim.x) {
+            const int gi = sl / kStageSlots, si = sl - gi * kStageSlots, l = si & 31, k = si >> 5;
+            const int g = g0 + gi;
+            if (g >= ngroups) continue;
+            const int c = g * 32 + l, ka = cs[c], n = cs[c + 1] - ka;
+            if (k == 0 && n > kStageK) s_over[gi] = 1;
+            if (k >= n || k >= kStageK) continue;
+            R *r = rec + (size_t)gi * kStageFields * kStageSlots + si;
+            const int p = perm[s0 + ka + k];
+            if (A.phase[p] != 0) {
+                // not deposited: a zero z weight and derivative in every slot
+                // make each task skip it, as the direct walk skips it
+#pragma unroll
+                for (int j = 0; j < W; ++j) {
+                    r[(SF_AZW + j) * kStageSlots] = R(0);
+                    r[(SF_AZD + j) * kStageSlots] = R(0);
+                }
+                continue;
+            }
+            int iv[3];
+            bool inter[3];
+            double xo[3];
+            cell_frame<R, ORD>(P, tc, c % T, (c / T) % T, c / (T * T), iv, inter, xo);
+            const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
+            double xw[3];
+            R f[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                xw[d] = dual_x(P, d, x[d]);
+                f[d] = (R)((xw[d] - xo[d]) * P.dxi[d]);
+            }
+            AxisW<R, W> ax, ay, az;
+            fact_axis_weights<R, ORD>(*tab, P, 0, xw[0], iv[0], inter[0], f[0], ax);
+            fact_axis_weights<R, ORD>(*tab, P, 1, xw[1], iv[1], inter[1], f[1], ay);
+            fact_axis_weights<R, ORD>(*tab, P, 2, xw[2], iv[2], inter[2], f[2], az);
+            const R m = A.mass[p], vol = A.vol[p];
+            const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
+                              x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] &&
+                              x[2] < P.slab_hi[2];
+            r[SF_M * kStageSlots] = m;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                r[(SF_MV + d) * kStageSlots] = m * A.v[d][p];
+                r[(SF_BD + d) * kStageSlots] = fma(m, grav[d], slab ? (R)P.extforce[d] : R(0));
+            }
+#pragma unroll
+            for (int c6 = 0; c6 < 6; ++c6) r[(SF_SG + c6) * kStageSlots] = -vol * A.sig[c6][p];
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                r[(SF_AXW + j) * kStageSlots] = ax.w[j];
+                r[(SF_AXD + j) * kStageSlots] = ax.dw[j];
+                r[(SF_AYW + j) * kStageSlots] = ay.w[j];
+                r[(SF_AYD + j) * kStageSlots] = ay.dw[j];
+                r[(SF_AZW + j) * kStageSlots] = az.w[j];
+                r[(SF_AZD + j) * kStageSlots] = az.dw[j];
+            }
+        }
+        __syncthreads();
+        const int g = g0 + gsub;
+        const int c = g * 32 + lane;
+        if (g < ngroups && cs[c] < cs[c + 1]) {
+            const int ka = cs[c], kb = cs[c + 1];
+            const int lx = c % T, ly = (c / T) % T, lz = c / (T * T);
+            FactAcc<R> acc[ROWS][W];
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+                for (int sx = 0; sx < W; ++sx) acc[r][sx].zero();
+            bool any = false;
+            if (s_over[gsub]) {
+                int iv[3];
+                bool inter[3];
+                double xo[3];
+                cell_frame<R, ORD>(P, tc, lx, ly, lz, iv, inter, xo);
+                any = fact_deposit_cell<R, ORD, ROWS, 1>(tab, P, A, perm, s0, ka, kb, iv, inter, xo, sz, 0, grav, acc);
+            } else {
+                const R *rg = rec + (size_t)gsub * kStageFields * kStageSlots + lane;
+                for (int k = 0; k < kb - ka; ++k) {
+                    const R *r = rg + k * 32;
+                    const R wz = r[(SF_AZW + sz) * kStageSlots];
+                    const R dwz = r[(SF_AZD + sz) * kStageSlots];
+                    if (wz == R(0) && dwz == R(0)) continue;
+                    any = true;
+                    const R m = r[SF_M * kStageSlots];
+                    R sg[6];
+#pragma unroll
+                    for (int c6 = 0; c6 < 6; ++c6) sg[c6] = r[(SF_SG + c6) * kStageSlots];
+                    const R s0r[3] = {sg[0], sg[1], sg[2]}, s1r[3] = {sg[1], sg[3], sg[4]},
+                            s2r[3] = {sg[2], sg[4], sg[5]};
+                    FactZ<R> z;
+                    z.m = m * wz;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const R bd = r[(SF_BD + d) * kStageSlots];
+                        const R sd0 = d == 0 ? s0r[0] : (d == 1 ? s1r[0] : s2r[0]);
+                        const R sd1 = d == 0 ? s0r[1] : (d == 1 ? s1r[1] : s2r[1]);
+                        const R sd2 = d == 0 ? s0r[2] : (d == 1 ? s1r[2] : s2r[2]);
+                        z.p[d] = r[(SF_MV + d) * kStageSlots] * wz;
+                        z.a[d] = fma(sd2, dwz, bd * wz);
+                        z.b[d] = sd1 * wz;
+                        z.c[d] = sd0 * wz;
+                    }
+                    R axw[W], axd[W];
+#pragma unroll
+                    for (int j = 0; j < W; ++j) {
+                        axw[j] = r[(SF_AXW + j) * kStageSlots];
+                        axd[j] = r[(SF_AXD + j) * kStageSlots];
+                    }
+#pragma unroll
+                    for (int ry = 0; ry < ROWS; ++ry) {
+                        const FactRow<R, 1> row =
+                            fact_row<R>(z, r[(SF_AYW + ry) * kStageSlots], r[(SF_AYD + ry) * kStageSlots]);
+#pragma unroll
+                        for (int sx = 0; sx < W; ++sx) {
+                            if constexpr (sizeof(R) == 4)
+                                acc[ry][sx].add(row, make_float2(axw[sx], axw[sx]), make_float2(axd[sx], axd[sx]));
+                            else
+                                acc[ry][sx].add(row, axw[sx], axd[sx]);
+                        }
+                    }
+                }
+            }
+            if (any) {
+#pragma unroll
+                for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+                    for (int sx = 0; sx < W; ++sx) {
+                        const int idx = ((lz + sz) * B + (ly + r)) * B + (lx + sx);
+#pragma unroll
+                        for (int ch = 0; ch < NCH; ++ch)
+                            fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, acc[r][sx].get(ch), sc[ch]);
+                    }
+            }
+        }
+        __syncthreads();
+    }
+    fx_store<R>(acc_lo, acc_hi, NCH * B3, staging + (long long)w * stg_stride<R>((long long)NCH * B3));
+    __syncthreads();
+}
+
 // Segments a row of a tile is cut into for p2g_tile_xrun (1: whole rows;
 // half rows measured no faster: the block's closing barrier waits for the
 // slowest segment either way).
@@ -1738,9 +1942,13 @@ __global__ void __launch_bounds__(P2GVar<R, ORD, V>::THREADS, P2GVar<R, ORD, V>:
         __syncthreads();
         const int w = s_item;
         if (w >= nitems) break;
-        p2g_tile_factorized<R, ORD, P2GVar<R, ORD, V>::ROWS, P2GVar<R, ORD, V>::MAP>(tab, acc_lo, acc_hi, P, A, active,
-                                                                                start, cell_start, perm, staging,
-                                                                                sc, grav, w);
+        if constexpr (P2GVar<R, ORD, V>::STAGED)
+            p2g_tile_staged<R, ORD, P2GVar<R, ORD, V>::ROWS>(
+                tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm, staging, sc, grav, w,
+                reinterpret_cast<R *>(acc_hi + NCH * B3));
+        else
+            p2g_tile_factorized<R, ORD, P2GVar<R, ORD, V>::ROWS, P2GVar<R, ORD, V>::MAP>(
+                tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm, staging, sc, grav, w);
     }
 }
 
@@ -2723,7 +2931,8 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
                                          const Material *mats, const int *active, const int *start, const int *count,
                                          const int32_t *perm, int mode, int w, double dt, double asr, bool upd_vel,
                                          float (&run_b)[CH_ALL], double &run_speed, bool &red, unsigned &status,
-                                         bool staged = false, int kbeg = 0, int kend = 1 << 30) {
+                                         bool staged = false, int kbeg = 0, int kend = 1 << 30,
+                                         long long np_cap = 1ll << 62) {
     const int B = P.B, B3 = B * B * B;
     const int t = active[w];
     int tc[3];
@@ -2751,11 +2960,19 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
     // v' is read only for rigid particles and for G2P without it
     const bool vel_only = mode == GM_VEL, fresh_vp = vel_only || upd_vel;
     // the particles kbeg .. kend - 1 of the tile (one work item)
-    const int k_end = s0 + min(n, kend);
+    int k_end = s0 + min(n, kend);
+    if (kbeg < 0 || kbeg >= n || s0 < 0 || (long long)s0 + n > np_cap) {
+        status |= ST_BOUNDS;
+        k_end = 0;
+    }
     for (int k = s0 + kbeg + threadIdx.x; k < k_end; k += blockDim.x) {
         if (EXG_G2P_PREFETCH && k + EXG_G2P_PREFETCH * (int)blockDim.x < s0 + n)
             prefetch_particle<R>(A, k + EXG_G2P_PREFETCH * blockDim.x, !fresh_vp);
         const int p = perm[k];
+        if (p < 0 || (long long)p >= np_cap) {
+            status |= ST_BOUNDS;
+            continue;
+        }
         const int phase = A.phase[p];
         double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
         const bool read_vp = !vel_only && (phase != 0 || !upd_vel);
@@ -2832,22 +3049,34 @@ __device__ __forceinline__ void g2p_tile(const SplineTables *tab, R *nb, const P
                             iv2[2] < P.nc[2];
             if (in) {
                 const double vd[3] = {(double)v[0], (double)v[1], (double)v[2]};
-                double sd[6];
+                const float fv[3] = {(float)v[0], (float)v[1], (float)v[2]};
+                float fsig[6];
 #pragma unroll
-                for (int c = 0; c < 6; ++c) sd[c] = (double)sig[c];
-                double q[3] = {0, 0, 0}, cp = 0, T = 0, kc = 0, Q = 0;
-                if (!LEAN && P.use_temp) {
-                    for (int d = 0; d < 3; ++d) q[d] = (double)A.q[d][p];
-                    cp = A.cp[p];
-                    T = A.T[p];
-                    kc = A.kc[p];
-                    Q = A.Q[p];
+                for (int c = 0; c < 6; ++c) fsig[c] = (float)sig[c];
+                // FP32 state without temperature: the same FP32 bounds in
+                // every G2P kernel (lean, full and batched), so a scene's
+                // steps do not depend on which one runs it
+                if (sizeof(R) == 4 && (LEAN || !P.use_temp)) {
+                    lean_bounds_f(P, mt, (float)mass, fv, (float)vol, fsig, (float)rho, run_b, run_speed);
+                } else {
+                    double sd[6];
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) sd[c] = (double)sig[c];
+                    double q[3] = {0, 0, 0}, cp = 0, T = 0, kc = 0, Q = 0;
+                    if (!LEAN && P.use_temp) {
+                        for (int d = 0; d < 3; ++d) q[d] = (double)A.q[d][p];
+                        cp = A.cp[p];
+                        T = A.T[p];
+                        kc = A.kc[p];
+                        Q = A.Q[p];
+                    }
+                    double bnd[CH_ALL], speed;
+                    particle_bounds<R>(P, mt, (double)mass, vd, (double)vol, sd, (double)rho, cp, T, kc, q, Q, bnd,
+                                       speed);
+#pragma unroll
+                    for (int c = 0; c < CH_ALL; ++c) run_b[c] = fmaxf(run_b[c], __double2float_ru(bnd[c]));
+                    run_speed = fmax(run_speed, speed);
                 }
-                double bnd[CH_ALL], speed;
-                particle_bounds<R>(P, mt, (double)mass, vd, (double)vol, sd, (double)rho, cp, T, kc, q, Q, bnd, speed);
-#pragma unroll
-                for (int c = 0; c < CH_ALL; ++c) run_b[c] = fmaxf(run_b[c], __double2float_ru(bnd[c]));
-                run_speed = fmax(run_speed, speed);
                 red = true;
             }
         }
@@ -2962,7 +3191,8 @@ __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g
                                                         const Material *mats, const int *active, const int *start,
                                                         const int *count, const int32_t *perm,
                                                         const int *item_start, Ctl *ctl, int mode,
-                                                        const __grid_constant__ CUtensorMap tmap, int use_tma) {
+                                                        const __grid_constant__ CUtensorMap tmap, int use_tma,
+                                                        long long np) {
     extern __shared__ __align__(128) unsigned char smraw[];
     SplineTables *tab = reinterpret_cast<SplineTables *>(smraw);
     const size_t tab_bytes = (sizeof(SplineTables) + 127) & ~size_t(127);
@@ -3002,9 +3232,11 @@ __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g
             __syncthreads();
             const int it = s_item;
             if (it >= nitems) break;
-            const int w = s_w, kb = (it - item_start[w]) * kG2PChunk;
+            const int w = s_w;
+            int kb = (w >= 0 && w < nact) ? (it - item_start[w]) * kG2PChunk : -1;
+            if (kb < 0) status |= ST_BOUNDS;
             g2p_tile<R, ORD, LEAN>(tab, nb, P, A, Bo, Nd, bc, mats, active, start, count, perm, mode, w, dt, asr,
-                                   upd_vel, run_b, run_speed, red, status, false, kb, kb + kG2PChunk);
+                                   upd_vel, run_b, run_speed, red, status, false, kb, kb + kG2PChunk, np);
         }
     } else {
         // The node block of each tile comes by one TMA box from the nodal
@@ -3040,7 +3272,9 @@ __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g
         for (;;) {
             const int it = s_items[cur];
             if (it >= nitems) break;
-            const int w = s_ws[cur], kb = (it - item_start[w]) * kG2PChunk;
+            const int w = s_ws[cur];
+            int kb = (w >= 0 && w < nact) ? (it - item_start[w]) * kG2PChunk : -1;
+            if (kb < 0) status |= ST_BOUNDS;
             if (NBUF == 2 && threadIdx.x == 0) {
                 // the other buffer's last tile is done (the block synchronised)
                 const int i = atomicAdd(&ctl->next_g2p, 1);
@@ -3058,7 +3292,7 @@ __global__ void __launch_bounds__(G2PVar<R, V>::THREADS, G2PVar<R, V>::MINB) k_g
             }
             g2p_tile<R, ORD, LEAN>(tab, nb + cur * buf_words, P, A, Bo, Nd, bc, mats, active, start, count, perm,
                                    mode, w, dt, asr, upd_vel, run_b, run_speed, red, status, true, kb,
-                                   kb + kG2PChunk);
+                                   kb + kG2PChunk, np);
             if (NBUF == 2) {
                 cur ^= 1;
             } else {
@@ -4134,6 +4368,7 @@ template <class R, int ORD, int V>
 static void p2g_fact_v(Ctx &c) {
     const int B3 = c.P.B * c.P.B * c.P.B;
     size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned) * (fx_lo_words<R>() + 1) * CH_MOM_END * B3;
+    if (P2GVar<R, ORD, V>::STAGED) sm += kStageBytes;
     auto kern = k_p2g_fact<R, ORD, V>;
     constexpr int nthr = P2GVar<R, ORD, V>::THREADS;
     EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -4215,7 +4450,7 @@ static void g2p_lt(Ctx &c, int mode) {
     }
     kern<<<grid, nthr, sm, c.stream>>>(c.P, c.A<R>(), c.Bp<R>(), c.N<R>(), make_bc(c), c.mat_dev, c.sb.active,
                                        c.sb.tile_start, c.sb.tile_count, c.sb.perm, c.sb.item_start, c.ctl, mode,
-                                       c.tmap, c.tma ? 1 : 0);
+                                       c.tmap, c.tma ? 1 : 0, (long long)c.np);
     EXG_CUDA_OK(cudaGetLastError());
 }
 template <class R, int ORD>

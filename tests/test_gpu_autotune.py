@@ -18,6 +18,12 @@ NV = 3
 def small(name, precision):
     if name == "spheres_cubic":
         s, p = scenes.sphere_collision(n=32)
+        # off the lattice, so that weights reach the ends of their supports
+        # (where the truncated spline constants make them a little negative),
+        # and some rigid particles, which no variant deposits
+        dx = 1.0 / 32
+        p.pos += np.random.default_rng(5).uniform(-0.45, 0.45, p.pos.shape) * dx
+        p.idata[nt.I_PHASE, ::23] = 1
     else:
         s, p = scenes.dam_break(n=(32, 16, 16), size=(1.0, 0.5, 0.5), block=(0.4, 0.5, 0.3), seed=31)
     s.precision = precision

@@ -118,12 +118,17 @@ def test_p2g_momentum(order):
         assert e_v < TOL64 and e_p < TOL64, f"node velocity {c}: {e_v:.3e} {e_p:.3e}"
 
 
-@pytest.mark.parametrize("order", [2, 3])
-def test_p2g_light_node_velocities_fp64(order):
+@pytest.mark.parametrize("order,tol", [(2, 1e-12), (3, 1e-9)])
+def test_p2g_light_node_velocities_fp64(order, tol):
     # nodes that only the edges of particles' supports reach carry tiny
     # masses; their velocities p / m must keep relative precision (the FP64
-    # fixed point is 96 bits wide), because the G2P's velocity gradient
-    # weights them by dN, which vanishes more slowly than N
+    # fixed point is 96 bits wide; with 64 bits the error at nodes of 1e-10
+    # of the largest mass was about 5e-7 of the velocity scale), because the
+    # G2P's velocity gradient weights them by dN, which vanishes more slowly
+    # than N.  Cubic: near the end of its support the weight
+    # -r^3/6 + r^2 - 2r + 4/3 cancels terms of order 1 down to (2 - r)^3 / 6,
+    # so two evaluation orders differ by an ulp of 1 there, which at such
+    # nodes is ~1e-11 of the velocity scale; hence the looser cubic bound.
     s, p = small_dam(order=order, seed=60 + order)
     rng = np.random.default_rng(order)
     p.rdata[nt.R_VEL:nt.R_VEL + 3] = rng.normal(0, 0.3, (3, p.n))
@@ -141,7 +146,7 @@ def test_p2g_light_node_velocities_fp64(order):
     for c in range(3):
         vo, vg = o.nodes(nt.N_VEL + c), ctx.nodes(nt.N_VEL + c)
         e = np.abs(vg - vo)[light].max() / np.abs(vo).max()
-        assert e < 1e-12, f"velocity {c} at light nodes: {e:.3e}"
+        assert e < tol, f"velocity {c} at light nodes: {e:.3e}"
 
 
 def test_p2g_mixed_orders():
