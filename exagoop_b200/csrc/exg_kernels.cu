@@ -196,51 +196,65 @@ __global__ void k_keys(Params P, double *x0, double *x1, double *x2, long long n
     keys_body(P, x0, x1, x2, n, key, tile_count, ctl, wrap, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
-// Exclusive scan of tile counts (one block): tile starts, the ascending
-// list of non-empty tiles, each tile's slot in it, and the first fused-G2P
-// work item of each active tile (ceil(count / kG2PChunk) items a tile).
+// Exclusive scan of tile counts (one block of up to 1024 threads): tile
+// starts, the ascending list of non-empty tiles, each tile's slot in it, and
+// the first fused-G2P work item of each active tile (ceil(count /
+// kG2PChunk) items a tile).  Rounds of kScanK tiles a thread: the block
+// loads a round's counts into shared memory with coalesced reads, each
+// thread sums its kScanK consecutive tiles there, one block scan per
+// quantity gives the offsets, and each thread writes its tiles (four rounds
+// for 32,768 tiles where one tile a thread took 32).
+constexpr int kScanK = 8;
 __device__ __forceinline__ void tile_scan_block(int ntiles, const int *count, int *start, int *active, int *slot,
                                                 int *item_start, Ctl *ctl) {
     __shared__ int sh[34];
-    __shared__ int carry, acarry, icarry;
-    if (threadIdx.x == 0) {
-        carry = 0;
-        acarry = 0;
-        icarry = 0;
-    }
-    __syncthreads();
-    for (int base = 0; base < ntiles; base += blockDim.x) {
-        int i = base + threadIdx.x;
-        int c = i < ntiles ? count[i] : 0;
-        int a = c > 0;
-        int it = (c + kG2PChunk - 1) / kG2PChunk;
+    __shared__ int s_cnt[kScanK * 1024];
+    __shared__ int carry[3];
+    if (threadIdx.x < 3) carry[threadIdx.x] = 0;
+    const int R = kScanK * (int)blockDim.x;
+    for (int base = 0; base < ntiles; base += R) {
+        const int nr = min(R, ntiles - base);
+        for (int j = threadIdx.x; j < nr; j += blockDim.x) s_cnt[j] = count[base + j];
+        __syncthreads();
+        const int j0 = min(nr, (int)threadIdx.x * kScanK), j1 = min(nr, j0 + kScanK);
+        int sc = 0, sa = 0, si = 0;
+        for (int j = j0; j < j1; ++j) {
+            const int c = s_cnt[j];
+            sc += c;
+            sa += c > 0;
+            si += (c + kG2PChunk - 1) / kG2PChunk;
+        }
         int tc, ta, ti;
-        int ec = block_exclusive_scan(c, &tc, sh);
-        int ea = block_exclusive_scan(a, &ta, sh);
-        int ei = block_exclusive_scan(it, &ti, sh);
-        if (i < ntiles) {
-            start[i] = carry + ec;
-            if (a) {
-                active[acarry + ea] = i;
-                slot[i] = acarry + ea;
-                item_start[acarry + ea] = icarry + ei;
+        int oc = carry[0] + block_exclusive_scan(sc, &tc, sh);
+        int oa = carry[1] + block_exclusive_scan(sa, &ta, sh);
+        int oi = carry[2] + block_exclusive_scan(si, &ti, sh);
+        for (int j = j0; j < j1; ++j) {
+            const int i = base + j, c = s_cnt[j];
+            start[i] = oc;
+            oc += c;
+            if (c > 0) {
+                active[oa] = i;
+                slot[i] = oa;
+                item_start[oa] = oi;
+                ++oa;
+                oi += (c + kG2PChunk - 1) / kG2PChunk;
             } else {
                 slot[i] = -1;
             }
         }
-        __syncthreads();
+        __syncthreads();  // every thread has read carry and s_cnt
         if (threadIdx.x == 0) {
-            carry += tc;
-            acarry += ta;
-            icarry += ti;
+            carry[0] += tc;
+            carry[1] += ta;
+            carry[2] += ti;
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        ctl->n_active_tiles = acarry;
-        ctl->n_sorted = carry;
-        ctl->n_g2p_items = icarry;
-        item_start[acarry] = icarry;
+        ctl->n_active_tiles = carry[1];
+        ctl->n_sorted = carry[0];
+        ctl->n_g2p_items = carry[2];
+        item_start[carry[1]] = carry[2];
     }
 }
 __global__ void k_tile_scan(int ntiles, const int *count, int *start, int *active, int *slot, int *item_start,

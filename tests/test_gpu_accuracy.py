@@ -68,9 +68,12 @@ def workload(name):
     return scenes.heated_block(seed=99)
 
 
-# mixed-precision bounds on (velocity, stress)
+# mixed-precision bounds on (velocity, stress): the 1e-4 target, except the
+# heated block's velocity, whose oracle spreads by 2.8e-9 under one-ulp
+# changes (tests/golden/self_divergence.json), a 1e6 amplification that
+# turns FP32's 1e-7 into 1e-3
 MIXED = {"spheres": (1e-4, 1e-4), "twisted_column": (1e-4, 1e-4), "heated_block": (1e-3, 1e-4),
-         "dam_break": (5e-3, 5e-2)}
+         "dam_break": (1e-4, 1e-4)}
 
 
 def oracle_1000(s, p, phi):

@@ -332,13 +332,11 @@ def test_mixed_precision_error_elastic():
 
 
 def test_mixed_precision_error_fluid():
-    # dam break: wall reflections are discontinuous in position, so a few
-    # particles whose reflection step differs dominate the L2 norm once the
-    # water reaches a wall (the FP64 GPU path shows the same jump, at 1e-9);
-    # stated tolerance for this workload: 1e-3
+    # the same 1e-4 target on the dam break (Tait fluid, quadratic
+    # B-splines, slip walls)
     s, p = small_dam(seed=13)
     e = mixed_vs_oracle(s, p, 100)
-    assert e["vel"] < 1e-3 and e["stress"] < 1e-3, e
+    assert e["vel"] < 1e-4 and e["stress"] < 1e-4, e
     assert e["jacobian"] < 1e-6, e
 
 
