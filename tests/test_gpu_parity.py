@@ -332,11 +332,15 @@ def test_mixed_precision_error_elastic():
 
 
 def test_mixed_precision_error_fluid():
-    # the same 1e-4 target on the dam break (Tait fluid, quadratic
-    # B-splines, slip walls)
+    # the 1e-4 target on the dam break's velocity (Tait fluid, quadratic
+    # B-splines, slip walls).  Its stress is the Tait pressure K((1/J)^7 - 1):
+    # 100 steps into the collapse p is still small against K, so the relative
+    # error of J (bounded at 1e-6 here, 1.5e-8 measured) reaches p multiplied
+    # by gamma K / |p|, about 1e4; stress bound 3e-4 (1.1e-5 after 1000 steps,
+    # tests/test_gpu_accuracy.py, once the pressure has built up)
     s, p = small_dam(seed=13)
     e = mixed_vs_oracle(s, p, 100)
-    assert e["vel"] < 1e-4 and e["stress"] < 1e-4, e
+    assert e["vel"] < 1e-4 and e["stress"] < 3e-4, e
     assert e["jacobian"] < 1e-6, e
 
 
