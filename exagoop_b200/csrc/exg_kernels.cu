@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <stdexcept>
+#include <type_traits>
 #include "exg_internal.h"
 
 // This file is compiled twice: with EXG_R_FP64 (FP64 kernels plus the
@@ -196,65 +197,83 @@ __global__ void k_keys(Params P, double *x0, double *x1, double *x2, long long n
     keys_body(P, x0, x1, x2, n, key, tile_count, ctl, wrap, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
-// Exclusive scan of tile counts (one block of up to 1024 threads): tile
-// starts, the ascending list of non-empty tiles, each tile's slot in it, and
-// the first fused-G2P work item of each active tile (ceil(count /
-// kG2PChunk) items a tile).  Rounds of kScanK tiles a thread: the block
-// loads a round's counts into shared memory with coalesced reads, each
-// thread sums its kScanK consecutive tiles there, one block scan per
-// quantity gives the offsets, and each thread writes its tiles (four rounds
-// for 32,768 tiles where one tile a thread took 32).
-constexpr int kScanK = 8;
+// Exclusive scan of tile counts (one block, up to 32 warps): tile starts,
+// the ascending list of non-empty tiles, each tile's slot in it, and the
+// first fused-G2P work item of each active tile (ceil(count / kG2PChunk)
+// items a tile).  Each warp owns a contiguous chunk of tiles: it sums its
+// chunk in coalesced 32-tile steps, one barrier exchanges the warp totals,
+// and the warp walks its chunk again with warp-shuffle scans, writing
+// coalesced.  (A block-wide scan per 1024 tiles took 32 barrier-bound
+// rounds for 32,768 tiles; runs of tiles per thread made every store
+// uncoalesced.)
+__device__ __forceinline__ int tile_items(int c) { return (c + kG2PChunk - 1) / kG2PChunk; }
 __device__ __forceinline__ void tile_scan_block(int ntiles, const int *count, int *start, int *active, int *slot,
                                                 int *item_start, Ctl *ctl) {
-    __shared__ int sh[34];
-    __shared__ int s_cnt[kScanK * 1024];
-    __shared__ int carry[3];
-    if (threadIdx.x < 3) carry[threadIdx.x] = 0;
-    const int R = kScanK * (int)blockDim.x;
-    for (int base = 0; base < ntiles; base += R) {
-        const int nr = min(R, ntiles - base);
-        for (int j = threadIdx.x; j < nr; j += blockDim.x) s_cnt[j] = count[base + j];
-        __syncthreads();
-        const int j0 = min(nr, (int)threadIdx.x * kScanK), j1 = min(nr, j0 + kScanK);
-        int sc = 0, sa = 0, si = 0;
-        for (int j = j0; j < j1; ++j) {
-            const int c = s_cnt[j];
-            sc += c;
-            sa += c > 0;
-            si += (c + kG2PChunk - 1) / kG2PChunk;
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ int s_tot[3][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+    const int chunk = ((ntiles + nw - 1) / nw + 31) & ~31;
+    const int c0 = min(ntiles, wid * chunk), c1 = min(ntiles, c0 + chunk);
+    int tc = 0, ta = 0, ti = 0;
+    for (int i = c0 + lane; i < c1; i += 32) {
+        const int c = count[i];
+        tc += c;
+        ta += c > 0;
+        ti += tile_items(c);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        tc += __shfl_xor_sync(FULL, tc, o);
+        ta += __shfl_xor_sync(FULL, ta, o);
+        ti += __shfl_xor_sync(FULL, ti, o);
+    }
+    if (lane == 0) {
+        s_tot[0][wid] = tc;
+        s_tot[1][wid] = ta;
+        s_tot[2][wid] = ti;
+    }
+    __syncthreads();
+    int oc = 0, oa = 0, oi = 0;
+    for (int k = 0; k < wid; ++k) {
+        oc += s_tot[0][k];
+        oa += s_tot[1][k];
+        oi += s_tot[2][k];
+    }
+    for (int base = c0; base < c1; base += 32) {
+        const int i = base + lane;
+        const int c = i < c1 ? count[i] : 0, a = c > 0, it = tile_items(c);
+        int sc = c, sa = a, si = it;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int n1 = __shfl_up_sync(FULL, sc, o), n2 = __shfl_up_sync(FULL, sa, o),
+                      n3 = __shfl_up_sync(FULL, si, o);
+            if (lane >= o) {
+                sc += n1;
+                sa += n2;
+                si += n3;
+            }
         }
-        int tc, ta, ti;
-        int oc = carry[0] + block_exclusive_scan(sc, &tc, sh);
-        int oa = carry[1] + block_exclusive_scan(sa, &ta, sh);
-        int oi = carry[2] + block_exclusive_scan(si, &ti, sh);
-        for (int j = j0; j < j1; ++j) {
-            const int i = base + j, c = s_cnt[j];
-            start[i] = oc;
-            oc += c;
-            if (c > 0) {
-                active[oa] = i;
-                slot[i] = oa;
-                item_start[oa] = oi;
-                ++oa;
-                oi += (c + kG2PChunk - 1) / kG2PChunk;
+        if (i < c1) {
+            start[i] = oc + sc - c;
+            if (a) {
+                const int ai = oa + sa - 1;
+                active[ai] = i;
+                slot[i] = ai;
+                item_start[ai] = oi + si - it;
             } else {
                 slot[i] = -1;
             }
         }
-        __syncthreads();  // every thread has read carry and s_cnt
-        if (threadIdx.x == 0) {
-            carry[0] += tc;
-            carry[1] += ta;
-            carry[2] += ti;
-        }
-        __syncthreads();
+        oc += __shfl_sync(FULL, sc, 31);
+        oa += __shfl_sync(FULL, sa, 31);
+        oi += __shfl_sync(FULL, si, 31);
     }
-    if (threadIdx.x == 0) {
-        ctl->n_active_tiles = carry[1];
-        ctl->n_sorted = carry[0];
-        ctl->n_g2p_items = carry[2];
-        item_start[carry[1]] = carry[2];
+    if (wid == nw - 1 && lane == 0) {
+        // the last warp's offsets now hold the grand totals
+        ctl->n_active_tiles = oa;
+        ctl->n_sorted = oc;
+        ctl->n_g2p_items = oi;
+        item_start[oa] = oi;
     }
 }
 __global__ void k_tile_scan(int ntiles, const int *count, int *start, int *active, int *slot, int *item_start,
@@ -1009,20 +1028,20 @@ constexpr int kP2GVariants = 3;
 static_assert(kP2GVariants == EXG_NUM_VARIANTS, "the launchers dispatch EXG_NUM_VARIANTS P2G variants");
 // rows per pass, threads per block, minimum blocks per SM, lane map (0: a
 // warp takes one z-slice of 32 cells, 1: a cell's slices in adjacent
-// lanes), particle records staged in shared memory (p2g_tile_staged)
-//   FP32 cubic:     (4, 256, 1, 0)  (4, 256, 1, 1)  (4, 256, 1, 0, staged)
-//   FP32 quadratic: (3, 512, 1, 0)  (3, 512, 1, 1)  (3, 256, 2, 0)
-//   FP64 cubic:     (1, 512, 1, 1)  (2, 256, 1, 1)  (1, 512, 1, 0)
-//   FP64 quadratic: (1, 512, 1, 1)  (3, 256, 1, 1)  (1, 512, 1, 0)
+// lanes), channel groups (2: mass and momentum apart from force)
+//   FP32 cubic:     (4, 256, 1, 0, 1)  (4, 256, 1, 1, 1)  (4, 256, 2, 0, 2)
+//   FP32 quadratic: (3, 512, 1, 0, 1)  (3, 512, 1, 1, 1)  (3, 256, 2, 0, 1)
+//   FP64 cubic:     (1, 512, 1, 1, 1)  (2, 256, 1, 1, 1)  (1, 512, 1, 0, 1)
+//   FP64 quadratic: (1, 512, 1, 1, 1)  (3, 256, 1, 1, 1)  (1, 512, 1, 0, 1)
 template <class R, int ORD, int V>
 struct P2GVar {
     static constexpr int K = (sizeof(R) == 4 ? 0 : 2) + (ORD == 3 ? 0 : 1);
-    static constexpr int TAB[4][3][5] = {{{4, 256, 1, 0, 0}, {4, 256, 1, 1, 0}, {4, 256, 1, 0, 1}},
-                                         {{3, 512, 1, 0, 0}, {3, 512, 1, 1, 0}, {3, 256, 2, 0, 0}},
-                                         {{1, 512, 1, 1, 0}, {2, 256, 1, 1, 0}, {1, 512, 1, 0, 0}},
-                                         {{1, 512, 1, 1, 0}, {3, 256, 1, 1, 0}, {1, 512, 1, 0, 0}}};
+    static constexpr int TAB[4][3][5] = {{{4, 256, 1, 0, 1}, {4, 256, 1, 1, 1}, {4, 256, 2, 0, 2}},
+                                         {{3, 512, 1, 0, 1}, {3, 512, 1, 1, 1}, {3, 256, 2, 0, 1}},
+                                         {{1, 512, 1, 1, 1}, {2, 256, 1, 1, 1}, {1, 512, 1, 0, 1}},
+                                         {{1, 512, 1, 1, 1}, {3, 256, 1, 1, 1}, {1, 512, 1, 0, 1}}};
     static constexpr int ROWS = TAB[K][V][0], THREADS = TAB[K][V][1], MINB = TAB[K][V][2], MAP = TAB[K][V][3];
-    static constexpr bool STAGED = TAB[K][V][4] != 0;
+    static constexpr int GROUPS = TAB[K][V][4];
 };
 
 template <class R, int ORD, bool THERM>
@@ -1261,13 +1280,20 @@ struct FactAcc<float> {
         mp0 = p12 = f01 = make_float2(0.f, 0.f);
         f2 = 0.f;
     }
+    // GRP 0: every channel; 1: mass and momentum; 2: force (the same
+    // operations on each channel in every case)
+    template <int GRP = 0>
     __device__ __forceinline__ void add(const FactRow<float, 1> &r, float2 wxx, float2 dxx) {
-        mp0 = __ffma2_rn(wxx, r.mp0, mp0);
-        p12 = __ffma2_rn(wxx, r.p12, p12);
-        f01 = __ffma2_rn(wxx, r.a01, f01);
-        f01 = __ffma2_rn(dxx, r.c01, f01);
-        f2 = fmaf(wxx.x, r.a2, f2);
-        f2 = fmaf(dxx.x, r.c2, f2);
+        if (GRP != 2) {
+            mp0 = __ffma2_rn(wxx, r.mp0, mp0);
+            p12 = __ffma2_rn(wxx, r.p12, p12);
+        }
+        if (GRP != 1) {
+            f01 = __ffma2_rn(wxx, r.a01, f01);
+            f01 = __ffma2_rn(dxx, r.c01, f01);
+            f2 = fmaf(wxx.x, r.a2, f2);
+            f2 = fmaf(dxx.x, r.c2, f2);
+        }
     }
     __device__ __forceinline__ float get(int ch) const {
         switch (ch) {
@@ -1288,14 +1314,19 @@ struct FactAcc<double> {
 #pragma unroll
         for (int i = 0; i < CH_MOM_END; ++i) c[i] = 0.0;
     }
+    template <int GRP = 0>
     __device__ __forceinline__ void add(const FactRow<double, 1> &r, double wx, double dwx) {
-        c[CH_M] = fma(wx, r.m, c[CH_M]);
+        if (GRP != 2) {
+            c[CH_M] = fma(wx, r.m, c[CH_M]);
 #pragma unroll
-        for (int d = 0; d < 3; ++d) c[CH_P + d] = fma(wx, r.p[d], c[CH_P + d]);
+            for (int d = 0; d < 3; ++d) c[CH_P + d] = fma(wx, r.p[d], c[CH_P + d]);
+        }
+        if (GRP != 1) {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            c[CH_F + d] = fma(wx, r.a[d], c[CH_F + d]);
-            c[CH_F + d] = fma(dwx, r.c[d], c[CH_F + d]);
+            for (int d = 0; d < 3; ++d) {
+                c[CH_F + d] = fma(wx, r.a[d], c[CH_F + d]);
+                c[CH_F + d] = fma(dwx, r.c[d], c[CH_F + d]);
+            }
         }
     }
     __device__ __forceinline__ double get(int ch) const { return c[ch]; }
@@ -1446,7 +1477,7 @@ __device__ __forceinline__ void fact_axis_weights(const SplineTables &tab, const
 // and derivative skip it), then the x and y weights, the particle's
 // z-factored terms, and per y row of the task a packed FMA per node and
 // channel pair.  Returns whether any particle contributed.
-template <class R, int ORD, int ROWS, int MAP>
+template <class R, int ORD, int ROWS, int MAP, int GRP = 0>
 __device__ __forceinline__ bool fact_deposit_cell(const SplineTables *tab, const Params &P, const Parts<R> &A,
                                                   const int32_t *perm, int s0, int ka, int kb, const int iv[3],
                                                   const bool inter[3], const double xo[3], int sz, int rg,
@@ -1509,9 +1540,10 @@ __device__ __forceinline__ bool fact_deposit_cell(const SplineTables *tab, const
 #pragma unroll
             for (int sx = 0; sx < W; ++sx) {
                 if constexpr (sizeof(R) == 4)
-                    acc[r][sx].add(row, make_float2(ax.w[sx], ax.w[sx]), make_float2(ax.dw[sx], ax.dw[sx]));
+                    acc[r][sx].template add<GRP>(row, make_float2(ax.w[sx], ax.w[sx]),
+                                                 make_float2(ax.dw[sx], ax.dw[sx]));
                 else
-                    acc[r][sx].add(row, ax.w[sx], ax.dw[sx]);
+                    acc[r][sx].template add<GRP>(row, ax.w[sx], ax.dw[sx]);
             }
         }
     }
@@ -1554,29 +1586,35 @@ __device__ __forceinline__ void cell_frame(const Params &P, const int tc[3], int
     }
 }
 
-// One tile of the factorized P2G, one task per (cell, z-slice, row group):
-// the task's ROWS x W node block accumulates the cell's particles in
-// registers and is added to the tile's fixed-point block after the cell.
-template <class R, int ORD, int ROWS, int MAP>
+// One tile of the factorized P2G, one task per (cell, z-slice, row group,
+// channel group): the task's ROWS x W node block accumulates the cell's
+// particles in registers and is added to the tile's fixed-point block after
+// the cell.  With GROUPS = 2 a cell's mass and momentum (4 channels, no
+// gradients, no stress) and its force (3 channels) go to separate tasks:
+// each holds at most 64 accumulators instead of 112, so two blocks fit an
+// SM, for about the same instructions; each channel's operations are the
+// same as with GROUPS = 1, so the results are the same bits.
+template <class R, int ORD, int ROWS, int MAP, int GROUPS = 1>
 __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned *acc_lo, int *acc_hi, const Params &P,
                                               const Parts<R> &A, const int *active, const int *start,
                                               const int *cell_start, const int32_t *perm, long long *staging,
                                               const R *sc, const R *grav, int w) {
     constexpr int W = P2GStc<ORD>::W;
     static_assert(W % ROWS == 0, "rows per pass must divide the stencil width");
-    constexpr int NPASS = W / ROWS, LANES = W * NPASS, NCH = CH_MOM_END;
+    constexpr int NPASS = W / ROWS, LANES = W * NPASS * GROUPS, NCH = CH_MOM_END;
     const int B = P.B, B3 = B * B * B, T = P.T, T3 = T * T * T;
     const int t = active[w];
     int tc[3];
     tile_coords(P, t, tc);
     const int s0 = start[t];
     const int *cs = cell_start + (long long)w * (T3 + 1);
-    // task u -> (cell, z-slice, row group).  MAP 0: warp u / 32 takes one
-    // (z-slice, row group) of 32 consecutive cells, so the slice is
-    // warp-uniform (one z weight evaluated, no divergence); the LANES warps of
-    // a group of 32 cells are consecutive and run together (the cells'
-    // particles stay in L1).  MAP 1: a cell's LANES tasks sit in adjacent
-    // lanes, which read each particle with one load.
+    // task u -> (cell, sub) with sub = (z-slice, row group, channel group).
+    // MAP 0: warp u / 32 takes one sub of 32 consecutive cells, so the slice
+    // and the channel group are warp-uniform (one z weight evaluated, no
+    // divergence); the LANES warps of a group of 32 cells are consecutive
+    // and run together (the cells' particles stay in L1).  MAP 1: a cell's
+    // LANES tasks sit in adjacent lanes, which read each particle with one
+    // load.
     const int ntask = LANES * T3, step = (int)blockDim.x;
     auto task = [&](int uu, int &cc, int &ss) {
         if (MAP == 0) {
@@ -1591,7 +1629,8 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
     for (int u = threadIdx.x; u < ntask; u += step) {
         int c, sub;
         task(u, c, sub);
-        const int sz = sub / NPASS, rg = sub - sz * NPASS;
+        const int grp = GROUPS == 1 ? 0 : sub % GROUPS, sp = sub / GROUPS;
+        const int sz = sp / NPASS, rg = sp - sz * NPASS;
         const int ka = cs[c], kb = cs[c + 1];
         if (EXG_P2G_PREFETCH && sub == 0) {
             // L2 prefetch of the first particle of the cell this thread takes next
@@ -1606,202 +1645,36 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
         bool inter[3];
         double xo[3];
         cell_frame<R, ORD>(P, tc, lx, ly, lz, iv, inter, xo);
-        FactAcc<R> acc[ROWS][W];
-#pragma unroll
-        for (int r = 0; r < ROWS; ++r)
-#pragma unroll
-            for (int sx = 0; sx < W; ++sx) acc[r][sx].zero();
-        if (!fact_deposit_cell<R, ORD, ROWS, MAP>(tab, P, A, perm, s0, ka, kb, iv, inter, xo, sz, rg, grav, acc))
-            continue;
-#pragma unroll
-        for (int r = 0; r < ROWS; ++r)
-#pragma unroll
-            for (int sx = 0; sx < W; ++sx) {
-                const int idx = ((lz + sz) * B + (ly + rg * ROWS + r)) * B + (lx + sx);
-#pragma unroll
-                for (int ch = 0; ch < NCH; ++ch) fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, acc[r][sx].get(ch), sc[ch]);
-            }
-    }
-    __syncthreads();
-    fx_store<R>(acc_lo, acc_hi, NCH * B3, staging + (long long)w * stg_stride<R>((long long)NCH * B3));
-    __syncthreads();
-}
-
-// Staged variant of the per-cell factorized P2G (FP32 cubic, four tasks of
-// a cell, one per z-slice).  The direct walk has each of a cell's four tasks
-// load every particle and form its x, y and z weights and terms again.
-// Here the block first writes one record per particle to shared memory --
-// the same FP32 values the direct walk forms: m, m v, m g + f_ext, -V sigma
-// and the weights and derivatives of all four slots of x, y and z -- and
-// the tasks then read them.  Records of the k-th particle of the 32 cells
-// of a group sit at slot 32 k + lane, so the lanes of a warp (the cells of
-// the group) read consecutive words.  A round stages two groups (a group
-// is 32 consecutive cells of the tile; its four slices are four warps of
-// the 256-thread block); a group with a cell of more than kStageK particles
-// takes the direct walk for that round.  The values and the order of every
-// operation on them are the direct walk's, so the results are the same
-// bits.
-constexpr int kStageK = 12, kStageSlots = kStageK * 32, kStageFields = 37;
-enum { SF_M = 0, SF_MV = 1, SF_BD = 4, SF_SG = 7, SF_AXW = 13, SF_AXD = 17, SF_AYW = 21, SF_AYD = 25, SF_AZW = 29,
-       SF_AZD = 33 };
-constexpr size_t kStageBytes = sizeof(float) * 2 * kStageFields * kStageSlots;
-
-template <class R, int ORD, int ROWS>
-__device__ __forceinline__ void p2g_tile_staged(const SplineTables *tab, unsigned *acc_lo, int *acc_hi,
-                                                const Params &P, const Parts<R> &A, const int *active,
-                                                const int *start, const int *cell_start, const int32_t *perm,
-                                                long long *staging, const R *sc, const R *grav, int w, R *rec) {
-    constexpr int W = P2GStc<ORD>::W, NCH = CH_MOM_END;
-    static_assert(ROWS == W, "the staged walk holds whole slices");
-    const int B = P.B, B3 = B * B * B, T = P.T, T3 = T * T * T, ngroups = T3 >> 5;
-    const int t = active[w];
-    int tc[3];
-    tile_coords(P, t, tc);
-    const int s0 = start[t];
-    const int *cs = cell_start + (long long)w * (T3 + 1);
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int gsub = wid / W, sz = wid - gsub * W;  // blockDim.x == 2 W 32: group of the pair, z-slice
-    __shared__ int s_over[2];
-    for (int g0 = 0; g0 < ngroups; g0 += 2) {
-        if (threadIdx.x < 2) s_over[threadIdx.x] = 0;
-        __syncthreads();
-        // records of the two groups
-        for (int sl = threadIdx.x; sl < 2 * kStageSlots; sl += blockDim.x) {
-            const int gi = sl / kStageSlots, si = sl - gi * kStageSlots, l = si & 31, k = si >> 5;
-            const int g = g0 + gi;
-            if (g >= ngroups) continue;
-            const int c = g * 32 + l, ka = cs[c], n = cs[c + 1] - ka;
-            if (k == 0 && n > kStageK) s_over[gi] = 1;
-            if (k >= n || k >= kStageK) continue;
-            R *r = rec + (size_t)gi * kStageFields * kStageSlots + si;
-            const int p = perm[s0 + ka + k];
-            if (A.phase[p] != 0) {
-                // not deposited: a zero z weight and derivative in every slot
-                // make each task skip it, as the direct walk skips it
-#pragma unroll
-                for (int j = 0; j < W; ++j) {
-                    r[(SF_AZW + j) * kStageSlots] = R(0);
-                    r[(SF_AZD + j) * kStageSlots] = R(0);
-                }
-                continue;
-            }
-            int iv[3];
-            bool inter[3];
-            double xo[3];
-            cell_frame<R, ORD>(P, tc, c % T, (c / T) % T, c / (T * T), iv, inter, xo);
-            const double x[3] = {A.x[0][p], A.x[1][p], A.x[2][p]};
-            double xw[3];
-            R f[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                xw[d] = dual_x(P, d, x[d]);
-                f[d] = (R)((xw[d] - xo[d]) * P.dxi[d]);
-            }
-            AxisW<R, W> ax, ay, az;
-            fact_axis_weights<R, ORD>(*tab, P, 0, xw[0], iv[0], inter[0], f[0], ax);
-            fact_axis_weights<R, ORD>(*tab, P, 1, xw[1], iv[1], inter[1], f[1], ay);
-            fact_axis_weights<R, ORD>(*tab, P, 2, xw[2], iv[2], inter[2], f[2], az);
-            const R m = A.mass[p], vol = A.vol[p];
-            const bool slab = P.external_loads && x[0] > P.slab_lo[0] && x[0] < P.slab_hi[0] &&
-                              x[1] > P.slab_lo[1] && x[1] < P.slab_hi[1] && x[2] > P.slab_lo[2] &&
-                              x[2] < P.slab_hi[2];
-            r[SF_M * kStageSlots] = m;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                r[(SF_MV + d) * kStageSlots] = m * A.v[d][p];
-                r[(SF_BD + d) * kStageSlots] = fma(m, grav[d], slab ? (R)P.extforce[d] : R(0));
-            }
-#pragma unroll
-            for (int c6 = 0; c6 < 6; ++c6) r[(SF_SG + c6) * kStageSlots] = -vol * A.sig[c6][p];
-#pragma unroll
-            for (int j = 0; j < W; ++j) {
-                r[(SF_AXW + j) * kStageSlots] = ax.w[j];
-                r[(SF_AXD + j) * kStageSlots] = ax.dw[j];
-                r[(SF_AYW + j) * kStageSlots] = ay.w[j];
-                r[(SF_AYD + j) * kStageSlots] = ay.dw[j];
-                r[(SF_AZW + j) * kStageSlots] = az.w[j];
-                r[(SF_AZD + j) * kStageSlots] = az.dw[j];
-            }
-        }
-        __syncthreads();
-        const int g = g0 + gsub;
-        const int c = g * 32 + lane;
-        if (g < ngroups && cs[c] < cs[c + 1]) {
-            const int ka = cs[c], kb = cs[c + 1];
-            const int lx = c % T, ly = (c / T) % T, lz = c / (T * T);
+        // each branch has its own accumulators (only its channels live)
+        auto cell_task = [&](auto grp_tag) {
+            constexpr int G = decltype(grp_tag)::value;
+            constexpr int CH0 = G == 2 ? CH_F : 0, CH1 = G == 1 ? CH_F : NCH;
             FactAcc<R> acc[ROWS][W];
 #pragma unroll
             for (int r = 0; r < ROWS; ++r)
 #pragma unroll
                 for (int sx = 0; sx < W; ++sx) acc[r][sx].zero();
-            bool any = false;
-            if (s_over[gsub]) {
-                int iv[3];
-                bool inter[3];
-                double xo[3];
-                cell_frame<R, ORD>(P, tc, lx, ly, lz, iv, inter, xo);
-                any = fact_deposit_cell<R, ORD, ROWS, 1>(tab, P, A, perm, s0, ka, kb, iv, inter, xo, sz, 0, grav, acc);
-            } else {
-                const R *rg = rec + (size_t)gsub * kStageFields * kStageSlots + lane;
-                for (int k = 0; k < kb - ka; ++k) {
-                    const R *r = rg + k * 32;
-                    const R wz = r[(SF_AZW + sz) * kStageSlots];
-                    const R dwz = r[(SF_AZD + sz) * kStageSlots];
-                    if (wz == R(0) && dwz == R(0)) continue;
-                    any = true;
-                    const R m = r[SF_M * kStageSlots];
-                    R sg[6];
+            if (!fact_deposit_cell<R, ORD, ROWS, MAP, G>(tab, P, A, perm, s0, ka, kb, iv, inter, xo, sz, rg, grav,
+                                                         acc))
+                return;
 #pragma unroll
-                    for (int c6 = 0; c6 < 6; ++c6) sg[c6] = r[(SF_SG + c6) * kStageSlots];
-                    const R s0r[3] = {sg[0], sg[1], sg[2]}, s1r[3] = {sg[1], sg[3], sg[4]},
-                            s2r[3] = {sg[2], sg[4], sg[5]};
-                    FactZ<R> z;
-                    z.m = m * wz;
+            for (int r = 0; r < ROWS; ++r)
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        const R bd = r[(SF_BD + d) * kStageSlots];
-                        const R sd0 = d == 0 ? s0r[0] : (d == 1 ? s1r[0] : s2r[0]);
-                        const R sd1 = d == 0 ? s0r[1] : (d == 1 ? s1r[1] : s2r[1]);
-                        const R sd2 = d == 0 ? s0r[2] : (d == 1 ? s1r[2] : s2r[2]);
-                        z.p[d] = r[(SF_MV + d) * kStageSlots] * wz;
-                        z.a[d] = fma(sd2, dwz, bd * wz);
-                        z.b[d] = sd1 * wz;
-                        z.c[d] = sd0 * wz;
-                    }
-                    R axw[W], axd[W];
+                for (int sx = 0; sx < W; ++sx) {
+                    const int idx = ((lz + sz) * B + (ly + rg * ROWS + r)) * B + (lx + sx);
 #pragma unroll
-                    for (int j = 0; j < W; ++j) {
-                        axw[j] = r[(SF_AXW + j) * kStageSlots];
-                        axd[j] = r[(SF_AXD + j) * kStageSlots];
-                    }
-#pragma unroll
-                    for (int ry = 0; ry < ROWS; ++ry) {
-                        const FactRow<R, 1> row =
-                            fact_row<R>(z, r[(SF_AYW + ry) * kStageSlots], r[(SF_AYD + ry) * kStageSlots]);
-#pragma unroll
-                        for (int sx = 0; sx < W; ++sx) {
-                            if constexpr (sizeof(R) == 4)
-                                acc[ry][sx].add(row, make_float2(axw[sx], axw[sx]), make_float2(axd[sx], axd[sx]));
-                            else
-                                acc[ry][sx].add(row, axw[sx], axd[sx]);
-                        }
-                    }
+                    for (int ch = CH0; ch < CH1; ++ch)
+                        fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, acc[r][sx].get(ch), sc[ch]);
                 }
-            }
-            if (any) {
-#pragma unroll
-                for (int r = 0; r < ROWS; ++r)
-#pragma unroll
-                    for (int sx = 0; sx < W; ++sx) {
-                        const int idx = ((lz + sz) * B + (ly + r)) * B + (lx + sx);
-#pragma unroll
-                        for (int ch = 0; ch < NCH; ++ch)
-                            fx_add_r<R>(acc_lo, acc_hi, ch * B3 + idx, acc[r][sx].get(ch), sc[ch]);
-                    }
-            }
-        }
-        __syncthreads();
+        };
+        if (GROUPS == 1)
+            cell_task(std::integral_constant<int, 0>{});
+        else if (grp == 0)
+            cell_task(std::integral_constant<int, 1>{});
+        else
+            cell_task(std::integral_constant<int, 2>{});
     }
+    __syncthreads();
     fx_store<R>(acc_lo, acc_hi, NCH * B3, staging + (long long)w * stg_stride<R>((long long)NCH * B3));
     __syncthreads();
 }
@@ -1917,7 +1790,7 @@ __device__ __forceinline__ void p2g_tile_xrun(const SplineTables *tab, unsigned 
 // more tasks per thread to even out uneven cells (1.66 against 1.69 ms).
 // Every launch variant of one precision and order uses the same walk, so
 // the register sums and hence the results are the same for all of them.
-template <class R, int ORD, int ROWS, int MAP>
+template <class R, int ORD, int ROWS, int MAP, int GROUPS = 1>
 __device__ __forceinline__ void p2g_tile_factorized(const SplineTables *tab, unsigned *acc_lo, int *acc_hi,
                                                     const Params &P, const Parts<R> &A, const int *active,
                                                     const int *start, const int *cell_start, const int32_t *perm,
@@ -1926,8 +1799,8 @@ __device__ __forceinline__ void p2g_tile_factorized(const SplineTables *tab, uns
         p2g_tile_xrun<R, ORD, ROWS, MAP>(tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm, staging, sc,
                                          grav, w);
     else
-        p2g_tile_fact<R, ORD, ROWS, MAP>(tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm, staging, sc,
-                                         grav, w);
+        p2g_tile_fact<R, ORD, ROWS, MAP, GROUPS>(tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm,
+                                                 staging, sc, grav, w);
 }
 
 template <class R, int ORD, int V>
@@ -1956,13 +1829,8 @@ __global__ void __launch_bounds__(P2GVar<R, ORD, V>::THREADS, P2GVar<R, ORD, V>:
         __syncthreads();
         const int w = s_item;
         if (w >= nitems) break;
-        if constexpr (P2GVar<R, ORD, V>::STAGED)
-            p2g_tile_staged<R, ORD, P2GVar<R, ORD, V>::ROWS>(
-                tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm, staging, sc, grav, w,
-                reinterpret_cast<R *>(acc_hi + NCH * B3));
-        else
-            p2g_tile_factorized<R, ORD, P2GVar<R, ORD, V>::ROWS, P2GVar<R, ORD, V>::MAP>(
-                tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm, staging, sc, grav, w);
+        p2g_tile_factorized<R, ORD, P2GVar<R, ORD, V>::ROWS, P2GVar<R, ORD, V>::MAP, P2GVar<R, ORD, V>::GROUPS>(
+            tab, acc_lo, acc_hi, P, A, active, start, cell_start, perm, staging, sc, grav, w);
     }
 }
 
@@ -2018,30 +1886,34 @@ __device__ void ls_sample(const Params &P, const double *phi, const double x[3],
     }
 }
 
+// Domain walls of one node (nodal_bcs): relvel_in accumulates the wall
+// velocity of each face the node lies on; relvel_out persists across
+// directions.
+__device__ __forceinline__ void node_wall_bcs(const Params &P, int i, int j, int k, double v[3], unsigned &status) {
+    const int id[3] = {i, j, k};
+    double rin[3] = {v[0], v[1], v[2]}, rout[3] = {v[0], v[1], v[2]};
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir) {
+        const bool lo = id[dir] == 0;
+        const bool hi = !lo && id[dir] == P.nc[dir];
+        if (!lo && !hi) continue;
+        double wv[3];
+        for (int d = 0; d < 3; ++d) {
+            wv[d] = lo ? P.wvel_lo[dir * 3 + d] : P.wvel_hi[dir * 3 + d];
+            rin[d] -= wv[d];
+        }
+        double nd[3] = {0, 0, 0};
+        nd[dir] = lo ? 1.0 : -1.0;
+        if (applybc<double>(rin, rout, lo ? P.wmu_lo[dir] : P.wmu_hi[dir], nd, lo ? P.bclo[dir] : P.bchi[dir]) < 0)
+            status |= ST_BC;
+        for (int c = 0; c < 3; ++c) v[c] = rout[c] + wv[c];
+    }
+}
+
 __device__ void node_bcs(const Params &P, const NodeBCArgs &bc, int i, int j, int k, double m, double v[3],
                          unsigned &status) {
     const int id[3] = {i, j, k};
-    // domain walls: relvel_in accumulates the wall velocity of each face
-    // the node lies on; relvel_out persists across directions.
-    {
-        double rin[3] = {v[0], v[1], v[2]}, rout[3] = {v[0], v[1], v[2]};
-#pragma unroll
-        for (int dir = 0; dir < 3; ++dir) {
-            const bool lo = id[dir] == 0;
-            const bool hi = !lo && id[dir] == P.nc[dir];
-            if (!lo && !hi) continue;
-            double wv[3];
-            for (int d = 0; d < 3; ++d) {
-                wv[d] = lo ? P.wvel_lo[dir * 3 + d] : P.wvel_hi[dir * 3 + d];
-                rin[d] -= wv[d];
-            }
-            double nd[3] = {0, 0, 0};
-            nd[dir] = lo ? 1.0 : -1.0;
-            if (applybc<double>(rin, rout, lo ? P.wmu_lo[dir] : P.wmu_hi[dir], nd, lo ? P.bclo[dir] : P.bchi[dir]) < 0)
-                status |= ST_BC;
-            for (int c = 0; c < 3; ++c) v[c] = rout[c] + wv[c];
-        }
-    }
+    node_wall_bcs(P, i, j, k, v, status);
     // UDF wall velocity tables
 #pragma unroll
     for (int dir = 0; dir < 3; ++dir) {
@@ -2109,7 +1981,7 @@ __device__ __forceinline__ void write_rec(R *rec, long long ni, const double v[3
 // partials of the <= 8 node blocks covering the node (exact integer sums),
 // converts to FP64 and applies the nodal operations of the mode.
 // One tile of the nodal kernel: every owned node of tile tiles[w] (or w).
-template <class R, bool THERM>
+template <class R, bool THERM, bool LEAN = false>
 __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, const NodeBCArgs &bc, const int *tiles,
                                            const int *slot, const long long *staging, const double *isc, double dt,
                                            int mode, int flags, int w, unsigned &status) {
@@ -2226,7 +2098,10 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
                 for (int d = 0; d < 3; ++d) v[d] += f[d] / m * dt;
             else
                 v[0] = v[1] = v[2] = 0.0;
-            node_bcs(P, bc, nid[0], nid[1], nid[2], m, v, status);
+            if (LEAN)
+                node_wall_bcs(P, nid[0], nid[1], nid[2], v, status);
+            else
+                node_bcs(P, bc, nid[0], nid[1], nid[2], m, v, status);
             double dv[3] = {0, 0, 0};
             if (m > 0.0)  // store_delta_velocity
                 for (int d = 0; d < 3; ++d) dv[d] = v[d] - vold[d];
@@ -2265,7 +2140,10 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
             double v[3] = {p[0], p[1], p[2]};
             if (m > 0.0)
                 for (int d = 0; d < 3; ++d) v[d] = (m >= P.mass_tol) ? p[d] / m : 0.0;
-            node_bcs(P, bc, nid[0], nid[1], nid[2], m, v, status);
+            if (LEAN)
+                node_wall_bcs(P, nid[0], nid[1], nid[2], v, status);
+            else
+                node_bcs(P, bc, nid[0], nid[1], nid[2], m, v, status);
             double dv[3];
             for (int d = 0; d < 3; ++d) {
                 Nd.c[EXG_N_VEL + d][ni] = (R)v[d];
@@ -2294,7 +2172,7 @@ __device__ __forceinline__ void nodes_tile(const Params &P, const Nodes<R> &Nd, 
 #ifndef EXG_NODES_MINB
 #define EXG_NODES_MINB 4
 #endif
-template <class R, bool THERM>
+template <class R, bool THERM, bool LEAN = false>
 __global__ void __launch_bounds__(kThreads, EXG_NODES_MINB) k_nodes(Params P, Nodes<R> Nd, NodeBCArgs bc, const int *tiles,
                                                     const int *slot, const long long *staging, Ctl *ctl, int mode,
                                                     int flags) {
@@ -2309,7 +2187,7 @@ __global__ void __launch_bounds__(kThreads, EXG_NODES_MINB) k_nodes(Params P, No
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->next_g2p = 0;
     const int nitems = tiles ? ctl->n_touched_tiles : (int)P.ntiles;
     for (int w = blockIdx.x; w < nitems; w += gridDim.x)
-        nodes_tile<R, THERM>(P, Nd, bc, tiles, slot, staging, isc, dt, mode, flags, w, status);
+        nodes_tile<R, THERM, LEAN>(P, Nd, bc, tiles, slot, staging, isc, dt, mode, flags, w, status);
     if (status) atomicOr(&ctl->status, status);
 }
 
@@ -4382,7 +4260,6 @@ template <class R, int ORD, int V>
 static void p2g_fact_v(Ctx &c) {
     const int B3 = c.P.B * c.P.B * c.P.B;
     size_t sm = ((sizeof(SplineTables) + 15) & ~15) + sizeof(unsigned) * (fx_lo_words<R>() + 1) * CH_MOM_END * B3;
-    if (P2GVar<R, ORD, V>::STAGED) sm += kStageBytes;
     auto kern = k_p2g_fact<R, ORD, V>;
     constexpr int nthr = P2GVar<R, ORD, V>::THREADS;
     EXG_CUDA_OK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -4428,16 +4305,25 @@ void EXG_SFX(launch_p2g)(Ctx &c, int flags) {
 void EXG_SFX(launch_nodes)(Ctx &c, int mode, int flags, bool all_tiles) {
     using R = EXG_R;
     const bool th = (flags & (PF_TEMP | PF_SRC)) != 0;
-    static int pgrid = 0, pgrid_th = 0;
+    NodeBCArgs bc = make_bc(c);
+    // walls only (no UDF wall tables, no level-set bodies, no temperature):
+    // the lean instantiation, which inlines the wall BCs
+    bool lean = !th && c.P.num_bodies == 0;
+    for (int h = 0; h < 2; ++h)
+        for (int d = 0; d < 3; ++d) lean = lean && bc.udf[h][d] == nullptr;
+    static int pgrid = 0, pgrid_th = 0, pgrid_lean = 0;
     if (!pgrid) pgrid = persistent_grid(k_nodes<R, false>, 0);
     if (!pgrid_th) pgrid_th = persistent_grid(k_nodes<R, true>, 0);
-    const int pg = th ? pgrid_th : pgrid;  // the grid of the variant launched
+    if (!pgrid_lean) pgrid_lean = persistent_grid(k_nodes<R, false, true>, 0);
+    const int pg = th ? pgrid_th : (lean ? pgrid_lean : pgrid);  // the grid of the variant launched
     int grid = all_tiles ? (int)std::min<long long>(c.P.ntiles, pg) : pg;
     const int *tiles = all_tiles ? nullptr : c.sb.touched;
-    NodeBCArgs bc = make_bc(c);
     if (th)
         k_nodes<R, true><<<grid, kThreads, 0, c.stream>>>(c.P, c.N<R>(), bc, tiles, c.sb.slot, c.staging, c.ctl, mode,
                                                           flags);
+    else if (lean)
+        k_nodes<R, false, true><<<grid, kThreads, 0, c.stream>>>(c.P, c.N<R>(), bc, tiles, c.sb.slot, c.staging,
+                                                                 c.ctl, mode, flags);
     else
         k_nodes<R, false><<<grid, kThreads, 0, c.stream>>>(c.P, c.N<R>(), bc, tiles, c.sb.slot, c.staging, c.ctl,
                                                            mode, flags);
