@@ -988,6 +988,7 @@ constexpr int kCellThreads = 128;
 // block, minimum resident blocks per SM for the register cap); the fused
 // G2P measured fastest at 2 x 256 (128 registers) against 1 x 256, 4 x 128,
 // 3 x 128, 3 x 256, 2 x 384 and 1 x 512
+constexpr int kMaxTileCells = 512;  // T^3 for the largest tile side, 8
 #ifndef EXG_P2G2_THREADS
 #define EXG_P2G2_THREADS 512
 #endif
@@ -1608,14 +1609,36 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
     tile_coords(P, t, tc);
     const int s0 = start[t];
     const int *cs = cell_start + (long long)w * (T3 + 1);
-    // task u -> (cell, sub) with sub = (z-slice, row group, channel group).
-    // MAP 0: warp u / 32 takes one sub of 32 consecutive cells, so the slice
-    // and the channel group are warp-uniform (one z weight evaluated, no
-    // divergence); the LANES warps of a group of 32 cells are consecutive
-    // and run together (the cells' particles stay in L1).  MAP 1: a cell's
-    // LANES tasks sit in adjacent lanes, which read each particle with one
-    // load.
-    const int ntask = LANES * T3, step = (int)blockDim.x;
+    // The tile's non-empty cells, in cell order (a block-wide compaction), so
+    // that no lane walks an empty cell: at a body's surface half the cells
+    // of a tile can be empty.  Cells keep their own sums, and the fixed-point
+    // adds do not depend on the order, so the results do not change.
+    __shared__ int s_cells[kMaxTileCells];
+    __shared__ int s_scan[34];
+    int ncomp;
+    {
+        const int per = (T3 + (int)blockDim.x - 1) / (int)blockDim.x, c0 = (int)threadIdx.x * per;
+        int cnt = 0;
+        for (int k = 0; k < per; ++k) {
+            const int cc = c0 + k;
+            cnt += (cc < T3 && cs[cc] < cs[cc + 1]) ? 1 : 0;
+        }
+        int off = block_exclusive_scan(cnt, &ncomp, s_scan);
+        for (int k = 0; k < per; ++k) {
+            const int cc = c0 + k;
+            if (cc < T3 && cs[cc] < cs[cc + 1]) s_cells[off++] = cc;
+        }
+        __syncthreads();
+    }
+    // task u -> (cell index in the compacted list, sub) with sub = (z-slice,
+    // row group, channel group).  MAP 0: warp u / 32 takes one sub of 32
+    // consecutive listed cells, so the slice and the channel group are
+    // warp-uniform (one z weight evaluated, no divergence); the LANES warps
+    // of a group of 32 cells are consecutive and run together (the cells'
+    // particles stay in L1).  MAP 1: a cell's LANES tasks sit in adjacent
+    // lanes, which read each particle with one load.
+    const int nlist = MAP == 0 ? ((ncomp + 31) & ~31) : ncomp;
+    const int ntask = LANES * nlist, step = (int)blockDim.x;
     auto task = [&](int uu, int &cc, int &ss) {
         if (MAP == 0) {
             const int wi = uu >> 5, g = wi / LANES;
@@ -1627,19 +1650,20 @@ __device__ __forceinline__ void p2g_tile_fact(const SplineTables *tab, unsigned 
         }
     };
     for (int u = threadIdx.x; u < ntask; u += step) {
-        int c, sub;
-        task(u, c, sub);
+        int ci, sub;
+        task(u, ci, sub);
+        if (ci >= ncomp) continue;
+        const int c = s_cells[ci];
         const int grp = GROUPS == 1 ? 0 : sub % GROUPS, sp = sub / GROUPS;
         const int sz = sp / NPASS, rg = sp - sz * NPASS;
         const int ka = cs[c], kb = cs[c + 1];
         if (EXG_P2G_PREFETCH && sub == 0) {
             // L2 prefetch of the first particle of the cell this thread takes next
             const int un = u + step;
-            int cnext = 0, sn = 1;
-            if (un < ntask) task(un, cnext, sn);
-            if (un < ntask && sn == 0) prefetch_cell_head(A, perm, s0, cs, cnext);
+            int cn = 0, sn = 1;
+            if (un < ntask) task(un, cn, sn);
+            if (un < ntask && sn == 0 && cn < ncomp) prefetch_cell_head(A, perm, s0, cs, s_cells[cn]);
         }
-        if (ka == kb) continue;
         const int lx = c % T, ly = (c / T) % T, lz = c / (T * T);
         int iv[3];
         bool inter[3];
