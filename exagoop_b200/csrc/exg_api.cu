@@ -252,6 +252,7 @@ void free_list(std::vector<void *> &al) {
 // device (pid), so the host side is contiguous copies only.
 template <class R>
 void upload_parts(Ctx &c, const exg_particle_soa *h, const std::vector<int32_t> &mat) {
+    if (h->np == 0) return;  // an empty set: storage of one slot, nothing to copy
     Parts<R> &P = c.A<R>();
     const long long n = h->np;
     const bool f64 = sizeof(R) == 8;
