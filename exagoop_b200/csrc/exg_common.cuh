@@ -270,20 +270,23 @@ struct SplineTables {
 // 1-D value and derivative (d/dz) of the boundary-aware spline of `order`
 // and shape `type` at z, as cubicspline_1d / quadraticspline_1d and their
 // derivatives (interpolants.H:215-304).  The cubic interval floor(z)+2 is
-// clamped to [0,3]; the reference reads past its table there.
+// clamped to [0,3]; the reference reads past its table there.  Evaluated in
+// FP64 whatever R, from an FP64 offset, as the reference does: the expanded
+// pieces cancel to ~1e-16 absolute where they fall to zero, which FP32
+// arithmetic would leave at ~1e-7 (R = float rounds the results only).
 template <class R>
-__device__ __forceinline__ void spline_eval(const SplineTables &t, int order, int type, R z, R &val, R &der) {
+__device__ __forceinline__ void spline_eval(const SplineTables &t, int order, int type, double z, R &val, R &der) {
     if (order == 3) {
-        int iv = (int)floor((double)z) + 2;
+        int iv = (int)floor(z) + 2;
         iv = iv < 0 ? 0 : (iv > 3 ? 3 : iv);
         const double *c = t.cub[type][iv];
         const double *d = t.cubd[type][iv];
-        R z2 = z * z, z3 = z2 * z;
-        val = (R)c[0] * z3 + (R)c[1] * z2 + (R)c[2] * z + (R)c[3];
-        der = (R)d[0] * z2 + (R)d[1] * z + (R)d[2];
+        double z2 = z * z, z3 = z2 * z;
+        val = (R)(c[0] * z3 + c[1] * z2 + c[2] * z + c[3]);
+        der = (R)(d[0] * z2 + d[1] * z + d[2]);
     } else {
-        R shift = (type == 2) ? R(1.0) : R(1.5);
-        int raw = (int)floor((double)((z + shift) * R(2)));
+        double shift = (type == 2) ? 1.0 : 1.5;
+        int raw = (int)floor((z + shift) * 2.0);
         int iv = (raw < 0 || raw >= 6) ? -1 : t.qmap[type][raw];
         if (iv < 0) {
             val = R(0);
@@ -291,8 +294,8 @@ __device__ __forceinline__ void spline_eval(const SplineTables &t, int order, in
         } else {
             const double *c = t.quad[type][iv];
             const double *d = t.quadd[type][iv];
-            val = (R)c[0] * z * z + (R)c[1] * z + (R)c[2];
-            der = (R)d[0] * z + (R)d[1];
+            val = (R)(c[0] * z * z + c[1] * z + c[2]);
+            der = (R)(d[0] * z + d[1]);
         }
     }
 }
@@ -321,12 +324,12 @@ __device__ __forceinline__ void axis_weights(const SplineTables &t, const Params
         R val = R(0), der = R(0);
         if (l >= bmin && l < bmax) {
             if (od == 1) {
-                R r = (R)((x - (P.plo[d] + i * dx)) * P.dxi[d]);
-                val = (l == 0) ? (R(1) - r) : r;
+                const double r = (x - (P.plo[d] + i * dx)) * P.dxi[d];
+                val = (l == 0) ? (R)(1.0 - r) : (R)r;
                 der = (l == 0) ? -dxinv : dxinv;
             } else {
                 int ty = shape_type(i + l, P.nc[d], P.periodic[d]);
-                R r = (R)((x - (P.plo[d] + (i + l) * dx)) * P.dxi[d]);
+                const double r = (x - (P.plo[d] + (i + l) * dx)) * P.dxi[d];
                 spline_eval<R>(t, od, ty, r, val, der);
                 der *= dxinv;
             }

@@ -803,19 +803,131 @@ struct FxSum<double> {
     }
 };
 
+// Stencil width of the per-cell P2G: cells (linear, cubic, mixed orders) or
+// nearest-node bins (uniform quadratic).  The block index of stencil slot s
+// is (local cell or bin) + s in every case.
+template <int ORD>
+struct P2GStc {
+    static constexpr int W = (ORD == 1) ? 2 : (ORD == 2 ? 3 : 4);
+};
+
+// FP32 state: the interior B-spline pieces in forms without cancellation.
+// The reference evaluates the expanded pieces (a z^2 + b z + c, and the
+// cubic's a z^3 + ...) in FP64, whose rounding where a piece falls to zero
+// at the support's edge is ~1e-16 absolute.  In FP32 the same expansion
+// leaves ~1e-7 absolute there, against a true weight of (1/2) t^2 = 5e-9
+// for a particle t = 1e-4 inside a quadratic support's edge: the node's
+// weight, and with it its mass, comes out negative or many times too large,
+// its velocity p / m is garbage, and the next steps blow up (particles
+// started on a lattice sit exactly on such edges).  Factored, every weight
+// keeps FP32's relative precision: quadratic (1/2)(1/2 - u)^2, 3/4 - u^2,
+// (1/2)(1/2 + u)^2; cubic g^3 / 6, 2/3 + f^2 (f / 2 - 1),
+// 2/3 + g^2 (g / 2 - 1), f^3 / 6 with g = 1 - f.  The reference's truncated
+// constants round to the same floats as 1/6 and 2/3.  Per slot s (unscaled
+// derivative):
+__device__ __forceinline__ void slot_weight_f32(int ord, float f, int s, float &w, float &dw) {
+    if (ord == 3) {
+        const float t = (s == 0 || s == 2) ? 1.f - f : f, t2 = t * t;
+        if (s == 0 || s == 3) {
+            w = t2 * (t * (float)kOneBySix);
+            dw = (s == 0 ? -0.5f : 0.5f) * t2;
+        } else {
+            w = fmaf(t2, fmaf(0.5f, t, -1.f), (float)kTwoByThree);
+            dw = (s == 1 ? t : -t) * fmaf(1.5f, t, -2.f);
+        }
+    } else if (s == 1) {
+        w = fmaf(-f, f, 0.75f);
+        dw = -2.f * f;
+    } else {
+        const float t = s == 0 ? 0.5f - f : 0.5f + f;
+        w = 0.5f * (t * t);
+        dw = s == 0 ? -t : t;
+    }
+}
+
+// Interior weights of all W slots from the particle's offset f in its cell
+// (cubic, slot s at z = f + 1 - s) or bin (quadratic, u = offset from the
+// bin's node, slot s at u + 1 - s): the fixed pieces of the type-3 splines,
+// the same coefficients as the tables (FP64), or their factored forms (FP32,
+// two slots per packed instruction).
+template <class R, int ORD>
+__device__ __forceinline__ void interior_weights(R f, R dxinv, AxisW<R, P2GStc<ORD>::W> &a) {
+    if constexpr (ORD == 3 && sizeof(R) == 4) {
+        const float o6 = (float)kOneBySix, t3 = (float)kTwoByThree, g = 1.f - f;
+        // end slots (0, 3) in t = (g, f), middle slots (1, 2) in t = (f, g)
+        const float2 e = make_float2(g, f), c = make_float2(f, g);
+        const float2 e2 = __fmul2_rn(e, e), c2 = __fmul2_rn(c, c);
+        const float2 we = __fmul2_rn(e2, __fmul2_rn(e, make_float2(o6, o6)));
+        const float2 wc = __ffma2_rn(c2, __ffma2_rn(make_float2(0.5f, 0.5f), c, make_float2(-1.f, -1.f)),
+                                     make_float2(t3, t3));
+        const float2 de = __fmul2_rn(e2, make_float2(-0.5f * dxinv, 0.5f * dxinv));
+        const float2 dc = __fmul2_rn(__fmul2_rn(c, __ffma2_rn(make_float2(1.5f, 1.5f), c, make_float2(-2.f, -2.f))),
+                                     make_float2(dxinv, -dxinv));
+        a.w[0] = we.x;
+        a.w[1] = wc.x;
+        a.w[2] = wc.y;
+        a.w[3] = we.y;
+        a.dw[0] = de.x;
+        a.dw[1] = dc.x;
+        a.dw[2] = dc.y;
+        a.dw[3] = de.y;
+    } else if constexpr (ORD == 2 && sizeof(R) == 4) {
+        const float2 t = make_float2(0.5f - f, 0.5f + f);
+        const float2 wt = __fmul2_rn(make_float2(0.5f, 0.5f), __fmul2_rn(t, t));
+        a.w[0] = wt.x;
+        a.w[1] = fmaf(-f, f, 0.75f);
+        a.w[2] = wt.y;
+        a.dw[0] = -t.x * dxinv;
+        a.dw[1] = (-2.f * f) * dxinv;
+        a.dw[2] = t.y * dxinv;
+    } else if constexpr (ORD == 3) {
+        const R o6 = (R)kOneBySix, t3 = (R)kTwoByThree, f3 = (R)kFourByThree;
+        R z = f + R(1), z2 = z * z;
+        a.w[0] = fma(-o6, z2 * z, fma(R(1), z2, fma(R(-2), z, f3)));
+        a.dw[0] = fma(R(-0.5), z2, fma(R(2), z, R(-2))) * dxinv;
+        z = f;
+        z2 = z * z;
+        a.w[1] = fma(R(0.5), z2 * z, fma(R(-1), z2, fma(R(0), z, t3)));
+        a.dw[1] = fma(R(1.5), z2, fma(R(-2), z, R(0))) * dxinv;
+        z = f - R(1);
+        z2 = z * z;
+        a.w[2] = fma(R(-0.5), z2 * z, fma(R(-1), z2, fma(R(0), z, t3)));
+        a.dw[2] = fma(R(-1.5), z2, fma(R(-2), z, R(0))) * dxinv;
+        z = f - R(2);
+        z2 = z * z;
+        a.w[3] = fma(o6, z2 * z, fma(R(1), z2, fma(R(2), z, f3)));
+        a.dw[3] = fma(R(0.5), z2, fma(R(2), z, R(2))) * dxinv;
+    } else {
+        // quadratic on the bin's nodes n0 - 1, n0, n0 + 1 (pieces
+        // [0.5, 1.5], [-0.5, 0.5], [-1.5, -0.5])
+        R z = f + R(1);
+        a.w[0] = fma(R(0.5), z * z, fma(R(-1.5), z, R(1.125)));
+        a.dw[0] = (z - R(1.5)) * dxinv;
+        z = f;
+        a.w[1] = fma(R(-1), z * z, fma(R(0), z, R(0.75)));
+        a.dw[1] = (R(-2) * z) * dxinv;
+        z = f - R(1);
+        a.w[2] = fma(R(0.5), z * z, fma(R(1.5), z, R(1.125)));
+        a.dw[2] = (z + R(1.5)) * dxinv;
+    }
+}
+
 // Per-axis weights of a cell whose stencil nodes are all interior (shape
 // type 3): the polynomial piece of each stencil offset is fixed (linear,
 // cubic; quadratic uses dual_axis_weights); same coefficients as the tables.
 template <class R, int ORD>
 __device__ __forceinline__ void axis_weights_interior(const Params &P, int d, double x, int i,
                                                       AxisW<R, Stc<ORD>::W> &a) {
-    const R f = (R)((x - (P.plo[d] + i * P.dx[d])) * P.dxi[d]);
+    const double fd = (x - (P.plo[d] + i * P.dx[d])) * P.dxi[d];
+    const R f = (R)fd;
     const R dxinv = (R)P.dxi[d];
     if (ORD == 1) {
-        a.w[0] = R(1) - f;
+        a.w[0] = (R)(1.0 - fd);  // formed in FP64: relative precision as the weight vanishes
         a.w[1] = f;
         a.dw[0] = -dxinv;
         a.dw[1] = dxinv;
+    } else if constexpr (sizeof(R) == 4 && ORD == 3) {
+        interior_weights<R, 3>(f, dxinv, a);  // factored pieces (FP32)
     } else {
         // type-3 cubic pieces, interval 3 - s for stencil slot s
         const R o6 = (R)kOneBySix, t3 = (R)kTwoByThree, f3 = (R)kFourByThree;
@@ -858,6 +970,10 @@ __device__ __forceinline__ void dual_axis_weights(const SplineTables &tab, const
     const R dxinv = (R)P.dxi[d];
     if (interior) {
         const R u = (R)((x - (P.plo[d] + n0 * P.dx[d])) * P.dxi[d]);
+        if constexpr (sizeof(R) == 4) {
+            interior_weights<R, 2>(u, dxinv, a);  // factored pieces (FP32)
+            return;
+        }
         R z = u + R(1);  // node n0-1, piece [0.5, 1.5]
         a.w[0] = R(0.5) * z * z + R(-1.5) * z + R(1.125);
         a.dw[0] = (z - R(1.5)) * dxinv;
@@ -875,7 +991,7 @@ __device__ __forceinline__ void dual_axis_weights(const SplineTables &tab, const
         R val = R(0), der = R(0);
         if (P.periodic[d] || (n >= 0 && n <= P.nc[d])) {
             const int ty = shape_type(n, P.nc[d], P.periodic[d]);
-            const R r = (R)((x - (P.plo[d] + n * P.dx[d])) * P.dxi[d]);
+            const double r = (x - (P.plo[d] + n * P.dx[d])) * P.dxi[d];
             spline_eval<R>(tab, 2, ty, r, val, der);
             der *= dxinv;
         }
@@ -883,14 +999,6 @@ __device__ __forceinline__ void dual_axis_weights(const SplineTables &tab, const
         a.dw[s] = der;
     }
 }
-
-// Stencil width of the per-cell P2G: cells (linear, cubic, mixed orders) or
-// nearest-node bins (uniform quadratic).  The block index of stencil slot s
-// is (local cell or bin) + s in every case.
-template <int ORD>
-struct P2GStc {
-    static constexpr int W = (ORD == 1) ? 2 : (ORD == 2 ? 3 : 4);
-};
 
 template <class R, int ORD>
 __device__ __forceinline__ void p2g_axis_weights(const SplineTables &tab, const Params &P, int d, double x, int i,
@@ -1362,72 +1470,6 @@ __device__ __forceinline__ FactRow<R, 1> fact_row(const FactZ<R> &z, R wy, R dwy
     return r;
 }
 
-// Interior weights of all W slots from the particle's offset f in its cell
-// (cubic, slot s at z = f + 1 - s) or bin (quadratic, u = offset from the
-// bin's node, slot s at u + 1 - s): the fixed pieces of the type-3 splines,
-// the same coefficients as the tables.  FP32 evaluates two slots per packed
-// FMA.
-template <class R, int ORD>
-__device__ __forceinline__ void interior_weights(R f, R dxinv, AxisW<R, P2GStc<ORD>::W> &a) {
-    if constexpr (ORD == 3 && sizeof(R) == 4) {
-        const float o6 = (float)kOneBySix, t3 = (float)kTwoByThree, f3 = (float)kFourByThree;
-        const float2 dd = make_float2(dxinv, dxinv);
-        // slots (0, 1) at z = (f + 1, f), slots (2, 3) at z = (f - 1, f - 2)
-        const float2 za = make_float2(f + 1.f, f), zb = make_float2(f - 1.f, f - 2.f);
-        const float2 za2 = __fmul2_rn(za, za), zb2 = __fmul2_rn(zb, zb);
-        const float2 za3 = __fmul2_rn(za2, za), zb3 = __fmul2_rn(zb2, zb);
-        const float2 wa = __ffma2_rn(make_float2(-o6, 0.5f), za3,
-                                     __ffma2_rn(make_float2(1.f, -1.f), za2,
-                                                __ffma2_rn(make_float2(-2.f, 0.f), za, make_float2(f3, t3))));
-        const float2 wb = __ffma2_rn(make_float2(-0.5f, o6), zb3,
-                                     __ffma2_rn(make_float2(-1.f, 1.f), zb2,
-                                                __ffma2_rn(make_float2(0.f, 2.f), zb, make_float2(t3, f3))));
-        const float2 da = __fmul2_rn(__ffma2_rn(make_float2(-0.5f, 1.5f), za2,
-                                                __ffma2_rn(make_float2(2.f, -2.f), za, make_float2(-2.f, 0.f))),
-                                     dd);
-        const float2 db = __fmul2_rn(__ffma2_rn(make_float2(-1.5f, 0.5f), zb2,
-                                                __ffma2_rn(make_float2(-2.f, 2.f), zb, make_float2(0.f, 2.f))),
-                                     dd);
-        a.w[0] = wa.x;
-        a.w[1] = wa.y;
-        a.w[2] = wb.x;
-        a.w[3] = wb.y;
-        a.dw[0] = da.x;
-        a.dw[1] = da.y;
-        a.dw[2] = db.x;
-        a.dw[3] = db.y;
-    } else if constexpr (ORD == 3) {
-        const R o6 = (R)kOneBySix, t3 = (R)kTwoByThree, f3 = (R)kFourByThree;
-        R z = f + R(1), z2 = z * z;
-        a.w[0] = fma(-o6, z2 * z, fma(R(1), z2, fma(R(-2), z, f3)));
-        a.dw[0] = fma(R(-0.5), z2, fma(R(2), z, R(-2))) * dxinv;
-        z = f;
-        z2 = z * z;
-        a.w[1] = fma(R(0.5), z2 * z, fma(R(-1), z2, fma(R(0), z, t3)));
-        a.dw[1] = fma(R(1.5), z2, fma(R(-2), z, R(0))) * dxinv;
-        z = f - R(1);
-        z2 = z * z;
-        a.w[2] = fma(R(-0.5), z2 * z, fma(R(-1), z2, fma(R(0), z, t3)));
-        a.dw[2] = fma(R(-1.5), z2, fma(R(-2), z, R(0))) * dxinv;
-        z = f - R(2);
-        z2 = z * z;
-        a.w[3] = fma(o6, z2 * z, fma(R(1), z2, fma(R(2), z, f3)));
-        a.dw[3] = fma(R(0.5), z2, fma(R(2), z, R(2))) * dxinv;
-    } else {
-        // quadratic on the bin's nodes n0 - 1, n0, n0 + 1 (pieces
-        // [0.5, 1.5], [-0.5, 0.5], [-1.5, -0.5])
-        R z = f + R(1);
-        a.w[0] = fma(R(0.5), z * z, fma(R(-1.5), z, R(1.125)));
-        a.dw[0] = (z - R(1.5)) * dxinv;
-        z = f;
-        a.w[1] = fma(R(-1), z * z, fma(R(0), z, R(0.75)));
-        a.dw[1] = (R(-2) * z) * dxinv;
-        z = f - R(1);
-        a.w[2] = fma(R(0.5), z * z, fma(R(1.5), z, R(1.125)));
-        a.dw[2] = (z + R(1.5)) * dxinv;
-    }
-}
-
 // Weight and derivative of one slot (the task's z-slice): the interior piece
 // of that slot alone, or the boundary-aware tables.  s is warp-uniform (the
 // task mapping gives a warp one slice), so the switch does not diverge.
@@ -1436,7 +1478,9 @@ __device__ __forceinline__ void slot_weight(const SplineTables &tab, const Param
                                             bool interior, R f, int s, R &w, R &dw) {
     const R dxinv = (R)P.dxi[d];
     if (interior) {
-        if constexpr (ORD == 3) {
+        if constexpr (sizeof(R) == 4) {
+            slot_weight_f32(ORD, f, s, w, dw);
+        } else if constexpr (ORD == 3) {
             const R o6 = (R)kOneBySix, t3 = (R)kTwoByThree, f3 = (R)kFourByThree;
             const R z = f + R(1 - s), z2 = z * z;
             switch (s) {
@@ -2256,11 +2300,11 @@ __device__ __forceinline__ void interp_axis(const SplineTables &t, const Params 
         const int l = s - 1;
         R val = R(0);
         if (sch == 1) {
-            R r = (R)((x - (P.plo[d] + i * P.dx[d])) * P.dxi[d]);
-            val = (l == 0) ? R(1) - r : (l == 1 ? r : R(0));
+            const double r = (x - (P.plo[d] + i * P.dx[d])) * P.dxi[d];
+            val = (l == 0) ? (R)(1.0 - r) : (l == 1 ? (R)r : R(0));
         } else if (l >= bmin && l < bmax) {
             int ty = shape_type(i + l, P.nc[d], P.periodic[d]);
-            R r = (R)((x - (P.plo[d] + (i + l) * P.dx[d])) * P.dxi[d]);
+            const double r = (x - (P.plo[d] + (i + l) * P.dx[d])) * P.dxi[d];
             R der;
             spline_eval<R>(t, sch, ty, r, val, der);
         }

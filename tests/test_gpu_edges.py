@@ -132,3 +132,43 @@ def test_particle_count_above_int32_is_rejected():
     assert rc == -8  # EXG_ERR_ARG
     assert b"2^31" in ctx.L.exg_last_error(ctx.h)
     ctx.close()
+
+
+def rel_l2(g, r):
+    out = {}
+    for name, f, k in [("vel", nt.R_VEL, 3), ("stress", nt.R_STRESS, 6), ("jacobian", nt.R_JACOBIAN, 1)]:
+        a, b = g.rdata[f:f + k], r.rdata[f:f + k]
+        out[name] = np.linalg.norm(a - b) / np.linalg.norm(b)
+    return out
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_mixed_precision_edges(order):
+    # the same single particle and lattice through the FP32 kernels (mixed
+    # state): binning bit-exact (positions stay FP64), velocity and stress
+    # within 1e-4 relative L2 of the FP64 oracle, J within 1e-6
+    s, dx = unit_box(order)
+    s.precision = nt.PREC_MIXED
+    s64 = s.copy()
+    s64.precision = nt.PREC_FP64
+    ks = np.arange(0, 32) / 32.0
+    g3 = np.stack(np.meshgrid(ks, ks, ks, indexing="ij")).reshape(3, -1)
+    rng = np.random.default_rng(12)
+    cases = [(elastic(np.array([[0.4137], [0.5521], [0.2906]]), dx, 7), 20),
+             (elastic(g3[:, rng.choice(g3.shape[1], 6000, replace=False)], dx, 12, speed=0.02),
+              1 if order == 1 else 10)]
+    for p, nsteps in cases:
+        ctx = nt.Context(s)
+        ctx.upload(p)
+        o = orc.Oracle(s64)
+        o.upload(p)
+        keys, perm = ctx.sort_keys()
+        okeys, operm = o.sort_keys(ctx.tile())
+        assert np.array_equal(keys, okeys) and np.array_equal(perm, operm)
+        ctx.Initialise_Internal_Forces()
+        o.init_internal_forces()
+        ctx.step(nsteps)
+        assert o.step(nsteps) == 0
+        e = rel_l2(ctx.download(), o.download())
+        ctx.close()
+        assert e["vel"] < 1e-4 and e["stress"] < 1e-4 and e["jacobian"] < 1e-6, (p.n, e)
