@@ -172,3 +172,67 @@ def test_mixed_precision_edges(order):
         e = rel_l2(ctx.download(), o.download())
         ctx.close()
         assert e["vel"] < 1e-4 and e["stress"] < 1e-4 and e["jacobian"] < 1e-6, (p.n, e)
+
+
+# More step paths from the same lattice start (coordinates k dx / 2): a
+# periodic axis with particles on its face (the wrap of bins and nodes),
+# per-axis orders (the non-factorized P2G and the generic G2P window), and
+# the thermal path (temperature deposit, thermal G2P, heat flux)
+LATTICE_PATHS = {
+    "periodic_x": dict(order=2, periodic=0),
+    "orders_2_3_3": dict(order=(2, 3, 3)),
+    "thermal": dict(order=2, thermal=True),
+}
+
+
+def lattice_scene(order=2, periodic=None, thermal=False, seed=21):
+    s, dx = unit_box(order if isinstance(order, int) else 2)
+    if not isinstance(order, int):
+        for d in range(3):
+            s.order[d] = order[d]
+    if periodic is not None:
+        # a periodic axis needs three tiles: twice the length at the same dx
+        s.phi[periodic], s.ncells[periodic] = 2.0, 32
+        s.periodic[periodic] = 1
+        s.bclo[periodic] = s.bchi[periodic] = nt.BC_PERIODIC
+    ks = np.arange(0, 32) / 32.0
+    g3 = np.stack(np.meshgrid(ks, ks, ks, indexing="ij")).reshape(3, -1)
+    rng = np.random.default_rng(seed)
+    p = elastic(g3[:, rng.choice(g3.shape[1], 6000, replace=False)], dx, seed, speed=0.02)
+    if thermal:
+        s.use_temp = 1
+        for d in range(3):
+            s.bclo_temp[d] = s.bchi_temp[d] = nt.BCT_ADIABATIC
+        p.rdata[nt.R_TEMPERATURE] = 300.0 + rng.uniform(-20.0, 20.0, p.n)
+        p.rdata[nt.R_SPHEAT] = 900.0
+        p.rdata[nt.R_THERMCOND] = 50.0
+        p.rdata[nt.R_HEATSRC] = 1e5 * (1.0 + rng.uniform(-0.5, 0.5, p.n))
+    return s, p
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", list(LATTICE_PATHS))
+def test_lattice_start_paths(case, precision):
+    s, p = lattice_scene(**LATTICE_PATHS[case])
+    s64 = s.copy()
+    if precision == "mixed":
+        s.precision = nt.PREC_MIXED
+    ctx = nt.Context(s)
+    ctx.upload(p)
+    o = orc.Oracle(s64)
+    o.upload(p)
+    ctx.Initialise_Internal_Forces()
+    o.init_internal_forces()
+    ctx.step(10)
+    assert o.step(10) == 0
+    g, r = ctx.download(), o.download()
+    ctx.close()
+    if precision == "fp64":
+        check(g, r)
+    else:
+        e = rel_l2(g, r)
+        assert e["vel"] < 1e-4 and e["stress"] < 1e-4 and e["jacobian"] < 1e-6, e
+    if s.use_temp:
+        T = r.rdata[nt.R_TEMPERATURE]
+        eT = np.linalg.norm(g.rdata[nt.R_TEMPERATURE] - T) / np.linalg.norm(T)
+        assert eT < (1e-12 if precision == "fp64" else 1e-5), eT
