@@ -186,6 +186,12 @@ std::string validate(const exg_specs &s) {
     for (int d = 0; d < 3; ++d)
         if (s.periodic[d] && (s.ncells[d] % T != 0 || s.ncells[d] < 3 * T))
             return "periodic axes need ncells to be a multiple of the tile edge and at least three tiles";
+    // bin keys are 32-bit (tile index x T^3 + cell in the tile; 0xFFFFFFFF
+    // marks a particle outside the domain): the tile grid, as the context
+    // lays it out, must keep every key below that
+    long long cells = (long long)T * T * T;
+    for (int d = 0; d < 3; ++d) cells *= s.periodic[d] ? s.ncells[d] / T : (s.ncells[d] + 1 + T - 1) / T;
+    if (cells >= 0xFFFFFFFFll) return "grid too large for the 32-bit bin keys (tile-padded cells must stay below 2^32 - 1)";
     if (s.num_bodies < 0 || s.num_bodies > EXG_MAX_BODIES) return "too many level-set bodies";
     return "";
 }

@@ -229,7 +229,10 @@ void exg_particles_free_pinned(exg_particle_soa *p);
 /* ------------------------------------------------------------- context */
 typedef struct exg_ctx exg_ctx;
 
-/* Owns all device memory of one simulation on one GPU. */
+/* Owns all device memory of one simulation on one GPU.  EXG_ERR_CONFIG for
+ * specs the step cannot run: periodic axes of fewer than three tiles or not a
+ * multiple of the tile edge, more than EXG_MAX_BODIES bodies, or a grid whose
+ * tile-padded cell count reaches 2^32 - 1 (32-bit bin keys). */
 int exg_ctx_create(const exg_specs *specs, int device, exg_ctx **out);
 int exg_ctx_destroy(exg_ctx *ctx);
 const char *exg_last_error(const exg_ctx *ctx);

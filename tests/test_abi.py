@@ -4,6 +4,7 @@ import re
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 from exagoop_b200 import native as nt
 
@@ -122,3 +123,14 @@ def test_ascii_particle_file(tmp_path):
     assert p.rdata[nt.R_BULK, 1] == 2e6 and p.rdata[nt.R_GAMMA, 1] == 7
     assert np.allclose(p.pos[:, 1], [0.4, 0.5, 0.6])
     assert p.rdata[nt.R_DEFGRAD, 0] == 1.0 and p.rdata[nt.R_DEFGRAD + 1, 0] == 0.0
+
+
+def test_grid_beyond_the_32_bit_bin_keys_is_refused():
+    # spec validation runs before any CUDA call, so no GPU is needed: 1624^3
+    # cells pad to 204^3 tiles of 512 cells, 4.35e9 keys, beyond 2^32 - 1
+    s = nt.specs_defaults()
+    for d in range(3):
+        s.ncells[d] = 1624
+    with pytest.raises(nt.ExgError) as e:
+        nt.Context(s)
+    assert e.value.code == -1  # EXG_ERR_CONFIG
