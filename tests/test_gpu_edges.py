@@ -182,11 +182,22 @@ LATTICE_PATHS = {
     "periodic_x": dict(order=2, periodic=0),
     "orders_2_3_3": dict(order=(2, 3, 3)),
     "thermal": dict(order=2, thermal=True),
+    "neo_hookean": dict(order=3, model=2),
+    "tait_fluid": dict(order=2, model=1),
+    "musl": dict(order=3, musl=True),
+    "partial_slip_moving_walls": dict(order=2, walls=True),
 }
 
 
-def lattice_scene(order=2, periodic=None, thermal=False, seed=21):
+def lattice_scene(order=2, periodic=None, thermal=False, model=0, musl=False, walls=False, seed=21):
     s, dx = unit_box(order if isinstance(order, int) else 2)
+    if musl:
+        s.stress_update_scheme = 1
+    if walls:
+        for d in range(3):
+            s.bclo[d] = s.bchi[d] = nt.BC_PARTIALSLIP
+            s.wall_mu_lo[d] = s.wall_mu_hi[d] = 0.3
+            s.wall_vel_lo[3 * d + (d + 1) % 3] = 0.05
     if not isinstance(order, int):
         for d in range(3):
             s.order[d] = order[d]
@@ -195,10 +206,22 @@ def lattice_scene(order=2, periodic=None, thermal=False, seed=21):
         s.phi[periodic], s.ncells[periodic] = 2.0, 32
         s.periodic[periodic] = 1
         s.bclo[periodic] = s.bchi[periodic] = nt.BC_PERIODIC
-    ks = np.arange(0, 32) / 32.0
+    # with friction walls, particles on a face that move outwards leave the
+    # domain in the reference as here (EXG_ERR_DOMAIN): keep off the faces
+    ks = np.arange(1 if walls else 0, 31 if walls else 32) / 32.0
     g3 = np.stack(np.meshgrid(ks, ks, ks, indexing="ij")).reshape(3, -1)
     rng = np.random.default_rng(seed)
-    p = elastic(g3[:, rng.choice(g3.shape[1], 6000, replace=False)], dx, seed, speed=0.02)
+    pos = g3[:, rng.choice(g3.shape[1], 6000, replace=False)]
+    if model == 0:
+        p = elastic(pos, dx, seed, speed=0.02)
+    else:
+        # neo-Hookean solid (model 2) or Tait fluid (model 1: K, gamma 7,
+        # viscosity), with the same velocities
+        p = (scenes.make_particles(pos, dx, (2, 2, 2), 1000.0, 2, E=5e3, nu=0.3) if model == 2 else
+             scenes.make_particles(pos, dx, (2, 2, 2), 1000.0, 1, K=2e3, gamma=7.0, visc=1e-3))
+        p.rdata[nt.R_VEL:nt.R_VEL + 3] = np.random.default_rng(seed).normal(0, 0.02, (3, p.n))
+        if model == 2:
+            p.rdata[nt.R_STRAIN:nt.R_STRAIN + 6] = np.random.default_rng(seed + 1).normal(0, 1e-3, (6, p.n))
     if thermal:
         s.use_temp = 1
         for d in range(3):
