@@ -1131,8 +1131,9 @@ constexpr int kMaxTileCells = 512;  // T^3 for the largest tile side, 8
 // cubic): rows per pass, threads per block and the minimum resident blocks
 // per SM (the register cap).  Variant 0 is the default; the autotuner
 // measures all kP2GVariants on the context's own particles and keeps the
-// fastest.  FP32 cubic holds a 4 x 4 slice (112 accumulators) at 256 or 384
-// threads, or half a slice at 512; FP64 holds one or two rows.
+// fastest.  FP32 cubic holds a 4 x 4 slice (112 accumulators, one 256-thread
+// block per SM; half slices at 16 warps per SM measured 35 % slower); FP64
+// holds one or two rows.
 constexpr int kP2GVariants = 3;
 static_assert(kP2GVariants == EXG_NUM_VARIANTS, "the launchers dispatch EXG_NUM_VARIANTS P2G variants");
 // rows per pass, threads per block, minimum blocks per SM, lane map (0: a
